@@ -1,0 +1,202 @@
+/*
+ * qd.h -- C ABI of the B200 split-operator wavepacket propagator.
+ *
+ * The propagator advances a wavepacket psi(R, r, theta) of an atom + diatom
+ * system in reactant Jacobi coordinates with the split-operator scheme
+ *
+ *     psi <- dump * B * Rot(dt/2) * IFFT * T(dt) * FFT * Rot(dt/2) * F * V(dt) * psi
+ *
+ * (F/B = forward/backward Gauss-Legendre transform theta <-> l, T = radial
+ * kinetic phase, Rot = rotational phase, V = potential phase, dump = absorber)
+ * and accumulates the flux through a dividing surface r = r_s into
+ * initial-state-selected reaction probabilities P(E).
+ *
+ * The structs below carry exactly the fields of the Matlab struct that the
+ * reference MEX entry point reads (common/MatlabStructures.h:12-157,
+ * common/MatlabStructures.C:17-97, common-cuda/MatlabStructures.h:100), with the
+ * same names, units (bohr, hartree, atomic time, electron masses) and memory
+ * layouts:
+ *   psi, pot : column-major n1 x n2 x n_theta, index (k*n2 + j)*n1 + i,
+ *              psi complex128 interleaved (re, im), pot real double;
+ *   theta.legendre : (m+1) x n column-major, P_l(x_k) at [l + k*(m+1)].
+ * Arrays are owned by the caller; psi, time.steps and CRP.CRP are updated in
+ * place, as the reference does with Matlab-owned memory.
+ *
+ * Every function returns an int status: QD_OK (0) or a negative QD_ERR_* code;
+ * qd_last_error() returns the message of the last failure on the calling
+ * thread.  Nothing longjmps or throws across this boundary.
+ */
+#ifndef QD_H
+#define QD_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QD_ABI_VERSION 1
+
+/* status codes */
+#define QD_OK               0
+#define QD_ERR_INVALID     -1  /* bad argument / inconsistent sizes          */
+#define QD_ERR_CUDA        -2  /* CUDA runtime or driver error                */
+#define QD_ERR_NOMEM       -3  /* host or device allocation failed            */
+#define QD_ERR_PES         -4  /* PES callback returned non-zero or non-finite*/
+#define QD_ERR_NONFINITE   -5  /* NaN/Inf or norm growth detected in psi      */
+#define QD_ERR_UNSUPPORTED -6  /* size/option not supported by the kernels    */
+#define QD_ERR_IO          -7  /* file read/write error (.grids, checkpoint)  */
+#define QD_ERR_DEVICE      -8  /* device-side status word reported a failure  */
+
+/* arithmetic of the propagation */
+#define QD_PREC_FP64  0  /* plain form: complex128 psi, FP64 everywhere       */
+#define QD_PREC_FP32  1  /* complex64 psi, 3xTF32 tensor-core Legendre GEMM,
+                            FP64 flux-to-P(E) accumulation and norm          */
+
+/* RadialCoordinate (common/MatlabStructures.h:12-39).  r0, k0, delta are the
+ * initial-packet parameters that only the setup helpers read
+ * (H3/InitWavePacket.m:8-13, common/EtaSq.m:3-5). */
+typedef struct qd_radial {
+  int32_t       n;
+  const double *r;      /* n grid points, uniform spacing dr            */
+  double        dr;
+  double        mass;   /* reduced mass in electron masses              */
+  double        r0, k0, delta;
+} qd_radial;
+
+/* AngleCoordinate (common/MatlabStructures.h:41-66). */
+typedef struct qd_angle {
+  int32_t       n;        /* number of Gauss-Legendre points n_theta    */
+  int32_t       m;        /* highest Legendre order; n_l = m + 1        */
+  const double *x;        /* cos(theta_k), n                            */
+  const double *w;        /* quadrature weights, n                      */
+  const double *legendre; /* (m+1) x n, P_l(x_k) at [l + k*(m+1)]       */
+} qd_angle;
+
+/* EvolutionTime (common/MatlabStructures.h:68-90).  steps is in/out: a call
+ * with steps == 0 applies the V(-dt/2) pre-step first (timeEvol.C:664-665). */
+typedef struct qd_time {
+  int32_t total_steps;
+  double  time_step;
+  int32_t steps;
+} qd_time;
+
+/* Called every steps_to_copy_psi_from_device_to_host steps with the current
+ * theta-space psi (host copy, same layout as qd_data.psi) -- the C ABI
+ * counterpart of options.wave_to_matlab (common/wave2matlab.C:26-34,
+ * common-cuda/evolutionCUDA2.cu:540-546).  Return 0 to continue, non-zero to
+ * stop the propagation with QD_ERR_INVALID. */
+typedef int (*qd_progress_fn)(int32_t step, double norm, const double *psi,
+                              void *ctx);
+
+/* Options (common/MatlabStructures.h:92-113; the CUDA variant adds
+ * steps_to_copy_psi_from_device_to_host, common-cuda/MatlabStructures.h:100). */
+typedef struct qd_options {
+  const char    *wave_to_matlab;  /* kept for schema parity; not executed   */
+  const char    *test_name;
+  int32_t        steps_to_copy_psi_from_device_to_host; /* 0 = never       */
+  int32_t        precision;       /* QD_PREC_FP64 (default) or QD_PREC_FP32 */
+  qd_progress_fn progress;        /* optional                               */
+  void          *progress_ctx;
+} qd_options;
+
+/* DumpFunction (common/MatlabStructures.h:115-129).  NULL = absent; the
+ * absorber is applied only when both dump1 and dump2 are present
+ * (timeEvol.h:117). */
+typedef struct qd_dump {
+  const double *dump;
+} qd_dump;
+
+/* CummulativeReactionProbabilities (common/MatlabStructures.h:131-157).
+ * n_dividing_surface is a 1-based r2 index (Gradient3.F:45). */
+typedef struct qd_crp {
+  int32_t       n_dividing_surface;
+  int32_t       n_gradient_points;  /* odd, 3..11 (Gradient3.F:14-26)        */
+  int32_t       n_energies;
+  int32_t       calculate_CRP;
+  const double *energies;           /* hartree, n_energies                   */
+  const double *eta_sq;             /* n_energies                            */
+  double       *CRP;                /* out: P(E), n_energies                 */
+} qd_crp;
+
+/* The whole Matlab struct handed to TimeEvolutionMex / TimeEvolutionMexCUDA
+ * (common/TimeEvolutionMex.C:28-70). */
+typedef struct qd_data {
+  qd_radial   r1;       /* R, atom - diatom distance                         */
+  qd_radial   r2;       /* r, diatom bond length                             */
+  qd_angle    theta;
+  const double *pot;    /* n1*n2*n_theta hartree                             */
+  double     *psi;      /* n1*n2*n_theta complex128 interleaved, in/out      */
+  qd_time     time;
+  qd_options  options;
+  qd_dump     dump1, dump2;
+  qd_crp      CRP;
+} qd_data;
+
+/* ---- library ---------------------------------------------------------- */
+
+int         qd_abi_version(void);
+const char *qd_last_error(void);
+/* Number of CUDA kernel launches issued by this library in this process. */
+int64_t     qd_kernel_launch_count(void);
+
+/* Drop-in for the MEX entry point TimeEvolutionMexCUDA(struct)
+ * (common-cuda/TimeEvolutionMexCUDA.C:20-83, CPU twin
+ * common/TimeEvolutionMex.C:18-78): uploads pot and psi, propagates
+ * data->time.total_steps steps on device 0 of the calling thread, writes psi,
+ * time.steps and (if CRP.calculate_CRP) CRP.CRP back in place.  As in the
+ * reference, the flux accumulators start from zero at every call. */
+int qd_time_evolution(qd_data *data);
+
+/* ---- handle API: device-resident state across calls -------------------- */
+
+typedef struct qd_handle qd_handle;
+
+/* Validate data, build all tables on the device and upload psi.  data's
+ * arrays must stay valid until qd_destroy (psi/CRP are written back by
+ * qd_download / qd_get_crp). */
+int qd_create(const qd_data *data, qd_handle **out);
+int qd_destroy(qd_handle *h);
+/* Propagate n_steps steps (device-resident; no host copies). */
+int qd_propagate(qd_handle *h, int32_t n_steps);
+/* Current theta-space psi (layout of qd_data.psi) into psi_out (host). */
+int qd_get_psi(qd_handle *h, double *psi_out);
+/* Current P(E) (CRPAux.F:34-66 applied to the accumulated phi_E, dphi_E). */
+int qd_get_crp(qd_handle *h, double *crp_out);
+/* Copy psi, time.steps and CRP back into the qd_data given to qd_create. */
+int qd_download(qd_handle *h);
+/* Wavepacket norm after each propagated step (FP64, module_for_psi,
+ * timeEvol.C:220-243); norms_out holds n entries, oldest first, ending at the
+ * last step.  n <= steps propagated by this handle. */
+int qd_get_norms(qd_handle *h, double *norms_out, int32_t n);
+/* Kinetic, rotational, potential and total energy of the current psi
+ * (timeEvol.C:256-283, 323-360, 390-436), hartree. */
+int qd_energies(qd_handle *h, double out4[4]);
+/* Steps propagated so far (the handle's time.steps). */
+int qd_steps(qd_handle *h, int32_t *steps_out);
+/* Average device time per step (ms) of each kernel class over the last
+ * qd_propagate call when profiling is enabled via qd_set_profiling(h, 1). */
+int qd_set_profiling(qd_handle *h, int32_t on);
+int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written);
+
+/* Checkpoint / restart of the full propagation state (psi in l-space, steps,
+ * flux accumulators). */
+int qd_checkpoint(qd_handle *h, const char *path);
+int qd_restore(qd_handle *h, const char *path);
+
+/* ---- setup helpers (the Matlab-side L4 of the reference) --------------- */
+
+/* Gauss-Legendre nodes and weights from a "<n>-LegendreGauss.grids" file in
+ * dir (format of GaussLegendre/*.grids, reader common/GaussLegendre2.m:1-31):
+ * ceil(n/2) lines "x w" of the non-negative half, mirrored; x ascending. */
+int qd_read_grids(const char *dir, int32_t n, double *x, double *w);
+
+/* theta.legendre = P_l(x_k), (m+1) x n column-major, by the three-term
+ * recurrence of common/LegendreP2.m:9-21, computed in FP64 on the GPU. */
+int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QD_H */
