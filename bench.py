@@ -1,0 +1,322 @@
+"""Benchmark: grid-point * steps / s of the split-operator propagator.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1|c0]
+
+Workload (default c1): F + H2, J = 0, extended-LEPS surface on a
+128 x 128 x 64 Jacobi grid (n_l = 64), complex64 wavefunction with the
+3xTF32 Legendre GEMM and FP64 flux-to-P(E) accumulation, dt = 10 au; P(E)
+on 241 energies, 11-point flux stencil.  A step is one split-operator step
+of the whole grid (1,048,576 grid points) including the flux capture.
+
+value   device time (CUDA events on the library's stream) of K steps after
+        W warm-up steps, L2 flushed (256 MiB write) before every step outside
+        the timed spans; whole-job = sum over ranks' points / max rank time.
+e2e     the drop-in entry point qd_time_evolution on host arrays for the
+        same K steps: upload of pot and psi, table set-up, the K steps, P(E)
+        and the download of psi and P(E), wall clock.
+Multi-GPU: independent replicas (one propagation per rank, weak scaling,
+no data-path collective); rank times are reduced with MAX.
+
+--impl reference times the reference's own CPU propagator (common/timeEvol.C,
+built in oracle/_ref against the shims) on the host cores for a bounded
+sample of steps of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "quantum-dynamics_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "grid-pt*steps/s"
+FLUSH_BYTES = 256 << 20
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(name, precision):
+    from qd_b200 import systems as S
+    if name == "c1":
+        data = S.case_c1(precision=precision)
+        desc = ("F+H2 J=0 extended-LEPS, 128x128x64 Jacobi grid, n_l=64, dt=10 au, "
+                "241 energies, 11-point flux")
+    elif name == "c0":
+        data = S.case_c0(precision=precision)
+        desc = "H+H2 J=0 extended-LEPS, 64x64x40 Jacobi grid, n_l=39, dt=10 au, 241 energies"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return data, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(data, max_seconds, steps_cap=None):
+    """Time the reference CPU propagator (oracle/_ref) -- or, if it was not
+    built, the C oracle port -- on this workload: 1 warm-up step, then as many
+    steps as fit in about max_seconds.  Returns (rate, info)."""
+    from oracle import pyoracle as O
+    from qd_b200 import systems as S
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    use_ref = O.ref_available()
+    run = O.ref_time_evolution if use_ref else O.oracle_time_evolution
+    d = S.copy_case(data)
+    d.options.precision = 0
+    d.time.total_steps = 1
+    t0 = time.perf_counter()
+    run(d)
+    t_step = time.perf_counter() - t0
+    n = max(1, int(max_seconds / max(t_step, 1e-6)))
+    if steps_cap:
+        n = min(n, steps_cap)
+    d.time.total_steps = n
+    t0 = time.perf_counter()
+    run(d)
+    dt = time.perf_counter() - t0
+    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    info = {"kind": "reference" if use_ref else "port", "cores": threads,
+            "sample": f"{n} steps (after 1 warm-up step) of the same workload in FP64, "
+                      f"per-step energies/norm/CRP diagnostics included as in the reference"}
+    return pts * n / dt, info
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        return rank, world, local, dist
+    return rank, world, local, None
+
+
+def run_reference(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    data, desc = build_workload(args.workload, 0)
+    budget = float(os.environ.get("QD_REF_SECONDS", "60"))
+    rate, info = cpu_reference_rate(data, budget)
+    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    info["value"] = rate
+    info["unit"] = METRIC
+    line = {"metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": pts / rate * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "grid_points": pts, "precision": "FP64 (reference CPU)"},
+            "cpu_baseline": info,
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    from qd_b200 import QD_PREC_FP32, QD_PREC_FP64, Propagator, TimeEvolutionMexCUDA
+    from qd_b200 import systems as S
+    from qd_b200.timeevolution import kernel_launch_count, set_device
+    set_device(local)
+    prec = QD_PREC_FP64 if args.fp64 else QD_PREC_FP32
+    data, desc = build_workload(args.workload, prec)
+    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    K, W = args.steps, args.warmup
+
+    # --- device-resident throughput -------------------------------------------------
+    d = S.copy_case(data)
+    with Propagator(d) as p:
+        p.propagate_timed(W, FLUSH_BYTES)
+        if dist:
+            dist.barrier()
+        l0 = kernel_launch_count()
+        with ClockSampler(local) as clk:
+            ms = p.propagate_timed(K, FLUSH_BYTES)
+        launches = kernel_launch_count() - l0
+        # per-kernel-class device time (separate, profiled run)
+        from qd_b200 import _abi
+        import ctypes as C
+        lib = _abi.lib()
+        lib.qd_set_profiling(p._h, 1)
+        p.propagate(min(K, 400))
+        buf = (C.c_double * 10)()
+        nw = C.c_int32()
+        lib.qd_kernel_times(p._h, buf, 10, C.byref(nw))
+        lib.qd_set_profiling(p._h, 0)
+        kclass = list(buf)[:nw.value]
+        # unflushed (L2-resident steady state), for context
+        ms_warm = p.propagate_timed(K, 0)
+    t_max = ms
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = pts * K * world / (t_max * 1e-3)
+
+    # --- end to end through the drop-in entry point -------------------------------
+    e = S.copy_case(data)
+    e.time.total_steps = K
+    e.time.steps = 0
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    TimeEvolutionMexCUDA(e)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = data.pot.nbytes + data.psi.nbytes + data.theta.legendre.nbytes
+    d2h = data.psi.nbytes + data.CRP.CRP.nbytes
+    e2e = {"value": pts * K * world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+           "seconds": e2e_s, "entry_point": "qd_time_evolution (TimeEvolutionMexCUDA)"}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # --- roofline of the dominant kernel class ----------------------------------------
+    peak, peak_kind = load_peaks()
+    nl, nth, n12 = int(data.theta.m) + 1, int(data.theta.n), int(data.r1.n) * int(data.r2.n)
+    cb = 16 if args.fp64 else 8        # bytes per complex
+    alg = {  # algorithmic bytes per launch group
+        "column": n12 * (2 * nl * cb + nth * (16 if args.fp64 else 4)),
+        "lines": n12 * nl * 2 * cb,
+    }
+    names = ["column", "lines", "flux_prep", "flux_accum", "crp"]
+    per = {names[i]: kclass[i] for i in range(min(5, len(kclass)))}
+    step_ms = t_max / K
+    dom = max(("column", "lines"), key=lambda k: per.get(k, 0.0))
+    dom_ms = per.get(dom, float("nan"))
+    achieved = alg[dom] / (dom_ms * 1e-3) / 1e9 if dom_ms and dom_ms > 0 else None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": None,
+                "alg_bytes_per_launch": alg[dom], "avg_launch_ms": dom_ms,
+                "kernel_class_ms": per}
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        rate, info = cpu_reference_rate(data, float(os.environ.get("QD_CPU_SECONDS", "20")))
+        info["value"] = rate
+        info["unit"] = METRIC
+        cpu = info
+    curves_per_hour = 3600.0 / (e2e_s / K * 10000) if args.workload == "c1" else None
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32", "data": "synthetic",
+            "config": {"workload": desc, "grid_points": pts,
+                       "precision": "FP64 plain" if args.fp64 else
+                       "complex64 + 3xTF32 Legendre + FP64 flux accumulation",
+                       "l2": "flushed before every step (256 MiB write, outside timed spans)",
+                       "parallelism": f"replicas x{world}"},
+            "value_l2_resident": pts * K / (ms_warm * 1e-3),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "gpu_launches": launches,
+            "pe_curves_per_hour_e2e": curves_per_hour}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0"])
+    ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -140,6 +140,10 @@ int         qd_abi_version(void);
 const char *qd_last_error(void);
 /* Number of CUDA kernel launches issued by this library in this process. */
 int64_t     qd_kernel_launch_count(void);
+/* Select the CUDA device that later calls on this thread use (the library
+ * links the CUDA runtime statically, so the caller's own runtime device
+ * choice does not carry over). */
+int         qd_set_device(int32_t device);
 
 /* Drop-in for the MEX entry point TimeEvolutionMexCUDA(struct)
  * (common-cuda/TimeEvolutionMexCUDA.C:20-83, CPU twin
@@ -160,6 +164,12 @@ int qd_create(const qd_data *data, qd_handle **out);
 int qd_destroy(qd_handle *h);
 /* Propagate n_steps steps (device-resident; no host copies). */
 int qd_propagate(qd_handle *h, int32_t n_steps);
+/* qd_propagate that also reports the device time of the n_steps steps
+ * (CUDA events on the handle's stream, summed over steps).  If
+ * flush_bytes > 0 a buffer of that size is overwritten between steps, outside
+ * the timed spans, so that every step starts with a cold L2. */
+int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes,
+                       double *device_ms);
 /* Current theta-space psi (layout of qd_data.psi) into psi_out (host). */
 int qd_get_psi(qd_handle *h, double *psi_out);
 /* Current P(E) (CRPAux.F:34-66 applied to the accumulated phi_E, dphi_E). */

@@ -1,0 +1,138 @@
+// k_flux.cu -- flux through the dividing surface r = r_s and P(E).
+//
+//   k_flux_prep    psi_s(i,k) and d psi_s/dr by the central differences of
+//                  Gradient3.F:31-167 (3..11 points, same coefficient order),
+//                  from the surface rows captured by the column pass; stored
+//                  in FP64 in a history ring (one slot per step).
+//   k_flux_accum   phi_E += sum_t dt e^{iE t} psi_s(t), dphi_E likewise
+//                  (PsiTimeToPsiEnergyOnSurface, CRPAux.F:4-31, with the
+//                  e^{iEt} recurrence of timeEvol.C:807-817 evaluated
+//                  directly): a complex FP64 GEMM over a chunk of steps.
+//   k_crp          P(E) = Im(sum_k w_k sum_i conj(phi) dphi) / eta^2 dr1/mu2
+//                  (CalculateCRP, CRPAux.F:34-66), warp-shuffle reduction.
+#include "qd_kernels.h"
+
+namespace {
+
+// (offset m, integer coefficient) in the order Gradient3.F sums them
+__constant__ int c_grad_m[5][5] = {
+  {1, 0, 0, 0, 0}, {2, 1, 0, 0, 0}, {3, 2, 1, 0, 0}, {4, 3, 2, 1, 0}, {5, 4, 3, 2, 1}};
+__constant__ double c_grad_c[5][5] = {
+  {1, 0, 0, 0, 0}, {-1, 8, 0, 0, 0}, {1, -9, 45, 0, 0}, {-3, 32, -168, 672, 0},
+  {2, -25, 150, -600, 2100}};
+
+template <typename R>
+__global__ void k_flux_prep(FluxParams p)
+{
+  typedef typename Cplx<R>::T C;
+  const int nq = p.nth * p.n1;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  const C *s = reinterpret_cast<const C *>(p.surf);
+  const long rs = (long)nq;                 // row stride in surf
+  const int h = p.h, sel = h - 1;
+  const double2 v = to_z(s[(long)h * rs + q]);
+  double2 g = make_double2(0.0, 0.0);
+  for (int t = 0; t < h; t++) {
+    const int m = c_grad_m[sel][t];
+    const double c = c_grad_c[sel][t];
+    const double2 a = to_z(s[(long)(h + m) * rs + q]);
+    const double2 b = to_z(s[(long)(h - m) * rs + q]);
+    const double dx = a.x - b.x, dy = a.y - b.y;
+    if (t == 0 && c == 1.0) { g.x = dx; g.y = dy; }
+    else if (t == 0 && c == -1.0) { g.x = -dx; g.y = -dy; }
+    else { g.x += c * dx; g.y += c * dy; }
+  }
+  g.x /= p.den_dx;
+  g.y /= p.den_dx;
+  const long o = (long)p.slot * nq + q;
+  p.ring_psi[o] = v;
+  p.ring_g[o] = g;
+}
+
+constexpr int EB = 8;          // energies per CTA
+constexpr int TMAX = 128;      // max steps per chunk
+
+__global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
+{
+  __shared__ double2 ph[EB][TMAX];
+  const int e0 = blockIdx.y * EB;
+  for (int x = threadIdx.x; x < EB * p.nt; x += blockDim.x) {
+    const int e = x / p.nt, t = x % p.nt;
+    double2 c = make_double2(0.0, 0.0);
+    if (e0 + e < p.ne) {
+      const double edt = p.energies[e0 + e] * p.dt;
+      double sn, cs;
+      sincos(edt * (double)(p.t0 + t + 1), &sn, &cs);
+      c = make_double2(p.dt * cs, p.dt * sn);
+    }
+    ph[e][t] = c;
+  }
+  __syncthreads();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= p.nq) return;
+  double2 a[EB], b[EB];
+#pragma unroll
+  for (int e = 0; e < EB; e++) { a[e] = make_double2(0, 0); b[e] = make_double2(0, 0); }
+  for (int t = 0; t < p.nt; t++) {
+    const double2 zp = p.ring_psi[(long)t * p.nq + q];
+    const double2 zg = p.ring_g[(long)t * p.nq + q];
+#pragma unroll
+    for (int e = 0; e < EB; e++) {
+      const double2 c = ph[e][t];
+      a[e].x += c.x * zp.x - c.y * zp.y; a[e].y += c.x * zp.y + c.y * zp.x;
+      b[e].x += c.x * zg.x - c.y * zg.y; b[e].y += c.x * zg.y + c.y * zg.x;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < EB; e++) {
+    if (e0 + e >= p.ne) break;
+    const long o = (long)(e0 + e) * p.nq + q;
+    double2 f = p.fai[o], df = p.dfai[o];
+    f.x += a[e].x; f.y += a[e].y; df.x += b[e].x; df.y += b[e].y;
+    p.fai[o] = f; p.dfai[o] = df;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_crp(CrpParams p)
+{
+  __shared__ double red[32];
+  const int e = blockIdx.x;
+  const long nq = (long)p.nth * p.n1;
+  const double2 *f = p.fai + (long)e * nq, *df = p.dfai + (long)e * nq;
+  double s = 0.0;
+  for (long q = threadIdx.x; q < nq; q += blockDim.x) {
+    const int k = (int)(q / p.n1);
+    const double2 a = f[q], b = df[q];
+    s += p.w[k] * (a.x * b.y - a.y * b.x);   // Im(conj(phi) dphi)
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) p.crp[e] = s / p.eta_sq[e] * p.dr1_mu2;
+}
+
+}  // namespace
+
+template <typename R>
+cudaError_t launch_flux_prep(const FluxParams &p, cudaStream_t s)
+{
+  const int nq = p.nth * p.n1;
+  k_flux_prep<R><<<(nq + 255) / 256, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+template cudaError_t launch_flux_prep<float>(const FluxParams &, cudaStream_t);
+template cudaError_t launch_flux_prep<double>(const FluxParams &, cudaStream_t);
+
+cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
+{
+  if (p.nt <= 0) return cudaSuccess;
+  if (p.nt > TMAX) return cudaErrorInvalidValue;
+  dim3 grid((p.nq + 255) / 256, (p.ne + EB - 1) / EB);
+  k_flux_accum<<<grid, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crp(const CrpParams &p, cudaStream_t s)
+{
+  k_crp<<<p.ne, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}

@@ -1,0 +1,152 @@
+// k_setup.cu -- one-off tables of a propagation, built on the GPU in FP64.
+//
+//   FP64 form (the reference's tables, same arithmetic):
+//     expV[k][j][i] = exp(-i V dt)                       setup_exp_ipot_dt    timeEvol.C:438-463
+//     rot[l][j][i]  = exp(-i l(l+1)(I1_i + I2_j) dt/2)   setup_exp_irot_dt_2  timeEvol.C:465-491
+//     kin[j][i]     = exp(-i(T1_i + T2_j) dt) / n1 / n2  setup_exp_ikin_dt    timeEvol.C:493-517
+//   FP32 form: the same phases as fractions of a turn, reduced in FP64 to
+//   [-1/2, 1/2] and stored as float, so that the complex64 propagation
+//   evaluates exp(2 pi i turns) with sincospif and no large-argument loss.
+//   Legendre matrices: P[k][l] = P_l(x_k) (LegendreP2.m:9-21 recurrence) and
+//   WP[k][l] = (l+1/2) w_k P_l(x_k) (setup_weight_legendre, timeEvol.C:737-760).
+#include "qd_kernels.h"
+
+namespace {
+
+__device__ __forceinline__ double turns(double phase_rad)
+{
+  const double t = phase_rad * 0.15915494309189533576888376337251;  // 1/(2 pi)
+  return t - rint(t);
+}
+
+__global__ void k_tables_fp64(int n1, int n2, int nth, int nl, double dt, const double *pot,
+                              const double *I1, const double *I2, const double *T1,
+                              const double *T2, double2 *expV, double2 *rot, double2 *kin)
+{
+  const long n12 = (long)n1 * n2;
+  const long nv = n12 * nth, nr = n12 * nl;
+  const double mdt = -dt, mdt2 = -dt / 2;
+  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < nv + nr + n12;
+       g += (long)gridDim.x * blockDim.x) {
+    double s, c;
+    if (g < nv) {
+      sincos(mdt * pot[g], &s, &c);
+      expV[g] = make_double2(c, s);
+    } else if (g < nv + nr) {
+      const long q = g - nv;
+      const int l = (int)(q / n12);
+      const long ij = q % n12;
+      const int j = (int)(ij / n1), i = (int)(ij % n1);
+      const double x = (double)(l * (l + 1)) * (I1[i] + I2[j]);
+      sincos(x * mdt2, &s, &c);
+      rot[q] = make_double2(c, s);
+    } else {
+      const long ij = g - nv - nr;
+      const int j = (int)(ij / n1), i = (int)(ij % n1);
+      sincos((T1[i] + T2[j]) * mdt, &s, &c);
+      kin[ij] = make_double2(c / n1 / n2, s / n1 / n2);
+    }
+  }
+}
+
+__global__ void k_tables_fp32(int n1, int n2, int nth, int nl, double dt, const double *pot,
+                              const double *I1, const double *I2, const double *T1,
+                              const double *T2, float *vturn, float *rt1, float *rt2,
+                              float *kt1, float *kt2)
+{
+  const long nv = (long)n1 * n2 * nth;
+  const long a1 = (long)nl * n1, a2 = (long)nl * n2;
+  const long total = nv + a1 + a2 + n1 + n2;
+  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < total;
+       g += (long)gridDim.x * blockDim.x) {
+    if (g < nv) {
+      vturn[g] = (float)turns(-dt * pot[g]);
+    } else if (g < nv + a1) {
+      const long q = g - nv;
+      const int l = (int)(q / n1), i = (int)(q % n1);
+      rt1[q] = (float)turns(-(double)(l * (l + 1)) * I1[i] * dt / 2);
+    } else if (g < nv + a1 + a2) {
+      const long q = g - nv - a1;
+      const int l = (int)(q / n2), j = (int)(q % n2);
+      rt2[q] = (float)turns(-(double)(l * (l + 1)) * I2[j] * dt / 2);
+    } else if (g < nv + a1 + a2 + n1) {
+      const int i = (int)(g - nv - a1 - a2);
+      kt1[i] = (float)turns(-T1[i] * dt);
+    } else {
+      const int j = (int)(g - nv - a1 - a2 - n1);
+      kt2[j] = (float)turns(-T2[j] * dt);
+    }
+  }
+}
+
+__global__ void k_legendre_matrices(int nth, int nl, const double *w, const double *legendre,
+                                    double *P, double *WP, float *P32, float *WP32)
+{
+  const int total = nth * nl;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const int k = g / nl, l = g % nl;
+    const double p = legendre[l + (long)k * nl];
+    const double f = l + 0.5;
+    const double wp = f * w[k] * p;
+    P[g] = p;
+    WP[g] = wp;
+    P32[g] = (float)p;
+    WP32[g] = (float)wp;
+  }
+}
+
+// P_0..P_m at each node by the three-term recurrence of LegendreP2.m:9-21;
+// one thread per node; output (m+1) x n column-major.
+__global__ void k_legendre_p2(int n, int m, const double *x, double *out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double xk = x[k];
+  double *v = out + (long)k * (m + 1);
+  double p0 = 1.0, p1 = xk;
+  v[0] = 1.0;
+  if (m >= 1) v[1] = xk;
+  for (int i = 2; i <= m; i++) {
+    const double p2 = (2.0 - 1.0 / i) * xk * p1 - (1.0 - 1.0 / i) * p0;
+    v[i] = p2;
+    p0 = p1;
+    p1 = p2;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_setup_tables_fp64(int n1, int n2, int nth, int nl, double dt,
+                                     const double *pot, const double *I1, const double *I2,
+                                     const double *T1, const double *T2, double2 *expV,
+                                     double2 *rot, double2 *kin, cudaStream_t s)
+{
+  k_tables_fp64<<<148 * 8, 256, 0, s>>>(n1, n2, nth, nl, dt, pot, I1, I2, T1, T2, expV, rot, kin);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
+                                     const double *pot, const double *I1, const double *I2,
+                                     const double *T1, const double *T2, float *vturn,
+                                     float *rt1, float *rt2, float *kt1, float *kt2,
+                                     cudaStream_t s)
+{
+  k_tables_fp32<<<148 * 8, 256, 0, s>>>(n1, n2, nth, nl, dt, pot, I1, I2, T1, T2, vturn, rt1,
+                                        rt2, kt1, kt2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_legendre_matrices(int nth, int nl, const double *, const double *w,
+                                     const double *legendre, double *P, double *WP,
+                                     float *P32, float *WP32, cudaStream_t s)
+{
+  k_legendre_matrices<<<(nth * nl + 255) / 256, 256, 0, s>>>(nth, nl, w, legendre, P, WP, P32,
+                                                             WP32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_legendre_p2(int n, int m, const double *x, double *legendre, cudaStream_t s)
+{
+  k_legendre_p2<<<(n + 127) / 128, 128, 0, s>>>(n, m, x, legendre);
+  return cudaGetLastError();
+}

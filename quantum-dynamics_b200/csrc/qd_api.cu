@@ -1,0 +1,748 @@
+// qd_api.cu -- C ABI of the propagator (include/qd.h): validation, device
+// state, the step loop and the reference-facing entry point
+// qd_time_evolution (the counterpart of TimeEvolutionMexCUDA,
+// common-cuda/TimeEvolutionMexCUDA.C:20-83).
+//
+// One step of the reference (timeEvol.C:649-685) is issued as
+//   column pass  (B, dump, flux rows, norm of step n; V, F of step n+1)
+//   l-space pass (Rot/2, FFT, T, IFFT, Rot/2 of step n+1)
+//   flux prep    (psi_s, d psi_s/dr of step n into the FP64 history ring)
+// with the E-accumulation GEMM every QD_RING steps and P(E) at the end of a
+// call.  The l-space wavepacket stays on the device between calls.
+#include <cuda_runtime.h>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "qd.h"
+#include "qd_kernels.h"
+#include "qd_tc.h"
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<int64_t> g_launches{0};
+
+int set_err(int code, const char *fmt, ...)
+{
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CU(x)                                                                           \
+  do {                                                                                  \
+    cudaError_t e_ = (x);                                                               \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(QD_ERR_CUDA, "%s failed: %s (%s:%d)", #x, cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                               \
+  } while (0)
+
+#define TRY(x)                  \
+  do {                          \
+    int rc_ = (x);              \
+    if (rc_ != QD_OK) return rc_; \
+  } while (0)
+
+constexpr int QD_RING = 100;   // steps per E-accumulation chunk
+
+bool radix_plan(int n, FftPlan &pl)
+{
+  pl.n = n;
+  pl.nst = 0;
+  int m = n;
+  const int pref[] = {8, 4, 2, 3, 5};
+  while (m > 1) {
+    bool found = false;
+    for (int r : pref) {
+      if (m % r == 0) {
+        if (pl.nst >= 16) return false;
+        pl.rad[pl.nst++] = r;
+        m /= r;
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  return true;
+}
+
+// Momentum grid by the repeated additions of get_momentum_for_fftw
+// (fftwinterface.C:110-125) and p^2/(2m), 1/(2 m r^2) (MatlabStructures.C:17-36).
+void radial_tables(const qd_radial &c, std::vector<double> &T, std::vector<double> &I)
+{
+  const int n = c.n;
+  T.assign(n, 0.0);
+  I.assign(n, 0.0);
+  const double xl = n * c.dr;
+  const double two_pi_xl = 2.0 * M_PI / xl;
+  const int half = n / 2;
+  double p1 = 0;
+  for (int i = 0; i <= half; i++) { T[i] = p1; p1 += two_pi_xl; }
+  p1 = two_pi_xl * (-half + 1);
+  for (int i = half + 1; i < n; i++) { T[i] = p1; p1 += two_pi_xl; }
+  for (int i = 0; i < n; i++) T[i] = T[i] * T[i] / (2 * c.mass);
+  const double m2 = c.mass + c.mass;
+  for (int i = 0; i < n; i++) I[i] = 1.0 / (m2 * c.r[i] * c.r[i]);
+}
+
+bool all_finite(const double *a, size_t n)
+{
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+struct qd_handle {
+  qd_data *data = nullptr;
+  int prec = QD_PREC_FP64;
+  int n1 = 0, n2 = 0, nth = 0, nl = 0;
+  long n12 = 0;
+  int npts = 0, h = 0, surf_j0 = 0, ne = 0;
+  bool do_crp = false, have_dump = false;
+  double dt = 0;
+  cudaStream_t st = nullptr;
+  std::vector<void *> allocs;
+
+  double *d_pot = nullptr, *d_w = nullptr, *d_leg = nullptr, *d_P = nullptr, *d_WP = nullptr;
+  float *d_P32 = nullptr, *d_WP32 = nullptr;
+  double *d_I1 = nullptr, *d_I2 = nullptr, *d_T1 = nullptr, *d_T2 = nullptr;
+  double *d_d1 = nullptr, *d_d2 = nullptr;
+  double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
+  float *d_vturn = nullptr, *d_rt1 = nullptr, *d_rt2 = nullptr, *d_kt1 = nullptr, *d_kt2 = nullptr;
+  double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
+  float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
+  void *d_lpsi = nullptr;
+  double2 *d_psi_z = nullptr;
+  void *d_surf = nullptr;
+  double2 *d_ring_psi = nullptr, *d_ring_g = nullptr, *d_fai = nullptr, *d_dfai = nullptr;
+  double *d_energies = nullptr, *d_eta = nullptr, *d_crp = nullptr;
+  double *d_norms = nullptr;
+  int norms_cap = 0;
+  TcPlan tc;                      // tensor-core column pass (FP32), if usable
+  bool use_tc = false;
+
+  FftPlan pl1, pl2;
+  int ring_fill = 0;
+  long acc_done = 0;
+  bool started = false;           // l-space state valid on the device
+  bool last_finalized = true;     // flux/norm of the last step already taken
+  int32_t steps = 0;
+  std::vector<double> norms_host;
+  bool profiling = false;
+  std::vector<double> kernel_ms;
+  void *d_flush = nullptr;        // L2 flush buffer of qd_propagate_timed
+  size_t flush_bytes = 0;
+  std::vector<cudaEvent_t> events;
+  std::vector<cudaEvent_t> prof_pool;
+  std::vector<int> prof_cls;
+  size_t prof_used = 0;
+
+  template <typename T> int alloc(T *&p, size_t count)
+  {
+    void *q = nullptr;
+    const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(QD_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes,
+                     cudaGetErrorString(e));
+    }
+    allocs.push_back(q);
+    p = reinterpret_cast<T *>(q);
+    return QD_OK;
+  }
+  ~qd_handle()
+  {
+    if (st) cudaStreamSynchronize(st);
+    for (void *p : allocs) cudaFree(p);
+    if (d_norms) cudaFree(d_norms);
+    if (d_flush) cudaFree(d_flush);
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+    for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
+    tc_plan_destroy(tc);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+int validate(const qd_data *d)
+{
+  if (!d) return set_err(QD_ERR_INVALID, "data is NULL");
+  const int n1 = d->r1.n, n2 = d->r2.n, nth = d->theta.n, m = d->theta.m;
+  if (n1 < 2 || n2 < 2 || n1 % 2 || n2 % 2)
+    return set_err(QD_ERR_INVALID, "r1.n (%d) and r2.n (%d) must be even and >= 2 "
+                   "(get_momentum_for_fftw requires even n)", n1, n2);
+  if (nth < 1 || m < 0) return set_err(QD_ERR_INVALID, "theta.n = %d, theta.m = %d", nth, m);
+  if (!d->r1.r || !d->r2.r || !d->theta.x || !d->theta.w || !d->theta.legendre || !d->pot ||
+      !d->psi)
+    return set_err(QD_ERR_INVALID, "a required array (r, theta.x/w/legendre, pot, psi) is NULL");
+  if (!(d->r1.dr > 0) || !(d->r2.dr > 0) || !(d->r1.mass > 0) || !(d->r2.mass > 0))
+    return set_err(QD_ERR_INVALID, "dr and mass must be positive");
+  if (!std::isfinite(d->time.time_step) || d->time.total_steps < 0 || d->time.steps < 0)
+    return set_err(QD_ERR_INVALID, "bad time struct");
+  for (int i = 0; i < n1; i++)
+    if (d->r1.r[i] == 0.0) return set_err(QD_ERR_INVALID, "r1.r contains 0");
+  for (int i = 0; i < n2; i++)
+    if (d->r2.r[i] == 0.0) return set_err(QD_ERR_INVALID, "r2.r contains 0");
+  FftPlan pl;
+  if (!radix_plan(n1, pl) || !radix_plan(n2, pl))
+    return set_err(QD_ERR_UNSUPPORTED, "r1.n = %d, r2.n = %d: FFT sizes must be 2^a 3^b 5^c",
+                   n1, n2);
+  if (d->options.precision != QD_PREC_FP64 && d->options.precision != QD_PREC_FP32)
+    return set_err(QD_ERR_INVALID, "options.precision = %d", d->options.precision);
+  const size_t npt = (size_t)n1 * n2 * nth;
+  if (!all_finite(d->pot, npt)) return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
+  if (!all_finite(d->psi, 2 * npt)) return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
+  if (d->CRP.calculate_CRP) {
+    const qd_crp &c = d->CRP;
+    if (c.n_energies < 1 || !c.energies || !c.eta_sq || !c.CRP)
+      return set_err(QD_ERR_INVALID, "CRP: n_energies/energies/eta_sq/CRP");
+    const int np = c.n_gradient_points;
+    if (np != 3 && np != 5 && np != 7 && np != 9 && np != 11)
+      return set_err(QD_ERR_INVALID, "NPoints error: n_gradient_points = %d (3,5,7,9,11)", np);
+    const int hh = (np - 1) / 2, j = c.n_dividing_surface - 1;
+    if (j - hh < 0 || j + hh > n2 - 1)
+      return set_err(QD_ERR_INVALID,
+                     "dividing surface %d with %d points reaches outside r2 (1..%d)",
+                     c.n_dividing_surface, np, n2);
+  }
+  return QD_OK;
+}
+
+// Kernel-class profiling (qd_set_profiling): an event after each launch
+// group; the span since the previous event is charged to that group.
+enum { PROF_COLUMN = 0, PROF_LINES = 1, PROF_FLUX = 2, PROF_ACCUM = 3, PROF_CRP = 4, PROF_N = 5 };
+
+int prof_mark(qd_handle *h, int cls)
+{
+  if (!h->profiling) return QD_OK;
+  if (h->prof_used == h->prof_pool.size()) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    h->prof_pool.push_back(e);
+  }
+  cudaEvent_t e = h->prof_pool[h->prof_used++];
+  CU(cudaEventRecord(e, h->st));
+  h->prof_cls.push_back(cls);
+  return QD_OK;
+}
+
+// After a stream sync: fold the recorded spans into per-class averages.
+int prof_collect(qd_handle *h)
+{
+  if (!h->profiling) return QD_OK;
+  double tot[PROF_N] = {0};
+  int cnt[PROF_N] = {0};
+  for (size_t i = 1; i < h->prof_used; i++) {
+    const int c = h->prof_cls[i];
+    if (c < 0) continue;
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, h->prof_pool[i - 1], h->prof_pool[i]));
+    tot[c] += ms;
+    cnt[c]++;
+  }
+  h->kernel_ms.assign(2 * PROF_N, 0.0);
+  for (int c = 0; c < PROF_N; c++) {
+    h->kernel_ms[c] = cnt[c] ? tot[c] / cnt[c] : 0.0;
+    h->kernel_ms[PROF_N + c] = cnt[c];
+  }
+  h->prof_used = 0;
+  h->prof_cls.clear();
+  return QD_OK;
+}
+
+template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double *norm_out,
+                                       bool out_z)
+{
+  ColumnParams p{};
+  p.n1 = h->n1; p.n2 = h->n2; p.nth = h->nth; p.nl = h->nl; p.n12 = h->n12;
+  p.lpsi = h->d_lpsi; p.psi_z = h->d_psi_z;
+  p.P = h->d_P; p.WP = h->d_WP; p.P32 = h->d_P32; p.WP32 = h->d_WP32;
+  p.expV = h->d_expV; p.vturn = h->d_vturn; p.pot = h->d_pot; p.dt = h->dt;
+  p.prestep = (mode == COL_HEAD && h->steps == 0);
+  p.d1 = h->have_dump ? h->d_d1 : nullptr;
+  p.d2 = h->have_dump ? h->d_d2 : nullptr;
+  p.do_flux = flux ? 1 : 0;
+  p.surf = h->d_surf; p.surf_j0 = h->surf_j0; p.surf_nrows = 2 * h->h + 1;
+  p.w = h->d_w; p.norm_out = norm_out; p.out_z = out_z ? 1 : 0;
+  cudaError_t e;
+  TRY(prof_mark(h, -1));
+  if (sizeof(R) == 4 && h->use_tc) e = launch_column_tc(h->tc, p, mode, h->st);
+  else e = launch_column<R>(p, mode, h->st);
+  g_launches++;
+  CU(e);
+  TRY(prof_mark(h, PROF_COLUMN));
+  if (flux) {
+    FluxParams f{};
+    f.n1 = h->n1; f.nth = h->nth; f.npts = h->npts; f.h = h->h; f.surf = h->d_surf;
+    static const int den[] = {0, 2, 12, 60, 840, 2520};
+    f.den_dx = den[h->h] * h->data->r2.dr;
+    f.ring_psi = h->d_ring_psi; f.ring_g = h->d_ring_g; f.slot = h->ring_fill;
+    CU(launch_flux_prep<R>(f, h->st));
+    g_launches++;
+    TRY(prof_mark(h, PROF_FLUX));
+    h->ring_fill++;
+    if (h->ring_fill == QD_RING) {
+      AccumParams a{};
+      a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+      a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
+      a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+      CU(launch_flux_accum(a, h->st));
+      g_launches++;
+      TRY(prof_mark(h, PROF_ACCUM));
+      h->acc_done += h->ring_fill;
+      h->ring_fill = 0;
+    }
+  }
+  return QD_OK;
+}
+
+template <typename R> int issue_lines(qd_handle *h)
+{
+  LineParams p{};
+  p.n1 = h->n1; p.n2 = h->n2; p.nl = h->nl; p.n12 = h->n12; p.lpsi = h->d_lpsi;
+  p.rot = h->d_rot; p.kin = h->d_kin;
+  p.rt1 = h->d_rt1; p.rt2 = h->d_rt2; p.kt1 = h->d_kt1; p.kt2 = h->d_kt2;
+  p.kscale = (float)(1.0 / ((double)h->n1 * h->n2));
+  if (sizeof(R) == 8) { p.tw1 = h->d_tw1_64; p.tw2 = h->d_tw2_64; }
+  else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
+  p.pl1 = h->pl1; p.pl2 = h->pl2;
+  TRY(prof_mark(h, -1));
+  CU(launch_lines<R>(p, h->st));
+  g_launches += lines_launches_per_step(h->n1, h->n2, h->prec);
+  TRY(prof_mark(h, PROF_LINES));
+  return QD_OK;
+}
+
+int flush_accum(qd_handle *h)
+{
+  if (h->ring_fill == 0) return QD_OK;
+  AccumParams a{};
+  a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+  a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
+  a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+  CU(launch_flux_accum(a, h->st));
+  g_launches++;
+  h->acc_done += h->ring_fill;
+  h->ring_fill = 0;
+  return QD_OK;
+}
+
+int compute_crp(qd_handle *h)
+{
+  if (!h->do_crp) return QD_OK;
+  TRY(flush_accum(h));
+  CrpParams c{};
+  c.n1 = h->n1; c.nth = h->nth; c.ne = h->ne; c.w = h->d_w; c.eta_sq = h->d_eta;
+  c.dr1_mu2 = h->data->r1.dr / h->data->r2.mass;
+  c.fai = h->d_fai; c.dfai = h->d_dfai; c.crp = h->d_crp;
+  TRY(prof_mark(h, -1));
+  CU(launch_crp(c, h->st));
+  g_launches++;
+  TRY(prof_mark(h, PROF_CRP));
+  return QD_OK;
+}
+
+template <typename R> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
+                                   double *device_ms = nullptr)
+{
+  if (n <= 0) {
+    if (device_ms) *device_ms = 0.0;
+    return QD_OK;
+  }
+  const bool timed = device_ms != nullptr;
+  if (timed) {
+    while (h->events.size() < (size_t)(2 * n + 2)) {
+      cudaEvent_t e;
+      CU(cudaEventCreate(&e));
+      h->events.push_back(e);
+    }
+    if (flush_bytes > h->flush_bytes) {
+      if (h->d_flush) cudaFree(h->d_flush);
+      h->d_flush = nullptr;
+      CU(cudaMalloc(&h->d_flush, flush_bytes));
+      h->flush_bytes = flush_bytes;
+    }
+  }
+  if (h->norms_cap < n) {
+    if (h->d_norms) cudaFree(h->d_norms);
+    h->d_norms = nullptr;
+    CU(cudaMalloc(&h->d_norms, sizeof(double) * n));
+    h->norms_cap = n;
+  }
+  CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n, h->st));
+  for (int s = 0; s < n; s++) {
+    if (timed && flush_bytes) CU(cudaMemsetAsync(h->d_flush, s & 0xff, flush_bytes, h->st));
+    if (timed) CU(cudaEventRecord(h->events[2 * s], h->st));
+    if (!h->started) {
+      TRY(issue_column<R>(h, COL_HEAD, false, nullptr, false));
+      h->started = true;
+    } else if (s == 0 && h->last_finalized) {
+      TRY(issue_column<R>(h, COL_MID, false, nullptr, false));
+    } else {
+      TRY(issue_column<R>(h, COL_MID, h->do_crp, h->d_norms + (s - 1), false));
+    }
+    TRY(issue_lines<R>(h));
+    h->steps++;
+    if (timed && s < n - 1) CU(cudaEventRecord(h->events[2 * s + 1], h->st));
+  }
+  TRY(issue_column<R>(h, COL_TAIL, h->do_crp, h->d_norms + (n - 1), false));
+  h->last_finalized = true;
+  TRY(compute_crp(h));
+  if (timed) CU(cudaEventRecord(h->events[2 * n - 1], h->st));
+  std::vector<double> nb(n);
+  CU(cudaMemcpyAsync(nb.data(), h->d_norms, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  TRY(prof_collect(h));
+  if (timed) {
+    double tot = 0.0;
+    for (int s = 0; s < n; s++) {
+      float ms = 0.f;
+      CU(cudaEventElapsedTime(&ms, h->events[2 * s], h->events[2 * s + 1]));
+      tot += ms;
+    }
+    *device_ms = tot;
+  }
+  const double scale = h->data->r1.dr * h->data->r2.dr;
+  for (int s = 0; s < n; s++) {
+    const double v = nb[s] * scale;
+    if (!std::isfinite(v))
+      return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d", h->steps - n + s + 1);
+    h->norms_host.push_back(v);
+  }
+  return QD_OK;
+}
+
+template <typename T>
+int upload(qd_handle *h, T *&dst, const T *src, size_t count)
+{
+  TRY(h->alloc(dst, count));
+  CU(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, h->st));
+  return QD_OK;
+}
+
+int create(const qd_data *d, qd_handle **out)
+{
+  TRY(validate(d));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_err(QD_ERR_CUDA, "no CUDA device visible: the propagator has no CPU path");
+  }
+  qd_handle *h = new qd_handle();
+  *out = h;
+  h->data = const_cast<qd_data *>(d);
+  h->prec = d->options.precision;
+  h->n1 = d->r1.n; h->n2 = d->r2.n; h->nth = d->theta.n; h->nl = d->theta.m + 1;
+  h->n12 = (long)h->n1 * h->n2;
+  h->dt = d->time.time_step;
+  h->steps = d->time.steps;
+  h->have_dump = d->dump1.dump && d->dump2.dump;
+  h->do_crp = d->CRP.calculate_CRP != 0;
+  if (h->do_crp) {
+    h->npts = d->CRP.n_gradient_points;
+    h->h = (h->npts - 1) / 2;
+    h->surf_j0 = d->CRP.n_dividing_surface - 1 - h->h;
+    h->ne = d->CRP.n_energies;
+  }
+  radix_plan(h->n1, h->pl1);
+  radix_plan(h->n2, h->pl2);
+  CU(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+
+  const long npt = h->n12 * h->nth;
+  const bool f64 = h->prec == QD_PREC_FP64;
+  TRY(upload(h, h->d_pot, d->pot, npt));
+  TRY(upload(h, h->d_w, d->theta.w, h->nth));
+  TRY(upload(h, h->d_leg, d->theta.legendre, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_P, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_WP, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_P32, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_WP32, (size_t)h->nth * h->nl));
+  std::vector<double> T1, I1, T2, I2;
+  radial_tables(d->r1, T1, I1);
+  radial_tables(d->r2, T2, I2);
+  TRY(upload(h, h->d_T1, T1.data(), h->n1));
+  TRY(upload(h, h->d_I1, I1.data(), h->n1));
+  TRY(upload(h, h->d_T2, T2.data(), h->n2));
+  TRY(upload(h, h->d_I2, I2.data(), h->n2));
+  if (h->have_dump) {
+    TRY(upload(h, h->d_d1, d->dump1.dump, h->n1));
+    TRY(upload(h, h->d_d2, d->dump2.dump, h->n2));
+  }
+  // FFT roots exp(-2 pi i k/n) in long double
+  for (int dim = 0; dim < 2; dim++) {
+    const int n = dim == 0 ? h->n1 : h->n2;
+    std::vector<double2> z(n);
+    std::vector<float2> f(n);
+    for (int k = 0; k < n; k++) {
+      const long double a = -2.0L * 3.141592653589793238462643383279502884L * k / n;
+      z[k] = make_double2((double)cosl(a), (double)sinl(a));
+      f[k] = make_float2((float)cosl(a), (float)sinl(a));
+    }
+    TRY(upload(h, dim == 0 ? h->d_tw1_64 : h->d_tw2_64, z.data(), n));
+    TRY(upload(h, dim == 0 ? h->d_tw1_32 : h->d_tw2_32, f.data(), n));
+  }
+  CU(launch_legendre_matrices(h->nth, h->nl, nullptr, h->d_w, h->d_leg, h->d_P, h->d_WP,
+                              h->d_P32, h->d_WP32, h->st));
+  g_launches++;
+  if (f64) {
+    TRY(h->alloc(h->d_expV, npt));
+    TRY(h->alloc(h->d_rot, (size_t)h->n12 * h->nl));
+    TRY(h->alloc(h->d_kin, h->n12));
+    CU(launch_setup_tables_fp64(h->n1, h->n2, h->nth, h->nl, h->dt, h->d_pot, h->d_I1,
+                                h->d_I2, h->d_T1, h->d_T2, h->d_expV, h->d_rot, h->d_kin,
+                                h->st));
+  } else {
+    TRY(h->alloc(h->d_vturn, npt));
+    TRY(h->alloc(h->d_rt1, (size_t)h->nl * h->n1));
+    TRY(h->alloc(h->d_rt2, (size_t)h->nl * h->n2));
+    TRY(h->alloc(h->d_kt1, h->n1));
+    TRY(h->alloc(h->d_kt2, h->n2));
+    CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth, h->nl, h->dt, h->d_pot, h->d_I1,
+                                h->d_I2, h->d_T1, h->d_T2, h->d_vturn, h->d_rt1, h->d_rt2,
+                                h->d_kt1, h->d_kt2, h->st));
+  }
+  g_launches++;
+  const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
+  void *lp = nullptr;
+  {
+    unsigned char *b = nullptr;
+    TRY(h->alloc(b, csz * h->n12 * h->nl));
+    lp = b;
+  }
+  h->d_lpsi = lp;
+  TRY(upload(h, h->d_psi_z, reinterpret_cast<const double2 *>(d->psi), npt));
+  if (h->do_crp) {
+    const size_t nq = (size_t)h->nth * h->n1;
+    unsigned char *b = nullptr;
+    TRY(h->alloc(b, csz * nq * (2 * h->h + 1)));
+    h->d_surf = b;
+    TRY(h->alloc(h->d_ring_psi, nq * QD_RING));
+    TRY(h->alloc(h->d_ring_g, nq * QD_RING));
+    TRY(h->alloc(h->d_fai, nq * h->ne));
+    TRY(h->alloc(h->d_dfai, nq * h->ne));
+    CU(cudaMemsetAsync(h->d_fai, 0, sizeof(double2) * nq * h->ne, h->st));
+    CU(cudaMemsetAsync(h->d_dfai, 0, sizeof(double2) * nq * h->ne, h->st));
+    TRY(upload(h, h->d_energies, d->CRP.energies, h->ne));
+    TRY(upload(h, h->d_eta, d->CRP.eta_sq, h->ne));
+    TRY(h->alloc(h->d_crp, h->ne));
+  }
+  if (!f64) {
+    int rc = tc_plan_create(h->tc, h->nth, h->nl, h->d_P, h->d_WP, h->st);
+    if (rc == QD_OK) h->use_tc = true;
+    else if (rc != QD_ERR_UNSUPPORTED) return rc;
+  }
+  CU(cudaStreamSynchronize(h->st));
+  return QD_OK;
+}
+
+int get_psi(qd_handle *h, double *psi_out)
+{
+  const long npt = h->n12 * h->nth;
+  if (h->started) {
+    if (h->prec == QD_PREC_FP64) TRY(issue_column<double>(h, COL_TAIL, false, nullptr, true));
+    else TRY(issue_column<float>(h, COL_TAIL, false, nullptr, true));
+  }
+  CU(cudaMemcpyAsync(psi_out, h->d_psi_z, sizeof(double2) * npt, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return QD_OK;
+}
+
+int get_crp(qd_handle *h, double *crp_out)
+{
+  if (!h->do_crp) return set_err(QD_ERR_INVALID, "CRP.calculate_CRP is 0");
+  if (!h->started) {
+    for (int e = 0; e < h->ne; e++) crp_out[e] = 0.0;
+    return QD_OK;
+  }
+  TRY(compute_crp(h));
+  CU(cudaMemcpyAsync(crp_out, h->d_crp, sizeof(double) * h->ne, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return QD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qd_abi_version(void) { return QD_ABI_VERSION; }
+const char *qd_last_error(void) { return g_err.c_str(); }
+int64_t qd_kernel_launch_count(void) { return g_launches.load(); }
+
+int qd_set_device(int32_t device)
+{
+  CU(cudaSetDevice(device));
+  return QD_OK;
+}
+
+int qd_create(const qd_data *data, qd_handle **out)
+{
+  if (!out) return set_err(QD_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  qd_handle *h = nullptr;
+  int rc = create(data, &h);
+  if (rc != QD_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return QD_OK;
+}
+
+int qd_destroy(qd_handle *h)
+{
+  delete h;
+  return QD_OK;
+}
+
+int qd_propagate(qd_handle *h, int32_t n_steps)
+{
+  if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
+  if (n_steps < 0) return set_err(QD_ERR_INVALID, "n_steps < 0");
+  if (h->prec == QD_PREC_FP64) return propagate<double>(h, n_steps);
+  return propagate<float>(h, n_steps);
+}
+
+int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes, double *device_ms)
+{
+  if (!h || !device_ms) return set_err(QD_ERR_INVALID, "NULL argument");
+  if (n_steps < 0 || flush_bytes < 0) return set_err(QD_ERR_INVALID, "negative argument");
+  if (h->prec == QD_PREC_FP64) return propagate<double>(h, n_steps, (size_t)flush_bytes, device_ms);
+  return propagate<float>(h, n_steps, (size_t)flush_bytes, device_ms);
+}
+
+int qd_get_psi(qd_handle *h, double *psi_out)
+{
+  if (!h || !psi_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  return get_psi(h, psi_out);
+}
+
+int qd_get_crp(qd_handle *h, double *crp_out)
+{
+  if (!h || !crp_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  return get_crp(h, crp_out);
+}
+
+int qd_download(qd_handle *h)
+{
+  if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
+  TRY(get_psi(h, h->data->psi));
+  if (h->do_crp && h->started) TRY(get_crp(h, h->data->CRP.CRP));
+  h->data->time.steps = h->steps;
+  return QD_OK;
+}
+
+int qd_get_norms(qd_handle *h, double *norms_out, int32_t n)
+{
+  if (!h || !norms_out || n < 0) return set_err(QD_ERR_INVALID, "bad argument");
+  if ((size_t)n > h->norms_host.size())
+    return set_err(QD_ERR_INVALID, "%d norms requested, %zu available", n, h->norms_host.size());
+  std::memcpy(norms_out, h->norms_host.data() + (h->norms_host.size() - n), sizeof(double) * n);
+  return QD_OK;
+}
+
+int qd_steps(qd_handle *h, int32_t *steps_out)
+{
+  if (!h || !steps_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  *steps_out = h->steps;
+  return QD_OK;
+}
+
+int qd_set_profiling(qd_handle *h, int32_t on)
+{
+  if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
+  h->profiling = on != 0;
+  return QD_OK;
+}
+
+int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written)
+{
+  if (!h || !n_written) return set_err(QD_ERR_INVALID, "NULL argument");
+  int32_t k = 0;
+  for (; k < n && k < (int32_t)h->kernel_ms.size(); k++) ms_out[k] = h->kernel_ms[k];
+  *n_written = k;
+  return QD_OK;
+}
+
+int qd_energies(qd_handle *h, double out4[4])
+{
+  if (!h || !out4) return set_err(QD_ERR_INVALID, "NULL argument");
+  return set_err(QD_ERR_UNSUPPORTED, "qd_energies: not available in this build");
+}
+
+int qd_checkpoint(qd_handle *h, const char *path)
+{
+  if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
+  return set_err(QD_ERR_UNSUPPORTED, "qd_checkpoint: not available in this build");
+}
+
+int qd_restore(qd_handle *h, const char *path)
+{
+  if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
+  return set_err(QD_ERR_UNSUPPORTED, "qd_restore: not available in this build");
+}
+
+int qd_time_evolution(qd_data *data)
+{
+  qd_handle *h = nullptr;
+  TRY(qd_create(data, &h));
+  int rc = qd_propagate(h, data->time.total_steps);
+  if (rc == QD_OK) rc = qd_download(h);
+  qd_destroy(h);
+  return rc;
+}
+
+int qd_read_grids(const char *dir, int32_t n, double *x, double *w)
+{
+  if (!dir || !x || !w) return set_err(QD_ERR_INVALID, "NULL argument");
+  if (n < 1 || n > 599) return set_err(QD_ERR_INVALID, "argument should be 1 <= n <= 599");
+  std::string path = std::string(dir) + "/" + std::to_string(n) + "-LegendreGauss.grids";
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return set_err(QD_ERR_IO, "\"%s\" does not exist", path.c_str());
+  std::vector<double> xs, ws;
+  double a, b;
+  while (fscanf(f, "%lf %lf", &a, &b) == 2) { xs.push_back(a); ws.push_back(b); }
+  fclose(f);
+  const int nh = (int)xs.size();
+  if (n != 2 * nh - (n % 2))
+    return set_err(QD_ERR_IO, "%s: %d lines do not describe n = %d", path.c_str(), nh, n);
+  // mirror the non-negative half (GaussLegendre2.m:19-25)
+  int o = 0;
+  const int start = (n % 2) ? nh - 1 : nh - 1;
+  for (int i = start; i >= ((n % 2) ? 1 : 0); i--) { x[o] = -xs[i]; w[o] = ws[i]; o++; }
+  for (int i = 0; i < nh; i++) { x[o] = xs[i]; w[o] = ws[i]; o++; }
+  return QD_OK;
+}
+
+int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre)
+{
+  if (!x || !legendre || n < 1 || m < 0) return set_err(QD_ERR_INVALID, "bad argument");
+  double *dx = nullptr, *dl = nullptr;
+  CU(cudaMalloc(&dx, sizeof(double) * n));
+  cudaError_t e = cudaMalloc(&dl, sizeof(double) * (size_t)n * (m + 1));
+  if (e != cudaSuccess) { cudaFree(dx); CU(e); }
+  int rc = QD_OK;
+  if (cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+      launch_legendre_p2(n, m, dx, dl, 0) != cudaSuccess ||
+      cudaMemcpy(legendre, dl, sizeof(double) * (size_t)n * (m + 1), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    rc = set_err(QD_ERR_CUDA, "qd_legendre_matrix: %s", cudaGetErrorString(cudaGetLastError()));
+  g_launches++;
+  cudaFree(dx);
+  cudaFree(dl);
+  return rc;
+}
+
+}  // extern "C"

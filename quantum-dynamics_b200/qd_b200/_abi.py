@@ -156,10 +156,12 @@ def lib():
         "qd_abi_version": (C.c_int, []),
         "qd_last_error": (C.c_char_p, []),
         "qd_kernel_launch_count": (C.c_int64, []),
+        "qd_set_device": (C.c_int, [C.c_int32]),
         "qd_time_evolution": (C.c_int, [P(QdData)]),
         "qd_create": (C.c_int, [P(QdData), P(H)]),
         "qd_destroy": (C.c_int, [H]),
         "qd_propagate": (C.c_int, [H, C.c_int32]),
+        "qd_propagate_timed": (C.c_int, [H, C.c_int32, C.c_int64, c_double_p]),
         "qd_get_psi": (C.c_int, [H, c_double_p]),
         "qd_get_crp": (C.c_int, [H, c_double_p]),
         "qd_download": (C.c_int, [H]),

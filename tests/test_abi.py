@@ -1,0 +1,90 @@
+"""The C-ABI library: loads, exports every entry point of include/qd.h,
+validates its input the way the reference's insist() checks do, and refuses
+to run without a GPU (there is no CPU path).  No compute runs here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO, GOLDEN, have_gpu
+from qd_b200 import _abi, systems as S
+from qd_b200.timeevolution import TimeEvolutionMexCUDA
+
+
+def header_functions():
+    src = open(os.path.join(REPO, "include", "qd.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(qd_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(qdlib):
+    names = header_functions()
+    assert len(names) >= 19
+    for n in names:
+        assert hasattr(qdlib, n), n
+    assert qdlib.qd_abi_version() == 1
+
+
+def test_read_grids_matches_python_reader(qdlib):
+    from qd_b200.timeevolution import read_grids
+    for n in (8, 41, 64):
+        x, w = read_grids(os.path.join(GOLDEN, "grids"), n)
+        xs, ws = S.read_grids(os.path.join(GOLDEN, "grids"), n)
+        assert np.array_equal(x, xs) and np.array_equal(w, ws)
+    x = np.empty(5); w = np.empty(5)
+    rc = qdlib.qd_read_grids(b"/nonexistent", 5, x.ctypes.data_as(_abi.c_double_p),
+                             w.ctypes.data_as(_abi.c_double_p))
+    assert rc == _abi.QD_ERR_IO and b"does not exist" in qdlib.qd_last_error()
+
+
+def _small():
+    return S.build_case("h+h2", 16, 12, 8, m=6, total_steps=3, n_energies=5,
+                        n_gradient_points=5)
+
+
+@pytest.mark.parametrize("mutate,code,msg", [
+    (lambda d: setattr(d.r1, "n", 15), _abi.QD_ERR_INVALID, b"even"),
+    (lambda d: setattr(d.CRP, "n_gradient_points", 4), _abi.QD_ERR_INVALID, b"NPoints"),
+    (lambda d: setattr(d.CRP, "n_dividing_surface", 1), _abi.QD_ERR_INVALID, b"dividing surface"),
+    (lambda d: setattr(d.CRP, "n_dividing_surface", 12), _abi.QD_ERR_INVALID, b"dividing surface"),
+    (lambda d: d.pot.__setitem__((0, 0, 0), np.nan), _abi.QD_ERR_NONFINITE, b"pot"),
+    (lambda d: d.psi.__setitem__((1, 1, 1), np.inf), _abi.QD_ERR_NONFINITE, b"psi"),
+    (lambda d: setattr(d.options, "precision", 7), _abi.QD_ERR_INVALID, b"precision"),
+])
+def test_invalid_input_rejected_before_device_work(qdlib, mutate, code, msg):
+    d = _small()
+    mutate(d)
+    c = _abi.to_c(d)
+    if d.r1.n == 15:
+        c.r1.n = 15
+    h = C.c_void_p()
+    rc = qdlib.qd_create(C.byref(c), C.byref(h))
+    assert rc == code
+    assert msg in qdlib.qd_last_error()
+    assert not h.value
+
+
+def test_unsupported_fft_size(qdlib):
+    d = S.build_case("h+h2", 14, 12, 8, m=6, total_steps=1, n_energies=5, n_gradient_points=5)
+    c = _abi.to_c(d)
+    h = C.c_void_p()
+    assert qdlib.qd_create(C.byref(c), C.byref(h)) == _abi.QD_ERR_UNSUPPORTED
+
+
+@pytest.mark.skipif(have_gpu(), reason="checks the no-GPU behaviour")
+def test_fails_loudly_without_gpu(qdlib):
+    d = _small()
+    with pytest.raises(_abi.QdError) as e:
+        TimeEvolutionMexCUDA(d)
+    assert e.value.code == _abi.QD_ERR_CUDA
+    assert "no CPU path" in str(e.value)
+
+
+def test_struct_layout_matches_header():
+    # sizes of the ctypes mirror equal the C struct sizes on x86-64
+    assert C.sizeof(_abi.QdRadial) == 56
+    assert C.sizeof(_abi.QdAngle) == 32
+    assert C.sizeof(_abi.QdTime) == 24
+    assert C.sizeof(_abi.QdCrp) == 40

@@ -1,0 +1,129 @@
+"""GPU propagation through the C ABI against the CPU oracle (which is pinned
+bit-exactly to the reference's own common/timeEvol.C).
+
+Tolerances (north_star): FP64 plain form -- wavepacket norm 1e-10 relative,
+P(E) 1e-8 absolute; complex64 form -- |dP(E)| <= 1e-3 over energies where
+eta^2 > 1e-3 max eta^2, norm 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, golden_case
+from oracle import pyoracle as O
+from qd_b200 import systems as S, QD_PREC_FP32, QD_PREC_FP64
+from qd_b200.timeevolution import TimeEvolutionMexCUDA, Propagator
+
+pytestmark = pytest.mark.gpu
+
+FP64_PSI_REL = 1e-10
+FP64_CRP_ABS = 1e-8
+FP32_CRP_ABS = 1e-3
+
+
+def norm(data, psi):
+    w = data.theta.w
+    return float(np.sum(w[:, None, None] * np.abs(psi) ** 2) * data.r1.dr * data.r2.dr)
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_fp64_matches_reference_outputs(name):
+    data, exp = golden_case(name)
+    TimeEvolutionMexCUDA(data)
+    assert data.time.steps == exp["steps"]
+    assert rel(data.psi, exp["psi"]) < FP64_PSI_REL
+    assert np.abs(data.CRP.CRP - exp["crp"]).max() < FP64_CRP_ABS
+
+
+CASES = [
+    # (system, n1, n2, nth, m, steps, npts, extra)
+    ("h+h2", 64, 64, 40, 38, 60, 11, {}),
+    ("f+h2", 48, 40, 24, 20, 40, 7, {}),            # 48 = 16*3, 40 = 8*5
+    ("h+h2", 12, 10, 6, 5, 30, 3, {}),               # tiny odd-radix grid
+    ("f+h2", 32, 96, 16, 15, 25, 9, dict(r=(0.5, 9.0))),  # radix-3 in r
+    ("h+h2", 32, 24, 10, 12, 20, 5, {}),             # n_l > n_theta
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{c[1]}x{c[2]}x{c[3]}-m{c[4]}")
+def test_fp64_matches_oracle(case):
+    system, n1, n2, nth, m, steps, npts, extra = case
+    base = S.build_case(system, n1, n2, nth, m=m, total_steps=steps, n_energies=17,
+                        n_gradient_points=npts, **extra)
+    a, b = S.copy_case(base), S.copy_case(base)
+    norms, _ = O.oracle_time_evolution(a, norms=True)
+    with Propagator(b) as p:
+        p.propagate(steps)
+        gnorms = p.norms(steps)
+        p.download()
+    assert b.time.steps == a.time.steps == steps
+    assert rel(b.psi, a.psi) < FP64_PSI_REL
+    assert np.abs(gnorms - norms).max() < FP64_PSI_REL * norms.max()
+    assert np.abs(b.CRP.CRP - a.CRP.CRP).max() < FP64_CRP_ABS
+
+
+def test_fp64_no_absorber_no_crp_and_resume():
+    base = S.build_case("h+h2", 32, 32, 16, m=15, total_steps=10, n_energies=5)
+    base.dump1.dump = None
+    base.CRP.calculate_CRP = 0
+    a, b = S.copy_case(base), S.copy_case(base)
+    O.oracle_time_evolution(a)
+    TimeEvolutionMexCUDA(b)
+    assert rel(b.psi, a.psi) < FP64_PSI_REL
+    assert np.all(b.CRP.CRP == 0)
+    # second call resumes from steps = 10 without the pre-step
+    O.oracle_time_evolution(a)
+    TimeEvolutionMexCUDA(b)
+    assert a.time.steps == b.time.steps == 20
+    assert rel(b.psi, a.psi) < FP64_PSI_REL
+
+
+def test_fp64_unitary_without_absorbers():
+    base = S.build_case("h+h2", 32, 32, 16, m=15, total_steps=50, n_energies=5)
+    base.dump1.dump = None
+    base.dump2.dump = None
+    with Propagator(base) as p:
+        p.propagate(50)
+        n = p.norms(50)
+    assert np.abs(n - n[0]).max() < 1e-12 * n[0]
+
+
+def test_handle_split_calls_equal_one_call():
+    base = S.build_case("f+h2", 32, 32, 16, m=15, total_steps=30, n_energies=9,
+                        n_gradient_points=5)
+    a, b = S.copy_case(base), S.copy_case(base)
+    O.oracle_time_evolution(a)
+    with Propagator(b) as p:
+        for n in (7, 1, 22):
+            p.propagate(n)
+        assert p.steps == 30
+        p.download()
+    assert rel(b.psi, a.psi) < FP64_PSI_REL
+    assert np.abs(b.CRP.CRP - a.CRP.CRP).max() < FP64_CRP_ABS
+
+
+def test_fp32_matches_oracle_within_budget():
+    base = S.build_case("f+h2", 64, 64, 32, m=31, total_steps=200, n_energies=41,
+                        n_gradient_points=11)
+    a, b = S.copy_case(base), S.copy_case(base)
+    b.options.precision = QD_PREC_FP32
+    norms, _ = O.oracle_time_evolution(a, norms=True)
+    with Propagator(b) as p:
+        p.propagate(200)
+        gn = p.norms(200)
+        p.download()
+    eta = base.CRP.eta_sq
+    sel = eta > 1e-3 * eta.max()
+    assert np.abs(b.CRP.CRP - a.CRP.CRP)[sel].max() < FP32_CRP_ABS
+    assert np.abs(gn - norms).max() < 1e-5 * norms.max()
+    assert rel(b.psi, a.psi) < 1e-4
+
+
+def test_legendre_matrix_on_gpu():
+    from qd_b200.timeevolution import legendre_matrix_gpu
+    x, _ = S.gauss_legendre(40)
+    P = legendre_matrix_gpu(40, 38, x)
+    assert np.abs(P - S.legendre_p2(38, x)).max() < 1e-14
