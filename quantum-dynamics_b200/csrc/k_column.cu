@@ -18,10 +18,14 @@ template <typename R> struct MatSel;
 template <> struct MatSel<double> {
   static __device__ __forceinline__ const double *P(const ColumnParams &p) { return p.P; }
   static __device__ __forceinline__ const double *WP(const ColumnParams &p) { return p.WP; }
+  static __device__ __forceinline__ const double *Plo(const ColumnParams &) { return nullptr; }
+  static __device__ __forceinline__ const double *WPlo(const ColumnParams &) { return nullptr; }
 };
 template <> struct MatSel<float> {
   static __device__ __forceinline__ const float *P(const ColumnParams &p) { return p.P32; }
   static __device__ __forceinline__ const float *WP(const ColumnParams &p) { return p.WP32; }
+  static __device__ __forceinline__ const float *Plo(const ColumnParams &p) { return p.P32lo; }
+  static __device__ __forceinline__ const float *WPlo(const ColumnParams &p) { return p.WP32lo; }
 };
 
 __device__ __forceinline__ double2 vphase(const ColumnParams &p, long g, double2)
@@ -29,10 +33,12 @@ __device__ __forceinline__ double2 vphase(const ColumnParams &p, long g, double2
 __device__ __forceinline__ float2 vphase(const ColumnParams &p, long g, float2)
 { return expi_turns(p.vturn[g]); }
 
-// out[o][t] = sum_c M[o*ldm + c] * in[c][t], o < nout, c < nin, KB outputs / thread
+// out[o][t] = sum_c M[o*ldm + c] * in[c][t], o < nout, c < nin, KB outputs / thread;
+// M = Mhi + Mlo when Mlo is given (float matrices carried to ~2^-48)
 template <typename R, typename C>
-__device__ __forceinline__ void contract(const R *__restrict__ M, int ldm, bool trans,
-                                         const C *in, int nin, C *out, int nout, int TP)
+__device__ __forceinline__ void contract(const R *__restrict__ M, const R *__restrict__ Mlo,
+                                         int ldm, bool trans, const C *in, int nin, C *out,
+                                         int nout, int TP)
 {
   const int ngroups = (nout + KB - 1) / KB;
   for (int e = threadIdx.x; e < ngroups * TP; e += blockDim.x) {
@@ -45,7 +51,13 @@ __device__ __forceinline__ void contract(const R *__restrict__ M, int ldm, bool 
 #pragma unroll
       for (int b = 0; b < KB; b++) {
         const int o = min(o0 + b, nout - 1);
-        const R m = trans ? __ldg(M + (long)c * ldm + o) : __ldg(M + (long)o * ldm + c);
+        const long mi = trans ? (long)c * ldm + o : (long)o * ldm + c;
+        const R m = __ldg(M + mi);
+        if (Mlo) {
+          const R ml = __ldg(Mlo + mi);
+          acc[b].x += ml * v.x;
+          acc[b].y += ml * v.y;
+        }
         acc[b].x += m * v.x;
         acc[b].y += m * v.y;
       }
@@ -100,7 +112,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
     }
     __syncthreads();
     // psi_theta(k) = sum_l P[k][l] psi_l(l)
-    contract<R, C>(P, p.nl, false, A, p.nl, B, p.nth, TP);
+    contract<R, C>(P, MatSel<R>::Plo(p), p.nl, false, A, p.nl, B, p.nth, TP);
   }
   __syncthreads();
 
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
   }
 
   // psi_l(l) = sum_k WP[k][l] psi_theta(k)
-  contract<R, C>(WP, p.nl, true, B, p.nth, A, p.nl, TP);
+  contract<R, C>(WP, MatSel<R>::WPlo(p), p.nl, true, B, p.nth, A, p.nl, TP);
   __syncthreads();
   for (int e = threadIdx.x; e < p.nl * TP; e += blockDim.x) {
     const int l = e / TP, t = e % TP;

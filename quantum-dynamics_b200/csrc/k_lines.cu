@@ -23,7 +23,7 @@ template <> struct Phase<float> {
   static __device__ __forceinline__ float2 rot(const LineParams &p, int l, int j, int i)
   { return expi_turns(p.rt1[l * p.n1 + i] + p.rt2[l * p.n2 + j]); }
   static __device__ __forceinline__ float2 kin(const LineParams &p, int j, int i)
-  { return cscale(expi_turns(p.kt1[i] + p.kt2[j]), p.kscale); }
+  { return cscale2(expi_turns(p.kt1[i] + p.kt2[j]), p.kscale, p.kscale_lo); }
 };
 
 // dir = -1: Rot then forward FFT along R;  dir = +1: inverse FFT then Rot.

@@ -80,7 +80,8 @@ __global__ void k_tables_fp32(int n1, int n2, int nth, int nl, double dt, const 
 }
 
 __global__ void k_legendre_matrices(int nth, int nl, const double *w, const double *legendre,
-                                    double *P, double *WP, float *P32, float *WP32)
+                                    double *P, double *WP, float *P32, float *WP32,
+                                    float *P32lo, float *WP32lo)
 {
   const int total = nth * nl;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
@@ -90,8 +91,12 @@ __global__ void k_legendre_matrices(int nth, int nl, const double *w, const doub
     const double wp = f * w[k] * p;
     P[g] = p;
     WP[g] = wp;
+    // float + float residual: the fixed rounding of a float-only matrix would
+    // make F*B = I + O(1e-7) and drift the norm systematically step by step
     P32[g] = (float)p;
     WP32[g] = (float)wp;
+    P32lo[g] = (float)(p - (double)(float)p);
+    WP32lo[g] = (float)(wp - (double)(float)wp);
   }
 }
 
@@ -138,10 +143,11 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
 
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *, const double *w,
                                      const double *legendre, double *P, double *WP,
-                                     float *P32, float *WP32, cudaStream_t s)
+                                     float *P32, float *WP32, float *P32lo, float *WP32lo,
+                                     cudaStream_t s)
 {
   k_legendre_matrices<<<(nth * nl + 255) / 256, 256, 0, s>>>(nth, nl, w, legendre, P, WP, P32,
-                                                             WP32);
+                                                             WP32, P32lo, WP32lo);
   return cudaGetLastError();
 }
 

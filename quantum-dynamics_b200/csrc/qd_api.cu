@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -115,7 +116,7 @@ struct qd_handle {
   std::vector<void *> allocs;
 
   double *d_pot = nullptr, *d_w = nullptr, *d_leg = nullptr, *d_P = nullptr, *d_WP = nullptr;
-  float *d_P32 = nullptr, *d_WP32 = nullptr;
+  float *d_P32 = nullptr, *d_WP32 = nullptr, *d_P32lo = nullptr, *d_WP32lo = nullptr;
   double *d_I1 = nullptr, *d_I2 = nullptr, *d_T1 = nullptr, *d_T2 = nullptr;
   double *d_d1 = nullptr, *d_d2 = nullptr;
   double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
@@ -263,6 +264,17 @@ int prof_collect(qd_handle *h)
   return QD_OK;
 }
 
+// Device-side status word of the tensor-core pass (bounded waits that ran out).
+int check_status(qd_handle *h)
+{
+  if (!h->use_tc) return QD_OK;
+  int st = 0;
+  CU(cudaMemcpy(&st, tc_status_ptr(h->tc), sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return set_err(QD_ERR_DEVICE, "tensor-core column pass: an MMA completion wait "
+                         "timed out (status %d)", st);
+  return QD_OK;
+}
+
 template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double *norm_out,
                                        bool out_z)
 {
@@ -270,6 +282,7 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   p.n1 = h->n1; p.n2 = h->n2; p.nth = h->nth; p.nl = h->nl; p.n12 = h->n12;
   p.lpsi = h->d_lpsi; p.psi_z = h->d_psi_z;
   p.P = h->d_P; p.WP = h->d_WP; p.P32 = h->d_P32; p.WP32 = h->d_WP32;
+  p.P32lo = h->d_P32lo; p.WP32lo = h->d_WP32lo;
   p.expV = h->d_expV; p.vturn = h->d_vturn; p.pot = h->d_pot; p.dt = h->dt;
   p.prestep = (mode == COL_HEAD && h->steps == 0);
   p.d1 = h->have_dump ? h->d_d1 : nullptr;
@@ -315,7 +328,9 @@ template <typename R> int issue_lines(qd_handle *h)
   p.n1 = h->n1; p.n2 = h->n2; p.nl = h->nl; p.n12 = h->n12; p.lpsi = h->d_lpsi;
   p.rot = h->d_rot; p.kin = h->d_kin;
   p.rt1 = h->d_rt1; p.rt2 = h->d_rt2; p.kt1 = h->d_kt1; p.kt2 = h->d_kt2;
-  p.kscale = (float)(1.0 / ((double)h->n1 * h->n2));
+  const double ks = 1.0 / ((double)h->n1 * h->n2);
+  p.kscale = (float)ks;
+  p.kscale_lo = (float)(ks - (double)p.kscale);
   if (sizeof(R) == 8) { p.tw1 = h->d_tw1_64; p.tw2 = h->d_tw2_64; }
   else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
   p.pl1 = h->pl1; p.pl2 = h->pl2;
@@ -406,6 +421,7 @@ template <typename R> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
   CU(cudaMemcpyAsync(nb.data(), h->d_norms, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
   CU(cudaStreamSynchronize(h->st));
   TRY(prof_collect(h));
+  TRY(check_status(h));
   if (timed) {
     double tot = 0.0;
     for (int s = 0; s < n; s++) {
@@ -470,6 +486,8 @@ int create(const qd_data *d, qd_handle **out)
   TRY(h->alloc(h->d_WP, (size_t)h->nth * h->nl));
   TRY(h->alloc(h->d_P32, (size_t)h->nth * h->nl));
   TRY(h->alloc(h->d_WP32, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_P32lo, (size_t)h->nth * h->nl));
+  TRY(h->alloc(h->d_WP32lo, (size_t)h->nth * h->nl));
   std::vector<double> T1, I1, T2, I2;
   radial_tables(d->r1, T1, I1);
   radial_tables(d->r2, T2, I2);
@@ -495,7 +513,7 @@ int create(const qd_data *d, qd_handle **out)
     TRY(upload(h, dim == 0 ? h->d_tw1_32 : h->d_tw2_32, f.data(), n));
   }
   CU(launch_legendre_matrices(h->nth, h->nl, nullptr, h->d_w, h->d_leg, h->d_P, h->d_WP,
-                              h->d_P32, h->d_WP32, h->st));
+                              h->d_P32, h->d_WP32, h->d_P32lo, h->d_WP32lo, h->st));
   g_launches++;
   if (f64) {
     TRY(h->alloc(h->d_expV, npt));
@@ -539,8 +557,10 @@ int create(const qd_data *d, qd_handle **out)
     TRY(upload(h, h->d_eta, d->CRP.eta_sq, h->ne));
     TRY(h->alloc(h->d_crp, h->ne));
   }
-  if (!f64) {
-    int rc = tc_plan_create(h->tc, h->nth, h->nl, h->d_P, h->d_WP, h->st);
+  const char *path = getenv("QD_COLUMN_PATH");   // "simt" forces the SIMT column pass
+  if (!f64 && !(path && std::string(path) == "simt")) {
+    int rc = tc_plan_create(h->tc, h->nth, h->nl, d->theta.legendre, d->theta.w, d->theta.x,
+                            h->st);
     if (rc == QD_OK) h->use_tc = true;
     else if (rc != QD_ERR_UNSUPPORTED) return rc;
   }

@@ -63,6 +63,22 @@ template <typename C> struct SmallDFT<4, C> {
   }
 };
 
+// Irrational butterfly constants as value + residual.  A float constant alone
+// would scale some outputs of every butterfly by a fixed 1 - O(1e-8); applied
+// at every stage of every step that is a systematic norm drift, so the FP32
+// butterflies multiply by hi + lo (residual ~1e-15).
+template <typename R> struct Konst;
+template <> struct Konst<float> {
+  static constexpr float rsqrt2_hi = 0.70710677f, rsqrt2_lo = 1.2101617e-8f;
+  static constexpr float sqrt3h_hi = 0.8660254f, sqrt3h_lo = 1.5543624e-8f;
+};
+template <> struct Konst<double> {
+  static constexpr double rsqrt2_hi = 0.70710678118654752440, rsqrt2_lo = 0.0;
+  static constexpr double sqrt3h_hi = 0.86602540378443864676, sqrt3h_lo = 0.0;
+};
+template <typename C, typename R> __device__ __forceinline__ C cscale2(C a, R hi, R lo)
+{ return mk(fma(a.x, hi, a.x * lo), fma(a.y, hi, a.y * lo)); }
+
 template <typename C> struct SmallDFT<8, C> {
   static __device__ __forceinline__ void run(C *v, int sgn, const C *, int)
   {
@@ -71,11 +87,11 @@ template <typename C> struct SmallDFT<8, C> {
     C o[4] = {v[1], v[3], v[5], v[7]};
     SmallDFT<4, C>::run(e, sgn, nullptr, 0);
     SmallDFT<4, C>::run(o, sgn, nullptr, 0);
-    const R h = (R)0.70710678118654752440084436210485;
-    // w8^m = exp(sgn 2 pi i m / 8)
-    C t1 = cmul(o[1], mk(h, sgn * h));
+    // w8^m = exp(sgn 2 pi i m / 8):  w8 = (1 + sgn i)/sqrt2, w8^3 = (-1 + sgn i)/sqrt2
+    const R hh = Konst<R>::rsqrt2_hi, hl = Konst<R>::rsqrt2_lo;
+    C t1 = cscale2(cadd(o[1], cmul_i(o[1], sgn)), hh, hl);
     C t2 = cmul_i(o[2], sgn);
-    C t3 = cmul(o[3], mk(-h, sgn * h));
+    C t3 = cscale2(csub(cmul_i(o[3], sgn), o[3]), hh, hl);
     v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
     v[1] = cadd(e[1], t1);   v[5] = csub(e[1], t1);
     v[2] = cadd(e[2], t2);   v[6] = csub(e[2], t2);
@@ -87,11 +103,10 @@ template <typename C> struct SmallDFT<3, C> {
   static __device__ __forceinline__ void run(C *v, int sgn, const C *, int)
   {
     typedef decltype(v[0].x) R;
-    const R hs = (R)0.86602540378443864676372317075294;   // sqrt(3)/2
     C a = v[0], b = v[1], c = v[2];
     C s = cadd(b, c);
     C t = mk(a.x - (R)0.5 * s.x, a.y - (R)0.5 * s.y);
-    C u = cmul_i(cscale(csub(b, c), hs), sgn);
+    C u = cmul_i(cscale2(csub(b, c), Konst<R>::sqrt3h_hi, Konst<R>::sqrt3h_lo), sgn);
     v[0] = cadd(a, s);
     v[1] = cadd(t, u);
     v[2] = csub(t, u);

@@ -25,8 +25,10 @@ struct ColumnParams {
   double2 *psi_z;          // theta-space staging (HEAD in / TAIL out)
   const double *P;         // [nth][nl]  P_l(x_k)
   const double *WP;        // [nth][nl]  (l+1/2) w_k P_l(x_k)
-  const float *P32;        // float copies for the FP32 kernels
+  const float *P32;        // FP32 kernels: P = P32 + P32lo (float + float residual)
   const float *WP32;
+  const float *P32lo;
+  const float *WP32lo;
   const double2 *expV;     // FP64: exp(-i V dt) [nth][n12]
   const float *vturn;      // FP32: -V dt / 2 pi reduced to [-1/2, 1/2) turns
   const double *pot;       // HEAD: potential (FP64) for the first V phase
@@ -49,7 +51,7 @@ struct LineParams {
   const double2 *kin;      // FP64: exp(-i(T1+T2)dt)/(n1 n2)    [n12]
   const float *rt1, *rt2;  // FP32: rotational phase turns [nl][n1], [nl][n2]
   const float *kt1, *kt2;  // FP32: kinetic phase turns [n1], [n2]
-  float kscale;            // FP32: 1/(n1 n2)
+  float kscale, kscale_lo; // FP32: 1/(n1 n2) = kscale + kscale_lo
   const void *tw1, *tw2;   // complex<R> root tables of n1, n2
   FftPlan pl1, pl2;
   int rows_per_cta;        // rows kernels
@@ -102,7 +104,8 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
                                      cudaStream_t s);
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const double *w,
                                      const double *legendre, double *P, double *WP,
-                                     float *P32, float *WP32, cudaStream_t s);
+                                     float *P32, float *WP32, float *P32lo, float *WP32lo,
+                                     cudaStream_t s);
 cudaError_t launch_legendre_p2(int n, int m, const double *x, double *legendre, cudaStream_t s);
 cudaError_t launch_roots(int n, double2 *tw64, float2 *tw32, cudaStream_t s);
 

@@ -118,7 +118,7 @@ def test_fp32_matches_oracle_within_budget():
     eta = base.CRP.eta_sq
     sel = eta > 1e-3 * eta.max()
     assert np.abs(b.CRP.CRP - a.CRP.CRP)[sel].max() < FP32_CRP_ABS
-    assert np.abs(gn - norms).max() < 1e-5 * norms.max()
+    assert np.abs(gn - norms).max() < 1e-4 * norms.max()
     assert rel(b.psi, a.psi) < 1e-4
 
 
@@ -127,3 +127,36 @@ def test_legendre_matrix_on_gpu():
     x, _ = S.gauss_legendre(40)
     P = legendre_matrix_gpu(40, 38, x)
     assert np.abs(P - S.legendre_p2(38, x)).max() < 1e-14
+
+
+@pytest.mark.parametrize("path", ["tc", "simt"])
+def test_fp32_c0_grid_against_oracle(path, monkeypatch):
+    # 64 x 64 x 40, n_l = 39: padded to 48 x 48 in the tensor-core pass
+    monkeypatch.setenv("QD_COLUMN_PATH", path)
+    base = S.case_c0(total_steps=150)
+    a, b = S.copy_case(base), S.copy_case(base)
+    b.options.precision = QD_PREC_FP32
+    norms, _ = O.oracle_time_evolution(a, norms=True)
+    with Propagator(b) as p:
+        p.propagate(150)
+        gn = p.norms(150)
+        p.download()
+    eta = base.CRP.eta_sq
+    sel = eta > 1e-3 * eta.max()
+    assert np.abs(b.CRP.CRP - a.CRP.CRP)[sel].max() < FP32_CRP_ABS
+    assert np.abs(gn - norms).max() < 1e-4 * norms.max()
+    assert rel(b.psi, a.psi) < 1e-4
+
+
+def test_fp32_tensor_core_and_simt_agree(monkeypatch):
+    base = S.build_case("f+h2", 128, 96, 64, m=63, total_steps=20, n_energies=9,
+                        n_gradient_points=7, r=(0.5, 9.0))
+    out = {}
+    for path in ("tc", "simt"):
+        monkeypatch.setenv("QD_COLUMN_PATH", path)
+        d = S.copy_case(base)
+        d.options.precision = QD_PREC_FP32
+        with Propagator(d) as p:
+            p.propagate(20)
+            out[path] = p.psi()
+    assert rel(out["tc"], out["simt"]) < 2e-5
