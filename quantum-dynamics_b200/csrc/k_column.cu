@@ -31,7 +31,7 @@ template <> struct MatSel<float> {
 __device__ __forceinline__ double2 vphase(const ColumnParams &p, long g, double2)
 { return p.expV[g]; }
 __device__ __forceinline__ float2 vphase(const ColumnParams &p, long g, float2)
-{ return expi_turns(p.vturn[g]); }
+{ return p.expV32[g]; }
 
 // out[o][t] = sum_c M[o*ldm + c] * in[c][t], o < nout, c < nin, KB outputs / thread;
 // M = Mhi + Mlo when Mlo is given (float matrices carried to ~2^-48)

@@ -1,0 +1,637 @@
+// k_column_tc.cu -- the column pass of the complex64 propagation on the
+// 5th-generation tensor cores (tcgen05, kind::tf32, accumulators in TMEM).
+//
+// Same work as k_column.cu (B, dump, flux rows, norm, V, F; see there for the
+// reference functions), with both Legendre contractions as back-to-back
+// GEMMs per tile of 64 grid columns (S = n_l, n_theta padded to 16):
+//   GEMM1  D[128 x S] = A1[128 x S] * B1[S x S]    A1 = psi_l tile, B1[l][k] = P_l(x_k)
+//   theta-space ops on D (tcgen05.ld -> registers) -> A2 (TMEM)
+//   GEMM2  D[128 x S] = A2[128 x S] * B2[S x S]    B2[k][l] = (l+1/2) w_k P_l(x_k)
+// The 128 GEMM rows are the real and imaginary parts of the 64 complex
+// points (row 2p = Re, 2p+1 = Im), so the complex-by-real transform is one
+// real GEMM.  FP32 accuracy from TF32 units by split products
+//   A*B ~ Ahi*(Bhi + Bmid + Blo) + Alo*Bhi,   A = Ahi + Alo,  Ahi = tf32(A),
+// with the constant Legendre matrices carried to ~2^-33 in three TF32 terms.
+//
+// Data placement: the A operands live in tensor memory (written by the
+// threads with tcgen05.st; each thread owns one TMEM lane = one GEMM row), the
+// constant B images in shared memory (K-major, 128-byte swizzle, built once
+// on the host), the accumulator in TMEM.  Shared memory is thus only the B
+// images, so two CTAs run on each SM and overlap each other's load / MMA /
+// epilogue phases.  TMEM per CTA: [Ahi | Alo | D], S columns each.
+//
+// Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
+// smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
+// steps would shrink the wavepacket by ~1%.  Both transforms are exact
+// isometries per grid column in the quadrature norms -- B (l -> theta)
+// whenever n_l <= n_theta (Gauss quadrature is exact to degree 2 n_theta - 1),
+// F (theta -> l) when its output is taken over all n_theta orders -- so each
+// column's output is rescaled to the exactly known input norm:
+//   sum_k w_k |psi_theta|^2 = sum_l |psi_l|^2/(l+1/2).
+// For n_l < n_theta, GEMM2 also forms the orders n_l..n_theta-1 (rows from the
+// same three-term recurrence) for the norm only; they are not stored.  This
+// fixes the magnitude only; shape and phase stay as computed.
+//
+// One thread issues the MMAs; completion arrives on an mbarrier through
+// tcgen05.commit.  Every wait is bounded: on timeout the CTA records an error
+// in the status word, releases its TMEM and returns.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "qd.h"
+#include "qd_tc.h"
+
+namespace {
+
+constexpr int TPTS = 64;          // complex grid points per tile
+constexpr int MROWS = 128;        // GEMM rows per tile
+constexpr int NTHREADS = 256;
+constexpr int MAXS = 64;          // max padded n_l / n_theta handled here
+constexpr uint32_t TMEM_COLS = 256;
+constexpr long WAIT_LIMIT = 1L << 22;   // mbarrier polls before giving up
+
+__host__ __device__ constexpr int pad16(int x) { return (x + 15) & ~15; }
+
+// byte offset of element (r, k) in a K-major SW128 operand of R rows
+__host__ __device__ __forceinline__ uint32_t sw128_off(int r, int k, int R)
+{
+  const int a = k >> 5, c = (k & 31) >> 2;
+  return (uint32_t)(a * R * 128 + r * 128 + ((c ^ (r & 7)) << 4) + ((k & 3) << 2));
+}
+
+// host: round to TF32 (nearest even on the 13 dropped bits)
+float tf32_round_host(float x)
+{
+  uint32_t b;
+  std::memcpy(&b, &x, 4);
+  if ((b & 0x7f800000u) != 0x7f800000u) {
+    b += 0xfffu + ((b >> 13) & 1u);
+    b &= 0xffffe000u;
+  }
+  float y;
+  std::memcpy(&y, &b, 4);
+  return y;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr)
+{
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3fffu);          // start address
+  d |= (uint64_t)1u << 16;                          // LBO (unused for SW128 K-major)
+  d |= (uint64_t)(1024u >> 4) << 32;                // SBO: 8 rows x 128 B
+  d |= (uint64_t)1u << 46;                          // descriptor version (sm100)
+  d |= (uint64_t)2u << 61;                          // SWIZZLE_128B
+  return d;
+}
+
+// kind::tf32 instruction descriptor: D f32, A/B tf32, both K-major, M=128, N
+__host__ __device__ constexpr uint32_t make_idesc(int N)
+{
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(MROWS >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase)
+{
+  for (long it = 0; it < WAIT_LIMIT; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(mbar), "r"(phase) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+struct TcDev {
+  const float4 *mats;    // B1 hi|mid|lo, B2 hi|mid|lo images
+  int *status;           // device status word (0 = ok)
+  int renorm;            // per-column isometry rescaling on
+  int nnorm;             // orders l < nnorm enter the GEMM2 output norm
+};
+
+
+// tcgen05.ld / tcgen05.st of 4 consecutive 32-bit columns of this thread's lane
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float &a, float &b, float &c, float &d)
+{
+  uint32_t r0, r1, r2, r3;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  a = __uint_as_float(r0); b = __uint_as_float(r1); c = __uint_as_float(r2); d = __uint_as_float(r3);
+}
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, float a, float b, float c, float d)
+{
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
+               :: "r"(taddr), "r"(__float_as_uint(a)), "r"(__float_as_uint(b)),
+                  "r"(__float_as_uint(c)), "r"(__float_as_uint(d)) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// the split of 4 values into the Ahi and Alo TMEM columns (col0 % 4 == 0)
+__device__ __forceinline__ void put4_tmem(uint32_t ahi, uint32_t alo, float x0, float x1,
+                                          float x2, float x3)
+{
+  const float h0 = tf32_rna(x0), h1 = tf32_rna(x1), h2 = tf32_rna(x2), h3 = tf32_rna(x3);
+  tmem_st4(ahi, h0, h1, h2, h3);
+  tmem_st4(alo, tf32_rna(x0 - h0), tf32_rna(x1 - h1), tf32_rna(x2 - h2), tf32_rna(x3 - h3));
+}
+
+__device__ __forceinline__ void mma_tf32_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+      :
+      : "r"(dtmem), "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// D = A * B over K = S, A in TMEM columns [ahi, ahi+S) and [alo, alo+S), B at
+// b (hi | mid | lo, b_bytes apart): the small split terms first, main last
+template <int S>
+__device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint32_t alo,
+                                              uint32_t b, int b_bytes)
+{
+  constexpr uint32_t idesc = make_idesc(S);
+#pragma unroll 1
+  for (int term = 0; term < 4; term++) {
+    // term 0: Ahi*Blo, 1: Ahi*Bmid, 2: Alo*Bhi, 3: Ahi*Bhi
+    const uint32_t a = term == 2 ? alo : ahi;
+    const uint32_t bt = b + (term == 0 ? 2 * b_bytes : term == 1 ? b_bytes : 0);
+#pragma unroll
+    for (int kk = 0; kk < S; kk += 8) {
+      const uint32_t boff = (uint32_t)((kk >> 5) * S * 128 + ((kk & 31) >> 3) * 32);
+      mma_tf32_ts(dtmem, a + kk, make_desc(bt + boff), idesc, (term | kk) ? 1u : 0u);
+    }
+  }
+}
+
+constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4 share a TMEM lane quarter)
+
+// sum over the 2*NG threads that hold one complex point (Re/Im rows x column
+// groups); `slot` is an [NG][TPTS] smem array.  Includes a CTA barrier.
+__device__ __forceinline__ float point_sum(float part, float *slot, int grp, int pt, bool is_im)
+{
+  part += __shfl_xor_sync(0xffffffffu, part, 1);
+  if (!is_im) slot[grp * TPTS + pt] = part;
+  __syncthreads();
+  float s = 0.f;
+#pragma unroll
+  for (int g = 0; g < NG; g++) s += slot[g * TPTS + pt];
+  return s;
+}
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev t)
+{
+  constexpr int mode = MODE;
+  constexpr int H = S / NG;                    // K columns per thread (one group)
+  constexpr int NKA = (S + 31) / 32;           // 128-byte swizzle atoms along K
+  constexpr int B_BYTES = NKA * S * 128;
+  static_assert(H % 4 == 0, "column group must be a multiple of 4");
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t base_u = smem_u32(smem_raw);
+  unsigned char *base = smem_raw + ((1024u - (base_u & 1023u)) & 1023u);
+  unsigned char *B1 = base;                     // hi | mid | lo
+  unsigned char *B2 = B1 + 3 * B_BYTES;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 3 * B_BYTES);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
+  double *red = reinterpret_cast<double *>(mbar + 4);
+  float *xch = reinterpret_cast<float *>(red + 32);      // [4 exchanges][NG][TPTS]
+  float *wk = xch + 4 * NG * TPTS;                        // [S] w_k (float), 0 beyond n_theta
+  float *linv = wk + S;                                   // [S] 1/(l+1/2)
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = (warp & 3) * 32 + lane;        // TMEM lane == GEMM row
+  const int grp = warp >> 2;                     // column group
+  const int c0 = grp * H;                        // first K/N column of this thread
+  const int pt = row >> 1;                       // complex point within tile
+  const bool is_im = row & 1;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(tmem_slot)), "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb3));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // the B images (6 * B_BYTES, a multiple of 16) by bulk asynchronous copies
+    // from this GPU's global memory into this CTA's shared memory
+    constexpr uint32_t total = 6 * B_BYTES, chunk = 16384;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(mb3), "r"(total) : "memory");
+    const char *src = reinterpret_cast<const char *>(t.mats);
+    for (uint32_t off = 0; off < total; off += chunk) {
+      const uint32_t n = total - off < chunk ? total - off : chunk;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+          :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");
+    }
+  }
+  for (int i = tid; i < S; i += NTHREADS) {
+    wk[i] = i < p.nth ? (float)p.w[i] : 0.f;
+    linv[i] = (float)(1.0 / (i + 0.5));
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = ((uint32_t)((warp & 3) * 32)) << 16;
+  const uint32_t Ahi = tmem, Alo = tmem + S, D = tmem + 2 * S;       // column bases
+  const uint32_t my_hi = Ahi + lane_base + c0, my_lo = Alo + lane_base + c0;
+  const uint32_t my_d = D + lane_base + c0;
+  const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
+  uint32_t ph1 = 0, ph2 = 0;
+  bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
+
+  float2 *surf = reinterpret_cast<float2 *>(p.surf);
+  const float *lsrc = reinterpret_cast<const float *>(p.lpsi);
+  float *ldst = reinterpret_cast<float *>(p.lpsi);
+  const long ntiles = (p.n12 + TPTS - 1) / TPTS;
+  const long n12 = p.n12;
+  const int nl = p.nl, nth = p.nth;
+  const int comp = is_im ? 1 : 0;
+  const float2 *expv = p.expV32;
+  double nsum = 0.0;
+
+  float a[H];
+#define QD_PREFETCH_A(tl)                                                              \
+  do {                                                                                 \
+    const long qq = (tl) * TPTS + pt;                                                  \
+    const bool ok = (tl) < ntiles && qq < n12;                                         \
+    _Pragma("unroll") for (int u = 0; u < H; u++) {                                    \
+      const int l = c0 + u;                                                            \
+      a[u] = (ok && l < nl) ? __ldg(lsrc + 2 * ((long)l * n12 + qq) + comp) : 0.f;     \
+    }                                                                                  \
+  } while (0)
+  if (mode != COL_HEAD) QD_PREFETCH_A((long)blockIdx.x);
+
+  for (long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const long q = tile * TPTS + pt;
+    const bool qok = q < n12;
+    const int j = qok ? (int)(q / p.n1) : 0, i = qok ? (int)(q % p.n1) : 0;
+    float2 ev[H];
+    float sc = 1.f;
+
+    if (mode != COL_HEAD) {
+      // ---- A1 = psi_l tile into TMEM, its l-space norm, GEMM1 ----------------------
+      float nl_part = 0.f;
+#pragma unroll
+      for (int u = 0; u < H; u += 4) {
+        put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
+        nl_part += a[u] * a[u] * linv[c0 + u] + a[u + 1] * a[u + 1] * linv[c0 + u + 1] +
+                   a[u + 2] * a[u + 2] * linv[c0 + u + 2] + a[u + 3] * a[u + 3] * linv[c0 + u + 3];
+      }
+      tmem_wait_st();
+      tc_fence_before();
+      nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
+      if (!is_im) xch[grp * TPTS + pt] = nl_part;
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
+        mma_commit(mb1);
+      }
+      if (mode == COL_MID) {                    // V phase of the tile, in flight during GEMM1
+#pragma unroll
+        for (int u = 0; u < H; u++) {
+          const int k = c0 + u;
+          ev[u] = (qok && k < nth) ? __ldg(expv + (long)k * n12 + q) : make_float2(1.f, 0.f);
+        }
+      }
+      float n_l = 0.f;
+#pragma unroll
+      for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
+      if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
+      ph1 ^= 1;
+      tc_fence_after();
+      // pass 1 over D: theta-space norm of the column -> isometry scale
+      float nt_part = 0.f;
+#pragma unroll
+      for (int u = 0; u < H; u += 4) {
+        float v0, v1, v2, v3;
+        tmem_ld4(my_d + u, v0, v1, v2, v3);
+        nt_part += wk[c0 + u] * v0 * v0 + wk[c0 + u + 1] * v1 * v1 +
+                   wk[c0 + u + 2] * v2 * v2 + wk[c0 + u + 3] * v3 * v3;
+      }
+      const float n_t = point_sum(nt_part, xch + NG * TPTS, grp, pt, is_im);
+      sc = (t.renorm && n_t > 0.f) ? sqrtf(n_l / n_t) : 1.f;
+    }
+
+    // ---- theta-space operations (pass 2), A2 into TMEM --------------------------------
+    float nt2_part = 0.f;
+    const float dd = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) * sc : sc;
+    const bool flux_row = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
+                          j < p.surf_j0 + p.surf_nrows;
+    float tsum = 0.f;
+#pragma unroll
+    for (int u = 0; u < H; u += 4) {
+      float v[4];
+      if (mode != COL_HEAD) {
+        tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+          const int k = c0 + u + x;
+          const float mine = v[x] * dd;
+          const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
+          const float re = is_im ? other : mine, im = is_im ? mine : other;
+          if (!is_im) {
+            tsum += wk[k] * (re * re + im * im);
+            if (qok && k < nth) {
+              if (flux_row) surf[((long)(j - p.surf_j0) * nth + k) * p.n1 + i] = make_float2(re, im);
+              if (p.out_z) p.psi_z[(long)k * n12 + q] = make_double2(re, im);
+            }
+          }
+          if (mode == COL_MID) {
+            const float2 e = ev[u + x];
+            v[x] = is_im ? re * e.y + im * e.x : re * e.x - im * e.y;
+          } else {
+            v[x] = mine;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+          const int k = c0 + u + x;
+          float val = 0.f;
+          if (qok && k < nth) {
+            const long g = (long)k * n12 + q;
+            const double2 z = p.psi_z[g];
+            double s, c;
+            sincos(p.dt * p.pot[g], &s, &c);      // exp(-i V dt) = (c, -s)
+            double2 f = make_double2(c, -s);
+            if (p.prestep) {                     // psi / sqrt(v) * v = psi * sqrt(v)
+              double sh, ch;
+              sincos(0.5 * atan2(-s, c), &sh, &ch);
+              f = make_double2(ch, sh);
+            }
+            val = (float)(is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y);
+          }
+          v[x] = val;
+        }
+      }
+      if (mode != COL_TAIL) {
+        put4_tmem(my_hi + u, my_lo + u, v[0], v[1], v[2], v[3]);
+        nt2_part += wk[c0 + u] * v[0] * v[0] + wk[c0 + u + 1] * v[1] * v[1] +
+                    wk[c0 + u + 2] * v[2] * v[2] + wk[c0 + u + 3] * v[3] * v[3];
+      }
+    }
+    if (p.norm_out && qok && mode != COL_HEAD) nsum += (double)tsum;
+    if (mode == COL_TAIL) {
+      QD_PREFETCH_A(tile + gridDim.x);
+      tc_fence_before();
+      __syncthreads();
+      continue;
+    }
+
+    // ---- GEMM2: D = A2 * B2 -------------------------------------------------------------
+    tmem_wait_st();
+    tc_fence_before();
+    nt2_part += __shfl_xor_sync(0xffffffffu, nt2_part, 1);
+    if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = nt2_part;
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
+      mma_commit(mb2);
+    }
+    float n_t2 = 0.f;
+#pragma unroll
+    for (int g = 0; g < NG; g++) n_t2 += xch[2 * NG * TPTS + g * TPTS + pt];
+    if (mode != COL_HEAD) QD_PREFETCH_A(tile + gridDim.x);   // next tile's loads fly during GEMM2
+    if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
+    ph2 ^= 1;
+    tc_fence_after();
+    float no_part = 0.f;
+#pragma unroll
+    for (int u = 0; u < H; u += 4) {
+      float v0, v1, v2, v3;
+      tmem_ld4(my_d + u, v0, v1, v2, v3);
+      no_part += (c0 + u < t.nnorm ? v0 * v0 * linv[c0 + u] : 0.f) +
+                 (c0 + u + 1 < t.nnorm ? v1 * v1 * linv[c0 + u + 1] : 0.f) +
+                 (c0 + u + 2 < t.nnorm ? v2 * v2 * linv[c0 + u + 2] : 0.f) +
+                 (c0 + u + 3 < t.nnorm ? v3 * v3 * linv[c0 + u + 3] : 0.f);
+    }
+    const float n_o = point_sum(no_part, xch + 3 * NG * TPTS, grp, pt, is_im);
+    const float sc2 = (t.renorm && n_o > 0.f) ? sqrtf(n_t2 / n_o) : 1.f;
+#pragma unroll
+    for (int u = 0; u < H; u += 4) {
+      float v[4];
+      tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const int l = c0 + u + x;
+        if (qok && l < nl) ldst[2 * ((long)l * n12 + q) + comp] = v[x] * sc2;
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+#undef QD_PREFETCH_A
+
+  if (failed && lane == 0) atomicExch(t.status, 1);
+  if (p.norm_out) {
+    const double s = block_sum(nsum, red);
+    if (tid == 0) atomicAdd(p.norm_out, s);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+template <int S> cudaError_t set_smem_attr(int bytes)
+{
+  cudaError_t e = cudaFuncSetAttribute(k_column_tc<S, COL_HEAD>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_TAIL>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
+
+template <int S>
+void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
+                 int mode)
+{
+  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD><<<grid, NTHREADS, smem, s>>>(p, t);
+  else if (mode == COL_MID) k_column_tc<S, COL_MID><<<grid, NTHREADS, smem, s>>>(p, t);
+  else k_column_tc<S, COL_TAIL><<<grid, NTHREADS, smem, s>>>(p, t);
+}
+
+template <int S> constexpr int smem_bytes_for()
+{
+  return 1024 + 6 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4;
+}
+
+// P_l(x_k) for l = 0..lmax by the recurrence of LegendreP2.m:9-21 (FP64)
+std::vector<double> legendre_rows(int nth, int lmax, const double *x)
+{
+  std::vector<double> P((size_t)nth * (lmax + 1));
+  for (int k = 0; k < nth; k++) {
+    double p0 = 1.0, p1 = x[k];
+    P[(size_t)k * (lmax + 1)] = 1.0;
+    if (lmax >= 1) P[(size_t)k * (lmax + 1) + 1] = x[k];
+    for (int l = 2; l <= lmax; l++) {
+      const double p2 = (2.0 - 1.0 / l) * x[k] * p1 - (1.0 - 1.0 / l) * p0;
+      P[(size_t)k * (lmax + 1) + l] = p2;
+      p0 = p1;
+      p1 = p2;
+    }
+  }
+  return P;
+}
+
+}  // namespace
+
+int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const double *w,
+                   const double *x, cudaStream_t s)
+{
+  const int S = pad16(nl > nth ? nl : nth);
+  if (S > MAXS) return QD_ERR_UNSUPPORTED;
+  // Extra orders l = n_l .. n_theta-1 for the GEMM2 norm, and a check that the
+  // quadrature makes the transform pair an isometry (else no rescaling).
+  bool renorm = nl <= nth;
+  std::vector<double> Pext;
+  if (renorm) {
+    Pext = legendre_rows(nth, nth - 1, x);
+    for (int k = 0; k < nth && renorm; k++)
+      for (int l = 0; l < nl; l++)
+        if (std::fabs(Pext[(size_t)k * nth + l] - legendre[l + (long)k * nl]) >
+            1e-10 * (1.0 + std::fabs(legendre[l + (long)k * nl]))) {
+          renorm = false;
+          break;
+        }
+    for (int l = 0; l < nth && renorm; l++)
+      for (int l2 = 0; l2 < nth; l2++) {
+        double g = 0.0;
+        for (int k = 0; k < nth; k++)
+          g += w[k] * Pext[(size_t)k * nth + l] * Pext[(size_t)k * nth + l2];
+        g *= (l2 + 0.5);
+        if (std::fabs(g - (l == l2 ? 1.0 : 0.0)) > 1e-9) { renorm = false; break; }
+      }
+  }
+  const int nka = (S + 31) / 32;
+  const int bb = nka * S * 128;
+  std::vector<unsigned char> img(6 * (size_t)bb, 0);
+  unsigned char *b1 = img.data(), *b2 = b1 + 3 * bb;
+  auto put = [&](unsigned char *img3, int r, int k, double val) {
+    const float h = tf32_round_host((float)val);
+    const double r1 = val - (double)h;
+    const float m = tf32_round_host((float)r1);
+    const float l = tf32_round_host((float)(r1 - (double)m));
+    const uint32_t off = sw128_off(r, k, S);
+    std::memcpy(img3 + off, &h, 4);
+    std::memcpy(img3 + bb + off, &m, 4);
+    std::memcpy(img3 + 2 * bb + off, &l, 4);
+  };
+  const int lrows = renorm ? nth : nl;          // orders formed by GEMM2
+  for (int k = 0; k < nth; k++) {
+    for (int l = 0; l < nl; l++) put(b1, k, l, legendre[l + (long)k * nl]);   // B1: row k, K = l
+    for (int l = 0; l < lrows; l++) {
+      const double P = l < nl ? legendre[l + (long)k * nl] : Pext[(size_t)k * nth + l];
+      put(b2, l, k, (l + 0.5) * w[k] * P);                                     // B2: row l, K = k
+    }
+  }
+  void *d = nullptr;
+  if (cudaMalloc(&d, img.size() + sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return QD_ERR_NOMEM;
+  }
+  if (cudaMemcpyAsync(d, img.data(), img.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemsetAsync((char *)d + img.size(), 0, sizeof(int), s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaFree(d);
+    return QD_ERR_CUDA;
+  }
+  plan.nth = nth; plan.nl = nl; plan.S = S; plan.renorm = renorm ? 1 : 0;
+  plan.mats = d;
+  plan.mats_bytes = img.size();
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  plan.grid = 2 * sms;             // two CTAs per SM (shared memory and TMEM allow it)
+  cudaError_t e = cudaSuccess;
+  switch (S) {
+    case 16: plan.smem_bytes = smem_bytes_for<16>();
+      e = set_smem_attr<16>(plan.smem_bytes); break;
+    case 32: plan.smem_bytes = smem_bytes_for<32>();
+      e = set_smem_attr<32>(plan.smem_bytes); break;
+    case 48: plan.smem_bytes = smem_bytes_for<48>();
+      e = set_smem_attr<48>(plan.smem_bytes); break;
+    default: plan.smem_bytes = smem_bytes_for<64>();
+      e = set_smem_attr<64>(plan.smem_bytes); break;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(d);
+    plan.mats = nullptr;
+    return QD_ERR_UNSUPPORTED;
+  }
+  return QD_OK;
+}
+
+void tc_plan_destroy(TcPlan &plan)
+{
+  if (plan.mats) cudaFree(plan.mats);
+  plan.mats = nullptr;
+}
+
+int *tc_status_ptr(const TcPlan &plan)
+{
+  return reinterpret_cast<int *>(static_cast<char *>(plan.mats) + plan.mats_bytes);
+}
+
+cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode,
+                             cudaStream_t s)
+{
+  TcDev t;
+  t.mats = reinterpret_cast<const float4 *>(plan.mats);
+  t.status = tc_status_ptr(plan);
+  t.renorm = plan.renorm;
+  t.nnorm = plan.nth < plan.S ? plan.nth : plan.S;
+  const long ntiles = (p.n12 + TPTS - 1) / TPTS;
+  const int grid = (int)(ntiles < plan.grid ? ntiles : plan.grid);
+  switch (plan.S) {
+    case 16: launch_mode<16>(grid, plan.smem_bytes, s, p, t, mode); break;
+    case 32: launch_mode<32>(grid, plan.smem_bytes, s, p, t, mode); break;
+    case 48: launch_mode<48>(grid, plan.smem_bytes, s, p, t, mode); break;
+    default: launch_mode<64>(grid, plan.smem_bytes, s, p, t, mode); break;
+  }
+  return cudaGetLastError();
+}

@@ -14,40 +14,12 @@
 
 namespace {
 
-// (offset m, integer coefficient) in the order Gradient3.F sums them
-__constant__ int c_grad_m[5][5] = {
-  {1, 0, 0, 0, 0}, {2, 1, 0, 0, 0}, {3, 2, 1, 0, 0}, {4, 3, 2, 1, 0}, {5, 4, 3, 2, 1}};
-__constant__ double c_grad_c[5][5] = {
-  {1, 0, 0, 0, 0}, {-1, 8, 0, 0, 0}, {1, -9, 45, 0, 0}, {-3, 32, -168, 672, 0},
-  {2, -25, 150, -600, 2100}};
-
 template <typename R>
 __global__ void k_flux_prep(FluxParams p)
 {
   typedef typename Cplx<R>::T C;
-  const int nq = p.nth * p.n1;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nq) return;
-  const C *s = reinterpret_cast<const C *>(p.surf);
-  const long rs = (long)nq;                 // row stride in surf
-  const int h = p.h, sel = h - 1;
-  const double2 v = to_z(s[(long)h * rs + q]);
-  double2 g = make_double2(0.0, 0.0);
-  for (int t = 0; t < h; t++) {
-    const int m = c_grad_m[sel][t];
-    const double c = c_grad_c[sel][t];
-    const double2 a = to_z(s[(long)(h + m) * rs + q]);
-    const double2 b = to_z(s[(long)(h - m) * rs + q]);
-    const double dx = a.x - b.x, dy = a.y - b.y;
-    if (t == 0 && c == 1.0) { g.x = dx; g.y = dy; }
-    else if (t == 0 && c == -1.0) { g.x = -dx; g.y = -dy; }
-    else { g.x += c * dx; g.y += c * dy; }
-  }
-  g.x /= p.den_dx;
-  g.y /= p.den_dx;
-  const long o = (long)p.slot * nq + q;
-  p.ring_psi[o] = v;
-  p.ring_g[o] = g;
+  if (q < p.nth * p.n1) flux_point<C>(p, q);
 }
 
 constexpr int EB = 8;          // energies per CTA

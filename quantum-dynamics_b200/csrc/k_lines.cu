@@ -21,9 +21,9 @@ template <> struct Phase<double> {
 };
 template <> struct Phase<float> {
   static __device__ __forceinline__ float2 rot(const LineParams &p, int l, int j, int i)
-  { return expi_turns(p.rt1[l * p.n1 + i] + p.rt2[l * p.n2 + j]); }
+  { return cmul(__ldg(p.rc1 + l * p.n1 + i), __ldg(p.rc2 + l * p.n2 + j)); }
   static __device__ __forceinline__ float2 kin(const LineParams &p, int j, int i)
-  { return cscale2(expi_turns(p.kt1[i] + p.kt2[j]), p.kscale, p.kscale_lo); }
+  { return cscale2(cmul(__ldg(p.kc1 + i), __ldg(p.kc2 + j)), p.kscale, p.kscale_lo); }
 };
 
 // dir = -1: Rot then forward FFT along R;  dir = +1: inverse FFT then Rot.

@@ -4,9 +4,11 @@
 //     expV[k][j][i] = exp(-i V dt)                       setup_exp_ipot_dt    timeEvol.C:438-463
 //     rot[l][j][i]  = exp(-i l(l+1)(I1_i + I2_j) dt/2)   setup_exp_irot_dt_2  timeEvol.C:465-491
 //     kin[j][i]     = exp(-i(T1_i + T2_j) dt) / n1 / n2  setup_exp_ikin_dt    timeEvol.C:493-517
-//   FP32 form: the same phases as fractions of a turn, reduced in FP64 to
-//   [-1/2, 1/2] and stored as float, so that the complex64 propagation
-//   evaluates exp(2 pi i turns) with sincospif and no large-argument loss.
+//   FP32 form: exp(-i V dt) and the separable factors of the rotational and
+//   kinetic phases (exp(-i l(l+1) I1 dt/2), exp(-i l(l+1) I2 dt/2),
+//   exp(-i T1 dt), exp(-i T2 dt)), each evaluated in FP64 with the phase
+//   reduced to a fraction of a turn and rounded once to complex64, so the
+//   complex64 propagation multiplies by unbiased unit-modulus factors.
 //   Legendre matrices: P[k][l] = P_l(x_k) (LegendreP2.m:9-21 recurrence) and
 //   WP[k][l] = (l+1/2) w_k P_l(x_k) (setup_weight_legendre, timeEvol.C:737-760).
 #include "qd_kernels.h"
@@ -51,31 +53,42 @@ __global__ void k_tables_fp64(int n1, int n2, int nth, int nl, double dt, const 
 
 __global__ void k_tables_fp32(int n1, int n2, int nth, int nl, double dt, const double *pot,
                               const double *I1, const double *I2, const double *T1,
-                              const double *T2, float *vturn, float *rt1, float *rt2,
-                              float *kt1, float *kt2)
+                              const double *T2, float2 *expV32, float2 *rc1, float2 *rc2,
+                              float2 *kc1, float2 *kc2)
 {
   const long nv = (long)n1 * n2 * nth;
   const long a1 = (long)nl * n1, a2 = (long)nl * n2;
   const long total = nv + a1 + a2 + n1 + n2;
   for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < total;
        g += (long)gridDim.x * blockDim.x) {
+    // every phase in FP64 (exact turn reduction), rounded once to complex64
+    double ph;
+    float2 *dst;
     if (g < nv) {
-      vturn[g] = (float)turns(-dt * pot[g]);
+      ph = -dt * pot[g];
+      dst = expV32 + g;
     } else if (g < nv + a1) {
       const long q = g - nv;
       const int l = (int)(q / n1), i = (int)(q % n1);
-      rt1[q] = (float)turns(-(double)(l * (l + 1)) * I1[i] * dt / 2);
+      ph = -(double)(l * (l + 1)) * I1[i] * dt / 2;
+      dst = rc1 + q;
     } else if (g < nv + a1 + a2) {
       const long q = g - nv - a1;
       const int l = (int)(q / n2), j = (int)(q % n2);
-      rt2[q] = (float)turns(-(double)(l * (l + 1)) * I2[j] * dt / 2);
+      ph = -(double)(l * (l + 1)) * I2[j] * dt / 2;
+      dst = rc2 + q;
     } else if (g < nv + a1 + a2 + n1) {
       const int i = (int)(g - nv - a1 - a2);
-      kt1[i] = (float)turns(-T1[i] * dt);
+      ph = -T1[i] * dt;
+      dst = kc1 + i;
     } else {
       const int j = (int)(g - nv - a1 - a2 - n1);
-      kt2[j] = (float)turns(-T2[j] * dt);
+      ph = -T2[j] * dt;
+      dst = kc2 + j;
     }
+    double s, c;
+    sincospi(2.0 * turns(ph), &s, &c);
+    *dst = make_float2((float)c, (float)s);
   }
 }
 
@@ -132,12 +145,12 @@ cudaError_t launch_setup_tables_fp64(int n1, int n2, int nth, int nl, double dt,
 
 cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
                                      const double *pot, const double *I1, const double *I2,
-                                     const double *T1, const double *T2, float *vturn,
-                                     float *rt1, float *rt2, float *kt1, float *kt2,
+                                     const double *T1, const double *T2, float2 *expV32,
+                                     float2 *rc1, float2 *rc2, float2 *kc1, float2 *kc2,
                                      cudaStream_t s)
 {
-  k_tables_fp32<<<148 * 8, 256, 0, s>>>(n1, n2, nth, nl, dt, pot, I1, I2, T1, T2, vturn, rt1,
-                                        rt2, kt1, kt2);
+  k_tables_fp32<<<148 * 8, 256, 0, s>>>(n1, n2, nth, nl, dt, pot, I1, I2, T1, T2, expV32, rc1,
+                                        rc2, kc1, kc2);
   return cudaGetLastError();
 }
 

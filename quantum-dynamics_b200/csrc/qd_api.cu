@@ -120,7 +120,9 @@ struct qd_handle {
   double *d_I1 = nullptr, *d_I2 = nullptr, *d_T1 = nullptr, *d_T2 = nullptr;
   double *d_d1 = nullptr, *d_d2 = nullptr;
   double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
-  float *d_vturn = nullptr, *d_rt1 = nullptr, *d_rt2 = nullptr, *d_kt1 = nullptr, *d_kt2 = nullptr;
+  float2 *d_expV32 = nullptr;
+  float2 *d_rc1 = nullptr, *d_rc2 = nullptr, *d_kc1 = nullptr, *d_kc2 = nullptr;
+  int slice_cluster = 0;          // fused slice kernel: CTAs per l-slice (0 = split kernels)
   double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
   void *d_lpsi = nullptr;
@@ -135,6 +137,7 @@ struct qd_handle {
 
   FftPlan pl1, pl2;
   int ring_fill = 0;
+  int flux_pending = -1;          // ring slot whose preparation is not yet issued
   long acc_done = 0;
   bool started = false;           // l-space state valid on the device
   bool last_finalized = true;     // flux/norm of the last step already taken
@@ -264,6 +267,18 @@ int prof_collect(qd_handle *h)
   return QD_OK;
 }
 
+FluxParams flux_params(qd_handle *h)
+{
+  FluxParams f{};
+  f.n1 = h->n1; f.nth = h->nth; f.npts = h->npts; f.h = h->h; f.surf = h->d_surf;
+  static const int den[] = {0, 2, 12, 60, 840, 2520};
+  f.den_dx = den[h->h] * h->data->r2.dr;
+  f.ring_psi = h->d_ring_psi; f.ring_g = h->d_ring_g; f.slot = h->flux_pending;
+  return f;
+}
+int after_flux_prep(qd_handle *h);
+template <typename R> int issue_flux_prep(qd_handle *h);
+
 // Device-side status word of the tensor-core pass (bounded waits that ran out).
 int check_status(qd_handle *h)
 {
@@ -283,7 +298,7 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   p.lpsi = h->d_lpsi; p.psi_z = h->d_psi_z;
   p.P = h->d_P; p.WP = h->d_WP; p.P32 = h->d_P32; p.WP32 = h->d_WP32;
   p.P32lo = h->d_P32lo; p.WP32lo = h->d_WP32lo;
-  p.expV = h->d_expV; p.vturn = h->d_vturn; p.pot = h->d_pot; p.dt = h->dt;
+  p.expV = h->d_expV; p.expV32 = h->d_expV32; p.pot = h->d_pot; p.dt = h->dt;
   p.prestep = (mode == COL_HEAD && h->steps == 0);
   p.d1 = h->have_dump ? h->d_d1 : nullptr;
   p.d2 = h->have_dump ? h->d_d2 : nullptr;
@@ -298,46 +313,127 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   CU(e);
   TRY(prof_mark(h, PROF_COLUMN));
   if (flux) {
-    FluxParams f{};
-    f.n1 = h->n1; f.nth = h->nth; f.npts = h->npts; f.h = h->h; f.surf = h->d_surf;
-    static const int den[] = {0, 2, 12, 60, 840, 2520};
-    f.den_dx = den[h->h] * h->data->r2.dr;
-    f.ring_psi = h->d_ring_psi; f.ring_g = h->d_ring_g; f.slot = h->ring_fill;
-    CU(launch_flux_prep<R>(f, h->st));
-    g_launches++;
-    TRY(prof_mark(h, PROF_FLUX));
-    h->ring_fill++;
-    if (h->ring_fill == QD_RING) {
-      AccumParams a{};
-      a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
-      a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
-      a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
-      CU(launch_flux_accum(a, h->st));
-      g_launches++;
-      TRY(prof_mark(h, PROF_ACCUM));
-      h->acc_done += h->ring_fill;
-      h->ring_fill = 0;
-    }
+    // the surface rows of this step go to ring slot ring_fill; with the fused
+    // slice kernel that preparation rides along in the next l-space launch
+    h->flux_pending = h->ring_fill;
+    if (!(sizeof(R) == 4 && h->slice_cluster > 0) || mode == COL_TAIL)
+      TRY(issue_flux_prep<R>(h));
   }
+  return QD_OK;
+}
+
+// ring bookkeeping after the flux preparation of a step has been issued
+int after_flux_prep(qd_handle *h)
+{
+  h->flux_pending = -1;
+  h->ring_fill++;
+  if (h->ring_fill == QD_RING) {
+    AccumParams a{};
+    a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+    a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
+    a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+    TRY(prof_mark(h, -1));
+    CU(launch_flux_accum(a, h->st));
+    g_launches++;
+    TRY(prof_mark(h, PROF_ACCUM));
+    h->acc_done += h->ring_fill;
+    h->ring_fill = 0;
+  }
+  return QD_OK;
+}
+
+template <typename R> int issue_flux_prep(qd_handle *h)
+{
+  TRY(prof_mark(h, -1));
+  CU(launch_flux_prep<R>(flux_params(h), h->st));
+  g_launches++;
+  TRY(prof_mark(h, PROF_FLUX));
+  return after_flux_prep(h);
+}
+
+LineParams line_params(qd_handle *h, bool f32)
+{
+  LineParams p{};
+  p.n1 = h->n1; p.n2 = h->n2; p.nl = h->nl; p.n12 = h->n12; p.lpsi = h->d_lpsi;
+  p.rot = h->d_rot; p.kin = h->d_kin;
+  p.rc1 = h->d_rc1; p.rc2 = h->d_rc2; p.kc1 = h->d_kc1; p.kc2 = h->d_kc2;
+  p.cluster = f32 ? h->slice_cluster : 0;
+  const double ks = 1.0 / ((double)h->n1 * h->n2);
+  p.kscale = (float)ks;
+  p.kscale_lo = (float)(ks - (double)p.kscale);
+  if (!f32) { p.tw1 = h->d_tw1_64; p.tw2 = h->d_tw2_64; }
+  else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
+  p.pl1 = h->pl1; p.pl2 = h->pl2;
+  return p;
+}
+
+// Autotuner of the complex64 l-space pass: time the fused slice kernel with
+// 1, 2 and 4 CTAs per slice (and the split kernels) on a scratch wavepacket
+// and keep the fastest.  QD_SLICE_CLUSTER=0|1|2|4 forces a choice.
+int tune_slice(qd_handle *h)
+{
+  h->slice_cluster = 0;
+  if (h->prec != QD_PREC_FP32) return QD_OK;
+  const char *force = getenv("QD_SLICE_CLUSTER");
+  if (force) {
+    const int cl = atoi(force);
+    h->slice_cluster = slice_cluster_ok(h->n1, h->n2, cl) ? cl : 0;
+    return QD_OK;
+  }
+  void *scratch = nullptr;
+  CU(cudaMalloc(&scratch, sizeof(float2) * h->n12 * h->nl));
+  CU(cudaMemsetAsync(scratch, 0, sizeof(float2) * h->n12 * h->nl, h->st));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  LineParams p = line_params(h, true);
+  p.lpsi = scratch;
+  float best = 1e30f;
+  for (int cl : {0, 1, 2, 4}) {
+    if (cl > 0 && !slice_cluster_ok(h->n1, h->n2, cl)) continue;
+    p.cluster = cl;
+    bool ok = true;
+    for (int it = 0; it < 2 && ok; it++)
+      ok = (cl ? launch_slice(p, h->st) : launch_lines<float>(p, h->st)) == cudaSuccess;
+    if (ok) ok = cudaEventRecord(e0, h->st) == cudaSuccess;
+    for (int it = 0; it < 5 && ok; it++)
+      ok = (cl ? launch_slice(p, h->st) : launch_lines<float>(p, h->st)) == cudaSuccess;
+    if (ok) ok = cudaEventRecord(e1, h->st) == cudaSuccess;
+    if (ok) ok = cudaStreamSynchronize(h->st) == cudaSuccess;
+    float ms = 0.f;
+    if (ok) ok = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    if (!ok) {                      // e.g. a cluster shape that cannot be scheduled
+      cudaGetLastError();
+      continue;
+    }
+    if (ms < best) { best = ms; h->slice_cluster = cl; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaFree(scratch));
   return QD_OK;
 }
 
 template <typename R> int issue_lines(qd_handle *h)
 {
-  LineParams p{};
-  p.n1 = h->n1; p.n2 = h->n2; p.nl = h->nl; p.n12 = h->n12; p.lpsi = h->d_lpsi;
-  p.rot = h->d_rot; p.kin = h->d_kin;
-  p.rt1 = h->d_rt1; p.rt2 = h->d_rt2; p.kt1 = h->d_kt1; p.kt2 = h->d_kt2;
-  const double ks = 1.0 / ((double)h->n1 * h->n2);
-  p.kscale = (float)ks;
-  p.kscale_lo = (float)(ks - (double)p.kscale);
-  if (sizeof(R) == 8) { p.tw1 = h->d_tw1_64; p.tw2 = h->d_tw2_64; }
-  else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
-  p.pl1 = h->pl1; p.pl2 = h->pl2;
+  LineParams p = line_params(h, sizeof(R) == 4);
+  const bool fused_flux = p.cluster > 0 && h->flux_pending >= 0;
+  if (fused_flux) {
+    p.flux = flux_params(h);
+    const int nq = h->nth * h->n1;
+    const int ctas = (nq + 511) / 512;                // 512 threads per slice CTA
+    p.flux_ctas = (ctas + p.cluster - 1) / p.cluster * p.cluster;
+  }
   TRY(prof_mark(h, -1));
-  CU(launch_lines<R>(p, h->st));
-  g_launches += lines_launches_per_step(h->n1, h->n2, h->prec);
+  if (p.cluster > 0) {
+    CU(launch_slice(p, h->st));
+    g_launches++;
+  } else {
+    CU(launch_lines<R>(p, h->st));
+    g_launches += lines_launches_per_step(h->n1, h->n2, h->prec);
+  }
   TRY(prof_mark(h, PROF_LINES));
+  if (fused_flux) TRY(after_flux_prep(h));
   return QD_OK;
 }
 
@@ -523,14 +619,14 @@ int create(const qd_data *d, qd_handle **out)
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV, h->d_rot, h->d_kin,
                                 h->st));
   } else {
-    TRY(h->alloc(h->d_vturn, npt));
-    TRY(h->alloc(h->d_rt1, (size_t)h->nl * h->n1));
-    TRY(h->alloc(h->d_rt2, (size_t)h->nl * h->n2));
-    TRY(h->alloc(h->d_kt1, h->n1));
-    TRY(h->alloc(h->d_kt2, h->n2));
+    TRY(h->alloc(h->d_expV32, npt));
+    TRY(h->alloc(h->d_rc1, (size_t)h->nl * h->n1));
+    TRY(h->alloc(h->d_rc2, (size_t)h->nl * h->n2));
+    TRY(h->alloc(h->d_kc1, h->n1));
+    TRY(h->alloc(h->d_kc2, h->n2));
     CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth, h->nl, h->dt, h->d_pot, h->d_I1,
-                                h->d_I2, h->d_T1, h->d_T2, h->d_vturn, h->d_rt1, h->d_rt2,
-                                h->d_kt1, h->d_kt2, h->st));
+                                h->d_I2, h->d_T1, h->d_T2, h->d_expV32, h->d_rc1, h->d_rc2,
+                                h->d_kc1, h->d_kc2, h->st));
   }
   g_launches++;
   const size_t csz = f64 ? sizeof(double2) : sizeof(float2);
@@ -564,6 +660,7 @@ int create(const qd_data *d, qd_handle **out)
     if (rc == QD_OK) h->use_tc = true;
     else if (rc != QD_ERR_UNSUPPORTED) return rc;
   }
+  TRY(tune_slice(h));
   CU(cudaStreamSynchronize(h->st));
   return QD_OK;
 }

@@ -30,7 +30,7 @@ struct ColumnParams {
   const float *P32lo;
   const float *WP32lo;
   const double2 *expV;     // FP64: exp(-i V dt) [nth][n12]
-  const float *vturn;      // FP32: -V dt / 2 pi reduced to [-1/2, 1/2) turns
+  const float2 *expV32;    // FP32: exp(-i V dt) from FP64, rounded to complex64
   const double *pot;       // HEAD: potential (FP64) for the first V phase
   double dt;
   int prestep;             // HEAD: divide by the principal sqrt(exp(-iVdt)) first
@@ -43,27 +43,68 @@ struct ColumnParams {
   int out_z;               // TAIL: also write psi_z
 };
 
-struct LineParams {
-  int n1, n2, nl;
-  long n12;
-  void *lpsi;              // complex<R>, in place
-  const double2 *rot;      // FP64: exp(-i l(l+1)(I1+I2) dt/2) [nl][n12]
-  const double2 *kin;      // FP64: exp(-i(T1+T2)dt)/(n1 n2)    [n12]
-  const float *rt1, *rt2;  // FP32: rotational phase turns [nl][n1], [nl][n2]
-  const float *kt1, *kt2;  // FP32: kinetic phase turns [n1], [n2]
-  float kscale, kscale_lo; // FP32: 1/(n1 n2) = kscale + kscale_lo
-  const void *tw1, *tw2;   // complex<R> root tables of n1, n2
-  FftPlan pl1, pl2;
-  int rows_per_cta;        // rows kernels
-  int cols_per_cta;        // column kernel
-};
-
 struct FluxParams {
   int n1, nth, npts, h;
   const void *surf;        // complex<R> [2h+1][nth][n1]
   double den_dx;           // den * dr2 (Gradient3.F divides by it)
   double2 *ring_psi, *ring_g;
   int slot;                // ring slot of this step
+};
+
+// psi_s and d psi_s / dr at grid point q = k*n1 + i of the dividing surface
+// from the 2h+1 captured rows: the central differences of Gradient3.F:31-167
+// with the integer coefficients summed in the same order, in FP64.
+template <typename C>
+__device__ __forceinline__ void flux_point(const FluxParams &p, int q)
+{
+  // (offset m, coefficient) in Gradient3.F order for h = 1..5
+  const int nq = p.nth * p.n1;
+  const C *s = reinterpret_cast<const C *>(p.surf);
+  const int h = p.h;
+  const double2 v = to_z(s[(long)h * nq + q]);
+  double gx = 0.0, gy = 0.0;
+#pragma unroll
+  for (int t = 0; t < 5; t++) {
+    if (t >= h) break;
+    const int m = h - t;   // offsets in descending order
+    double c;
+    switch (h) {
+      case 1: c = 1.0; break;
+      case 2: c = t == 0 ? -1.0 : 8.0; break;
+      case 3: c = t == 0 ? 1.0 : t == 1 ? -9.0 : 45.0; break;
+      case 4: c = t == 0 ? -3.0 : t == 1 ? 32.0 : t == 2 ? -168.0 : 672.0; break;
+      default: c = t == 0 ? 2.0 : t == 1 ? -25.0 : t == 2 ? 150.0 : t == 3 ? -600.0 : 2100.0; break;
+    }
+    const double2 a = to_z(s[(long)(h + m) * nq + q]);
+    const double2 b = to_z(s[(long)(h - m) * nq + q]);
+    const double dx = a.x - b.x, dy = a.y - b.y;
+    if (t == 0) { gx = c * dx; gy = c * dy; }   // first term exact (c * d, as Fortran's 0 + c*d)
+    else { gx += c * dx; gy += c * dy; }
+  }
+  const long o = (long)p.slot * nq + q;
+  p.ring_psi[o] = v;
+  p.ring_g[o] = make_double2(gx / p.den_dx, gy / p.den_dx);
+}
+
+struct LineParams {
+  int n1, n2, nl;
+  long n12;
+  void *lpsi;              // complex<R>, in place
+  const double2 *rot;      // FP64: exp(-i l(l+1)(I1+I2) dt/2) [nl][n12]
+  const double2 *kin;      // FP64: exp(-i(T1+T2)dt)/(n1 n2)    [n12]
+  // FP32: separable phases from FP64, rounded once to complex64:
+  //   rot = rc1[l][i] rc2[l][j],  rc1 = exp(-i l(l+1) I1 dt/2), rc2 likewise with I2
+  //   kin = kc1[i] kc2[j] (kscale + kscale_lo),  kc1 = exp(-i T1 dt), kc2 likewise
+  const float2 *rc1, *rc2;
+  const float2 *kc1, *kc2;
+  float kscale, kscale_lo; // FP32: 1/(n1 n2) = kscale + kscale_lo
+  const void *tw1, *tw2;   // complex<R> root tables of n1, n2
+  FftPlan pl1, pl2;
+  int rows_per_cta;        // rows kernels
+  int cols_per_cta;        // column kernel
+  int cluster;             // fused slice kernel: CTAs per slice (0 = split kernels)
+  FluxParams flux;         // fused slice kernel: flux preparation of the step ...
+  int flux_ctas;           // ... by this many extra CTAs (0 = none)
 };
 
 struct AccumParams {
@@ -99,9 +140,13 @@ cudaError_t launch_setup_tables_fp64(int n1, int n2, int nth, int nl, double dt,
                                      double2 *rot, double2 *kin, cudaStream_t s);
 cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
                                      const double *pot, const double *I1, const double *I2,
-                                     const double *T1, const double *T2, float *vturn,
-                                     float *rt1, float *rt2, float *kt1, float *kt2,
+                                     const double *T1, const double *T2, float2 *expV32,
+                                     float2 *rc1, float2 *rc2, float2 *kc1, float2 *kc2,
                                      cudaStream_t s);
+// fused slice kernel (FP32): CTAs per slice it can run with for these sizes
+// (0 if none), its launch, and the smem bytes it needs
+int slice_cluster_ok(int n1, int n2, int cluster);
+cudaError_t launch_slice(const LineParams &p, cudaStream_t s);
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const double *w,
                                      const double *legendre, double *P, double *WP,
                                      float *P32, float *WP32, float *P32lo, float *WP32lo,

@@ -160,3 +160,42 @@ def test_fp32_tensor_core_and_simt_agree(monkeypatch):
             p.propagate(20)
             out[path] = p.psi()
     assert rel(out["tc"], out["simt"]) < 2e-5
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 32), (128, 128, 64), (128, 96, 64), (48, 40, 24)])
+def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
+    # fused slice kernel with 1, 2, 4 CTAs per slice (where they fit) against
+    # the three-kernel split pass
+    n1, n2, nth = shape
+    base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=8, n_energies=5,
+                        n_gradient_points=5, r=(0.5, 9.0))
+    out = {}
+    for cl in ("0", "1", "2", "4"):
+        monkeypatch.setenv("QD_SLICE_CLUSTER", cl)
+        d = S.copy_case(base)
+        d.options.precision = QD_PREC_FP32
+        with Propagator(d) as p:
+            p.propagate(8)
+            out[cl] = p.psi()
+    ref = out["0"]
+    for cl, psi in out.items():
+        assert rel(psi, ref) < 2e-5, cl
+
+
+def test_fp32_c1_full_run_within_pe_budget():
+    # the F + H2 128 x 128 x 64 case over its full 10000 steps: complex64 with the
+    # tensor-core Legendre pass against the FP64 plain form (which is pinned to
+    # the oracle above), max |dP(E)| <= 1e-3 where eta^2 > 1e-3 max eta^2
+    c1 = S.case_c1()
+    out = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        d = S.copy_case(c1)
+        d.options.precision = prec
+        with Propagator(d) as p:
+            p.propagate(10000)
+            out[prec] = (p.crp(), p.norms(10000))
+    eta = c1.CRP.eta_sq
+    sel = eta > 1e-3 * eta.max()
+    dP = np.abs(out[QD_PREC_FP32][0] - out[QD_PREC_FP64][0])[sel].max()
+    assert dP < FP32_CRP_ABS, dP
+    assert np.abs(out[QD_PREC_FP32][1] - out[QD_PREC_FP64][1]).max() < 1e-3
