@@ -190,10 +190,30 @@ int qd_steps(qd_handle *h, int32_t *steps_out);
 int qd_set_profiling(qd_handle *h, int32_t on);
 int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written);
 
-/* Checkpoint / restart of the full propagation state (psi in l-space, steps,
- * flux accumulators). */
+/* Checkpoint / restart of the full propagation state: the l-space
+ * wavepacket, time.steps, the flux accumulators phi_E, dphi_E and the
+ * pending flux history, and the per-step norms.  The reference keeps only psi
+ * and time.steps across calls (timeEvol.C:664-665), so its P(E) restarts;
+ * qd_restore resumes the accumulation exactly.  qd_restore needs a handle
+ * created from data of the same sizes and precision. */
 int qd_checkpoint(qd_handle *h, const char *path);
 int qd_restore(qd_handle *h, const char *path);
+
+/* ---- batches: many propagations in the same launches ------------------- */
+
+/* runs[0..n_runs) share r1, r2, theta, time.time_step, time.steps,
+ * options.precision, the absorbers and the CRP settings (surface, stencil,
+ * number of energies); psi, pot, CRP.energies and CRP.eta_sq may differ per
+ * run (one potential table is kept when all pot arrays are equal).  All runs
+ * advance together; results per run.  No counterpart in the reference, whose
+ * MEX propagates one wavepacket per call. */
+int qd_create_batch(const qd_data *runs, int32_t n_runs, qd_handle **out);
+int qd_time_evolution_batch(qd_data *runs, int32_t n_runs);
+int qd_n_runs(qd_handle *h, int32_t *n_out);
+int qd_get_psi_run(qd_handle *h, int32_t run, double *psi_out);
+int qd_get_crp_run(qd_handle *h, int32_t run, double *crp_out);
+int qd_get_norms_run(qd_handle *h, int32_t run, double *norms_out, int32_t n);
+int qd_energies_run(qd_handle *h, int32_t run, double out4[4]);
 
 /* ---- setup helpers (the Matlab-side L4 of the reference) --------------- */
 

@@ -51,6 +51,8 @@ def lib():
         L.qdo_destroy.argtypes = [C.c_void_p]
         L.qdo_run_steps.argtypes = [C.c_void_p, C.c_int, dp, dp]
         L.qdo_run_steps.restype = C.c_int
+        L.qdo_energies.argtypes = [C.POINTER(_abi.QdData), dp]
+        L.qdo_energies.restype = C.c_int
         _o = L
     return _o
 
@@ -85,6 +87,15 @@ def oracle_time_evolution(data, norms=False, energies=False):
         raise RuntimeError(f"oracle failed: {rc}")
     _abi.from_c(d, data)
     return nb, eb
+
+
+def oracle_energies(data):
+    """(E_kin, E_rot, E_pot, E_total) of data.psi by the reference's formulas."""
+    out = np.zeros(4)
+    d = _abi.to_c(data)
+    if lib().qdo_energies(C.byref(d), _dp(out)) != 0:
+        raise RuntimeError("oracle energies failed")
+    return out
 
 
 def ref_time_evolution(data, verbose=False):

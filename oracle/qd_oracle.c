@@ -656,6 +656,38 @@ int qdo_time_evolution(qd_data *d, double *norms, double *energies)
   return rc;
 }
 
+/* Energies of the theta-space psi in d (no side effects on d->psi):
+ * kinetic_energy_for_psi (timeEvol.C:285-321), rotational_energy(1)
+ * (:323-360), potential_energy (:256-283); out = kin, rot, pot, total. */
+int qdo_energies(qd_data *d, double *out)
+{
+  qdo_state *s = qdo_create(d);
+  if (!s) return QD_ERR_INVALID;
+  const int n1 = s->n1, n2 = s->n2, nth = s->nth;
+  const long n12 = s->n12;
+  cplx *work = malloc(sizeof(cplx) * n12 * nth);
+  memcpy(work, s->psi, sizeof(cplx) * n12 * nth);
+  fft2d_batch(work, n1, n2, nth, -1);
+  double e = 0.0;
+  for (int k = 0; k < nth; k++) {
+    double ek = 0.0;
+    for (int j = 0; j < n2; j++)
+      for (int i = 0; i < n1; i++) {
+        cplx c = work[i + (long)n1 * (j + (long)n2 * k)];
+        ek += (c.re * c.re + c.im * c.im) * (s->psq2m1[i] + s->psq2m2[j]);
+      }
+    e += d->theta.w[k] * ek;
+  }
+  out[0] = e * d->r1.dr * d->r2.dr / (n1 * n2);
+  forward_legendre(s);
+  out[1] = rotational_energy_lpsi(s);
+  out[2] = potential_energy(s);
+  out[3] = out[0] + out[1] + out[2];
+  free(work);
+  qdo_destroy(s);
+  return QD_OK;
+}
+
 int qdo_num_threads(void)
 {
 #ifdef _OPENMP

@@ -32,6 +32,7 @@ int qdo_run_steps(qdo_state *s, int nsteps, double *norms, double *energies);
 double qdo_module_for_psi(qdo_state *s);
 int qdo_time_evolution(qd_data *d, double *norms, double *energies);
 int qdo_num_threads(void);
+int qdo_energies(qd_data *d, double *out4);
 
 #ifdef __cplusplus
 }

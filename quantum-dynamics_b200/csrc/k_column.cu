@@ -76,8 +76,12 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
   C *A = reinterpret_cast<C *>(smem);          // [nl][TP]   l-space tile
   C *B = A + p.nl * TP;                         // [nth][TP]  theta-space tile
   double *red = reinterpret_cast<double *>(B + p.nth * TP);
-  const long p0 = (long)blockIdx.x * TP;
-  C *lpsi = reinterpret_cast<C *>(p.lpsi);
+  const long tiles_per_run = (p.n12 + TP - 1) / TP;
+  const int run = (int)(blockIdx.x / tiles_per_run);
+  const long p0 = (long)(blockIdx.x % tiles_per_run) * TP;
+  C *lpsi = reinterpret_cast<C *>(p.lpsi) + (long)run * p.nl * p.n12;
+  const long zoff = (long)run * p.nth * p.n12;      // psi_z of this run
+  const long voff = (long)run * p.vrun;             // potential tables of this run
   const R *P = MatSel<R>::P(p);
   const R *WP = MatSel<R>::WP(p);
 
@@ -88,9 +92,9 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
       C v = mk((R)0, (R)0);
       if (q < p.n12) {
         const long g = (long)k * p.n12 + q;
-        double2 z = p.psi_z[g];
+        double2 z = p.psi_z[zoff + g];
         double s, c;
-        sincos(p.dt * p.pot[g], &s, &c);        // exp(-i V dt) = (c, -s)
+        sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
         double2 f = make_double2(c, -s);
         if (p.prestep) {
           // psi / sqrt(v) * v = psi * sqrt(v), principal branch
@@ -118,7 +122,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
 
   if (mode != COL_HEAD) {
     double nsum = 0.0;
-    C *surf = reinterpret_cast<C *>(p.surf);
+    C *surf = reinterpret_cast<C *>(p.surf) + (long)run * p.surf_nrows * p.nth * p.n1;
     for (int e = threadIdx.x; e < p.nth * TP; e += blockDim.x) {
       const int k = e / TP, t = e % TP;
       const long q = p0 + t;
@@ -133,13 +137,13 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
         nsum += p.w[k] * (z.x * z.x + z.y * z.y);
       }
       const long g = (long)k * p.n12 + q;
-      if (p.out_z) p.psi_z[g] = to_z(v);
-      if (mode == COL_MID) v = cmul(v, vphase(p, g, v));
+      if (p.out_z) p.psi_z[zoff + g] = to_z(v);
+      if (mode == COL_MID) v = cmul(v, vphase(p, voff + g, v));
       B[k * TP + t] = v;
     }
     if (p.norm_out) {
       const double s = block_sum(nsum, red);
-      if (threadIdx.x == 0) atomicAdd(p.norm_out, s);
+      if (threadIdx.x == 0) atomicAdd(p.norm_out + run, s);
     }
     if (mode == COL_TAIL) return;
     __syncthreads();
@@ -169,7 +173,7 @@ cudaError_t launch_column(const ColumnParams &p, int mode, cudaStream_t s)
     cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
-  const unsigned grid = (unsigned)((p.n12 + TP - 1) / TP);
+  const unsigned grid = (unsigned)((p.n12 + TP - 1) / TP * p.nruns);
   k_column<R><<<grid, 256, sm, s>>>(p, mode, TP);
   return cudaGetLastError();
 }

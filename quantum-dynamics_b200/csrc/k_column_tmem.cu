@@ -276,28 +276,33 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   float2 *surf = reinterpret_cast<float2 *>(p.surf);
   const float *lsrc = reinterpret_cast<const float *>(p.lpsi);
   float *ldst = reinterpret_cast<float *>(p.lpsi);
-  const long ntiles = (p.n12 + TPTS - 1) / TPTS;
+  const long tpr = (p.n12 + TPTS - 1) / TPTS;        // tiles per run
+  const long ntiles = tpr * p.nruns;
   const long n12 = p.n12;
   const int nl = p.nl, nth = p.nth;
   const int comp = is_im ? 1 : 0;
   const float2 *expv = p.expV32;
-  double nsum = 0.0;
 
   float a[H];
 #define QD_PREFETCH_A(tl)                                                              \
   do {                                                                                 \
-    const long qq = (tl) * TPTS + pt;                                                  \
+    const long rr = (tl) / tpr, qq = ((tl) - rr * tpr) * TPTS + pt;                    \
     const bool ok = (tl) < ntiles && qq < n12;                                         \
+    const float *src = lsrc + 2 * rr * nl * n12;                                       \
     _Pragma("unroll") for (int u = 0; u < H; u++) {                                    \
       const int l = c0 + u;                                                            \
-      a[u] = (ok && l < nl) ? __ldg(lsrc + 2 * ((long)l * n12 + qq) + comp) : 0.f;     \
+      a[u] = (ok && l < nl) ? __ldg(src + 2 * ((long)l * n12 + qq) + comp) : 0.f;      \
     }                                                                                  \
   } while (0)
   if (mode != COL_HEAD) QD_PREFETCH_A((long)blockIdx.x);
 
   for (long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const long q = tile * TPTS + pt;
+    const int run = (int)(tile / tpr);
+    const long q = (tile - (long)run * tpr) * TPTS + pt;
     const bool qok = q < n12;
+    const long voff = (long)run * p.vrun, zoff = (long)run * nth * n12;
+    float2 *surf_r = surf + (long)run * p.surf_nrows * nth * p.n1;
+    float *ldst_r = ldst + 2 * (long)run * nl * n12;
     const int j = qok ? (int)(q / p.n1) : 0, i = qok ? (int)(q % p.n1) : 0;
     float2 ev[H];
     float sc = 1.f;
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #pragma unroll
         for (int u = 0; u < H; u++) {
           const int k = c0 + u;
-          ev[u] = (qok && k < nth) ? __ldg(expv + (long)k * n12 + q) : make_float2(1.f, 0.f);
+          ev[u] = (qok && k < nth) ? __ldg(expv + voff + (long)k * n12 + q) : make_float2(1.f, 0.f);
         }
       }
       float n_l = 0.f;
@@ -367,8 +372,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           if (!is_im) {
             tsum += wk[k] * (re * re + im * im);
             if (qok && k < nth) {
-              if (flux_row) surf[((long)(j - p.surf_j0) * nth + k) * p.n1 + i] = make_float2(re, im);
-              if (p.out_z) p.psi_z[(long)k * n12 + q] = make_double2(re, im);
+              if (flux_row) surf_r[((long)(j - p.surf_j0) * nth + k) * p.n1 + i] = make_float2(re, im);
+              if (p.out_z) p.psi_z[zoff + (long)k * n12 + q] = make_double2(re, im);
             }
           }
           if (mode == COL_MID) {
@@ -385,9 +390,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           float val = 0.f;
           if (qok && k < nth) {
             const long g = (long)k * n12 + q;
-            const double2 z = p.psi_z[g];
+            const double2 z = p.psi_z[zoff + g];
             double s, c;
-            sincos(p.dt * p.pot[g], &s, &c);      // exp(-i V dt) = (c, -s)
+            sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
             double2 f = make_double2(c, -s);
             if (p.prestep) {                     // psi / sqrt(v) * v = psi * sqrt(v)
               double sh, ch;
@@ -405,7 +410,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
                     wk[c0 + u + 2] * v[2] * v[2] + wk[c0 + u + 3] * v[3] * v[3];
       }
     }
-    if (p.norm_out && qok && mode != COL_HEAD) nsum += (double)tsum;
+    if (p.norm_out && mode != COL_HEAD) {        // this tile's share of its run's norm
+      const double s = block_sum(qok ? (double)tsum : 0.0, red);
+      if (tid == 0) atomicAdd(p.norm_out + run, s);
+    }
     if (mode == COL_TAIL) {
       QD_PREFETCH_A(tile + gridDim.x);
       tc_fence_before();
@@ -450,7 +458,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #pragma unroll
       for (int x = 0; x < 4; x++) {
         const int l = c0 + u + x;
-        if (qok && l < nl) ldst[2 * ((long)l * n12 + q) + comp] = v[x] * sc2;
+        if (qok && l < nl) ldst_r[2 * ((long)l * n12 + q) + comp] = v[x] * sc2;
       }
     }
     tc_fence_before();
@@ -459,10 +467,6 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #undef QD_PREFETCH_A
 
   if (failed && lane == 0) atomicExch(t.status, 1);
-  if (p.norm_out) {
-    const double s = block_sum(nsum, red);
-    if (tid == 0) atomicAdd(p.norm_out, s);
-  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {

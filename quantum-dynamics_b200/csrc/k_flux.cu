@@ -19,7 +19,7 @@ __global__ void k_flux_prep(FluxParams p)
 {
   typedef typename Cplx<R>::T C;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < p.nth * p.n1) flux_point<C>(p, q);
+  if (q < p.nruns * p.nth * p.n1) flux_point<C>(p, q);
 }
 
 constexpr int EB = 8;          // energies per CTA
@@ -29,11 +29,13 @@ __global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
 {
   __shared__ double2 ph[EB][TMAX];
   const int e0 = blockIdx.y * EB;
+  const int run = blockIdx.z;
+  const double *energies = p.energies + (long)run * p.ne;
   for (int x = threadIdx.x; x < EB * p.nt; x += blockDim.x) {
     const int e = x / p.nt, t = x % p.nt;
     double2 c = make_double2(0.0, 0.0);
     if (e0 + e < p.ne) {
-      const double edt = p.energies[e0 + e] * p.dt;
+      const double edt = energies[e0 + e] * p.dt;
       double sn, cs;
       sincos(edt * (double)(p.t0 + t + 1), &sn, &cs);
       c = make_double2(p.dt * cs, p.dt * sn);
@@ -47,8 +49,9 @@ __global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
 #pragma unroll
   for (int e = 0; e < EB; e++) { a[e] = make_double2(0, 0); b[e] = make_double2(0, 0); }
   for (int t = 0; t < p.nt; t++) {
-    const double2 zp = p.ring_psi[(long)t * p.nq + q];
-    const double2 zg = p.ring_g[(long)t * p.nq + q];
+    const long o = ((long)t * p.nruns + run) * p.nq + q;
+    const double2 zp = p.ring_psi[o];
+    const double2 zg = p.ring_g[o];
 #pragma unroll
     for (int e = 0; e < EB; e++) {
       const double2 c = ph[e][t];
@@ -59,7 +62,7 @@ __global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
 #pragma unroll
   for (int e = 0; e < EB; e++) {
     if (e0 + e >= p.ne) break;
-    const long o = (long)(e0 + e) * p.nq + q;
+    const long o = ((long)run * p.ne + e0 + e) * p.nq + q;
     double2 f = p.fai[o], df = p.dfai[o];
     f.x += a[e].x; f.y += a[e].y; df.x += b[e].x; df.y += b[e].y;
     p.fai[o] = f; p.dfai[o] = df;
@@ -69,9 +72,9 @@ __global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
 __global__ void __launch_bounds__(256) k_crp(CrpParams p)
 {
   __shared__ double red[32];
-  const int e = blockIdx.x;
+  const int b = blockIdx.x;                    // run * ne + e
   const long nq = (long)p.nth * p.n1;
-  const double2 *f = p.fai + (long)e * nq, *df = p.dfai + (long)e * nq;
+  const double2 *f = p.fai + (long)b * nq, *df = p.dfai + (long)b * nq;
   double s = 0.0;
   for (long q = threadIdx.x; q < nq; q += blockDim.x) {
     const int k = (int)(q / p.n1);
@@ -79,7 +82,7 @@ __global__ void __launch_bounds__(256) k_crp(CrpParams p)
     s += p.w[k] * (a.x * b.y - a.y * b.x);   // Im(conj(phi) dphi)
   }
   s = block_sum(s, red);
-  if (threadIdx.x == 0) p.crp[e] = s / p.eta_sq[e] * p.dr1_mu2;
+  if (threadIdx.x == 0) p.crp[b] = s / p.eta_sq[b] * p.dr1_mu2;
 }
 
 }  // namespace
@@ -87,7 +90,7 @@ __global__ void __launch_bounds__(256) k_crp(CrpParams p)
 template <typename R>
 cudaError_t launch_flux_prep(const FluxParams &p, cudaStream_t s)
 {
-  const int nq = p.nth * p.n1;
+  const int nq = p.nruns * p.nth * p.n1;
   k_flux_prep<R><<<(nq + 255) / 256, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
@@ -98,13 +101,13 @@ cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 {
   if (p.nt <= 0) return cudaSuccess;
   if (p.nt > TMAX) return cudaErrorInvalidValue;
-  dim3 grid((p.nq + 255) / 256, (p.ne + EB - 1) / EB);
+  dim3 grid((p.nq + 255) / 256, (p.ne + EB - 1) / EB, p.nruns);
   k_flux_accum<<<grid, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_crp(const CrpParams &p, cudaStream_t s)
 {
-  k_crp<<<p.ne, 256, 0, s>>>(p);
+  k_crp<<<p.nruns * p.ne, 256, 0, s>>>(p);
   return cudaGetLastError();
 }

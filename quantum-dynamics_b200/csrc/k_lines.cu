@@ -35,14 +35,14 @@ __global__ void __launch_bounds__(256) k_rows(LineParams p, int dir)
   const int rb = p.rows_per_cta;
   C *bufA = reinterpret_cast<C *>(smem);
   C *bufB = bufA + rb * p.n1;
-  const int l = blockIdx.y;
+  const int sl = blockIdx.y, l = sl % p.nl;     // slice = run * nl + l
   const int j0 = blockIdx.x * rb;
   const int nrows = min(rb, p.n2 - j0);
-  C *slice = reinterpret_cast<C *>(p.lpsi) + (long)l * p.n12 + (long)j0 * p.n1;
+  C *slice = reinterpret_cast<C *>(p.lpsi) + (long)sl * p.n12 + (long)j0 * p.n1;
   const int nel = nrows * p.n1;
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     C v = slice[e];
-    if (dir < 0) v = cmul(v, Phase<R>::rot(p, l, j0 + e / p.n1, e % p.n1));
+    if (dir < 0 && !p.fft_only) v = cmul(v, Phase<R>::rot(p, l, j0 + e / p.n1, e % p.n1));
     bufA[e] = v;
   }
   __syncthreads();
@@ -63,10 +63,10 @@ __global__ void __launch_bounds__(256) k_cols(LineParams p)
   const int cb = p.cols_per_cta;
   C *bufA = reinterpret_cast<C *>(smem);
   C *bufB = bufA + cb * p.n2;
-  const int l = blockIdx.y;
+  const int sl = blockIdx.y;                     // slice = run * nl + l
   const int i0 = blockIdx.x * cb;
   const int ncols = min(cb, p.n1 - i0);
-  C *slice = reinterpret_cast<C *>(p.lpsi) + (long)l * p.n12;
+  C *slice = reinterpret_cast<C *>(p.lpsi) + (long)sl * p.n12;
   const int nel = ncols * p.n2;
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     const int j = e / ncols, c = e % ncols;
@@ -76,6 +76,13 @@ __global__ void __launch_bounds__(256) k_cols(LineParams p)
   const C *tw2 = reinterpret_cast<const C *>(p.tw2);
   C *res = smem_fft_lines<C>(bufA, bufB, p.pl2, ncols, 1, cb, true, tw2, -1);
   C *other = (res == bufA) ? bufB : bufA;
+  if (p.fft_only) {
+    for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+      const int j = e / ncols, c = e % ncols;
+      slice[(long)j * p.n1 + i0 + c] = res[j * cb + c];
+    }
+    return;
+  }
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     const int j = e / ncols, c = e % ncols;
     res[j * cb + c] = cmul(res[j * cb + c], Phase<R>::kin(p, j, i0 + c));
@@ -110,10 +117,10 @@ cudaError_t launch_lines(const LineParams &p0, cudaStream_t s)
   p.cols_per_cta = cb;
   const size_t sm_rows = 2 * sizeof(C) * (size_t)rb * p.n1;
   const size_t sm_cols = 2 * sizeof(C) * (size_t)cb * p.n2;
-  dim3 grows((p.n2 + rb - 1) / rb, p.nl), gcols((p.n1 + cb - 1) / cb, p.nl);
+  dim3 grows((p.n2 + rb - 1) / rb, p.nruns * p.nl), gcols((p.n1 + cb - 1) / cb, p.nruns * p.nl);
   k_rows<R><<<grows, 256, sm_rows, s>>>(p, -1);
   k_cols<R><<<gcols, 256, sm_cols, s>>>(p);
-  k_rows<R><<<grows, 256, sm_rows, s>>>(p, +1);
+  if (!p.fft_only) k_rows<R><<<grows, 256, sm_rows, s>>>(p, +1);
   return cudaGetLastError();
 }
 

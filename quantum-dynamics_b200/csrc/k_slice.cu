@@ -113,12 +113,12 @@ __global__ void __launch_bounds__(NT, 1) k_slice(LineParams p)
   float2 *sm = reinterpret_cast<float2 *>(smem4);
   const int n1 = p.n1, n2 = p.n2;
   const int rank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0;
-  if ((int)blockIdx.x >= p.nl * CL) {          // whole extra clusters: flux preparation
-    const int q = ((int)blockIdx.x - p.nl * CL) * NT + (int)threadIdx.x;
-    if (q < p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
+  if ((int)blockIdx.x >= p.nruns * p.nl * CL) {   // whole extra clusters: flux preparation
+    const int q = ((int)blockIdx.x - p.nruns * p.nl * CL) * NT + (int)threadIdx.x;
+    if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int l = blockIdx.x / CL;
+  const int sl = blockIdx.x / CL, l = sl % p.nl;   // slice = run * nl + l
   const int nrow = n2 / CL, ncol = n1 / CL;
   const int rs = n1 + n1 / 8;
   const int bufsz = slice_buf_elems(n1, n2, CL);
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(NT, 1) k_slice(LineParams p)
   for (int e = threadIdx.x; e < n1; e += NT) tw1[e] = gtw1[e];
   for (int e = threadIdx.x; e < n2; e += NT) tw2[e] = gtw2[e];
 
-  float2 *slice = reinterpret_cast<float2 *>(p.lpsi) + (long)l * p.n12;
+  float2 *slice = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * p.n12;
   const int j0 = rank * nrow;
   const LayRowPad rowlay{rs};
   // 1. own rows, Rot(dt/2)
@@ -285,19 +285,19 @@ __global__ void __launch_bounds__(NT, 2) k_slice_ct(LineParams p)
   extern __shared__ float4 smem4[];
   float2 *sm = reinterpret_cast<float2 *>(smem4);
   const int rank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0;
-  if ((int)blockIdx.x >= p.nl * CL) {          // whole extra clusters: flux preparation
-    const int q = ((int)blockIdx.x - p.nl * CL) * NT + (int)threadIdx.x;
-    if (q < p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
+  if ((int)blockIdx.x >= p.nruns * p.nl * CL) {   // whole extra clusters: flux preparation
+    const int q = ((int)blockIdx.x - p.nruns * p.nl * CL) * NT + (int)threadIdx.x;
+    if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int l = blockIdx.x / CL;
+  const int sl = blockIdx.x / CL, l = sl % p.nl;   // slice = run * nl + l
   float2 *tw1 = sm, *tw2 = sm + N1;
   float2 *X = tw2 + N2, *Y = X + BUF;
   const float2 *gtw1 = reinterpret_cast<const float2 *>(p.tw1);
   const float2 *gtw2 = reinterpret_cast<const float2 *>(p.tw2);
   for (int e = threadIdx.x; e < N1; e += NT) tw1[e] = gtw1[e];
   for (int e = threadIdx.x; e < N2; e += NT) tw2[e] = gtw2[e];
-  float2 *slice = reinterpret_cast<float2 *>(p.lpsi) + (long)l * (N1 * N2);
+  float2 *slice = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
   const float2 *rc1 = p.rc1 + l * N1, *rc2 = p.rc2 + l * N2;
   const int j0 = rank * NROW;
   const CRowPad<RS> rowlay;
@@ -378,7 +378,7 @@ template <int CL> cudaError_t launch_cl(const LineParams &p, cudaStream_t s)
                                        (int)sm);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(p.nl * CL + p.flux_ctas));
+  cfg.gridDim = dim3((unsigned)(p.nruns * p.nl * CL + p.flux_ctas));
   cfg.blockDim = dim3(NT);
   cfg.dynamicSmemBytes = sm;
   cfg.stream = s;

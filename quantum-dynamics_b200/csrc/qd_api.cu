@@ -105,7 +105,10 @@ bool all_finite(const double *a, size_t n)
 }  // namespace
 
 struct qd_handle {
-  qd_data *data = nullptr;
+  qd_data *data = nullptr;        // run 0 (holds the fields shared by the batch)
+  std::vector<qd_data *> runs;    // all runs of the batch
+  int nruns = 1;
+  long vrun = 0;                  // per-run stride of the potential tables (0 = shared)
   int prec = QD_PREC_FP64;
   int n1 = 0, n2 = 0, nth = 0, nl = 0;
   long n12 = 0;
@@ -271,6 +274,7 @@ FluxParams flux_params(qd_handle *h)
 {
   FluxParams f{};
   f.n1 = h->n1; f.nth = h->nth; f.npts = h->npts; f.h = h->h; f.surf = h->d_surf;
+  f.nruns = h->nruns;
   static const int den[] = {0, 2, 12, 60, 840, 2520};
   f.den_dx = den[h->h] * h->data->r2.dr;
   f.ring_psi = h->d_ring_psi; f.ring_g = h->d_ring_g; f.slot = h->flux_pending;
@@ -295,6 +299,7 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
 {
   ColumnParams p{};
   p.n1 = h->n1; p.n2 = h->n2; p.nth = h->nth; p.nl = h->nl; p.n12 = h->n12;
+  p.nruns = h->nruns; p.vrun = h->vrun;
   p.lpsi = h->d_lpsi; p.psi_z = h->d_psi_z;
   p.P = h->d_P; p.WP = h->d_WP; p.P32 = h->d_P32; p.WP32 = h->d_WP32;
   p.P32lo = h->d_P32lo; p.WP32lo = h->d_WP32lo;
@@ -330,6 +335,7 @@ int after_flux_prep(qd_handle *h)
   if (h->ring_fill == QD_RING) {
     AccumParams a{};
     a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+    a.nruns = h->nruns;
     a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
     a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
     TRY(prof_mark(h, -1));
@@ -355,6 +361,7 @@ LineParams line_params(qd_handle *h, bool f32)
 {
   LineParams p{};
   p.n1 = h->n1; p.n2 = h->n2; p.nl = h->nl; p.n12 = h->n12; p.lpsi = h->d_lpsi;
+  p.nruns = h->nruns;
   p.rot = h->d_rot; p.kin = h->d_kin;
   p.rc1 = h->d_rc1; p.rc2 = h->d_rc2; p.kc1 = h->d_kc1; p.kc2 = h->d_kc2;
   p.cluster = f32 ? h->slice_cluster : 0;
@@ -381,8 +388,9 @@ int tune_slice(qd_handle *h)
     return QD_OK;
   }
   void *scratch = nullptr;
-  CU(cudaMalloc(&scratch, sizeof(float2) * h->n12 * h->nl));
-  CU(cudaMemsetAsync(scratch, 0, sizeof(float2) * h->n12 * h->nl, h->st));
+  const size_t sbytes = sizeof(float2) * h->n12 * h->nl * h->nruns;
+  CU(cudaMalloc(&scratch, sbytes));
+  CU(cudaMemsetAsync(scratch, 0, sbytes, h->st));
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
@@ -420,7 +428,7 @@ template <typename R> int issue_lines(qd_handle *h)
   const bool fused_flux = p.cluster > 0 && h->flux_pending >= 0;
   if (fused_flux) {
     p.flux = flux_params(h);
-    const int nq = h->nth * h->n1;
+    const int nq = h->nth * h->n1 * h->nruns;
     const int ctas = (nq + 511) / 512;                // 512 threads per slice CTA
     p.flux_ctas = (ctas + p.cluster - 1) / p.cluster * p.cluster;
   }
@@ -442,6 +450,7 @@ int flush_accum(qd_handle *h)
   if (h->ring_fill == 0) return QD_OK;
   AccumParams a{};
   a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+  a.nruns = h->nruns;
   a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
   a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
   CU(launch_flux_accum(a, h->st));
@@ -457,6 +466,7 @@ int compute_crp(qd_handle *h)
   TRY(flush_accum(h));
   CrpParams c{};
   c.n1 = h->n1; c.nth = h->nth; c.ne = h->ne; c.w = h->d_w; c.eta_sq = h->d_eta;
+  c.nruns = h->nruns;
   c.dr1_mu2 = h->data->r1.dr / h->data->r2.mass;
   c.fai = h->d_fai; c.dfai = h->d_dfai; c.crp = h->d_crp;
   TRY(prof_mark(h, -1));
@@ -466,7 +476,7 @@ int compute_crp(qd_handle *h)
   return QD_OK;
 }
 
-template <typename R> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
+template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
                                    double *device_ms = nullptr)
 {
   if (n <= 0) {
@@ -487,34 +497,36 @@ template <typename R> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
       h->flush_bytes = flush_bytes;
     }
   }
-  if (h->norms_cap < n) {
+  const int R = h->nruns;                         // norms: [step][run]
+  if (h->norms_cap < n * R) {
     if (h->d_norms) cudaFree(h->d_norms);
     h->d_norms = nullptr;
-    CU(cudaMalloc(&h->d_norms, sizeof(double) * n));
-    h->norms_cap = n;
+    CU(cudaMalloc(&h->d_norms, sizeof(double) * n * R));
+    h->norms_cap = n * R;
   }
-  CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n, h->st));
+  CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n * R, h->st));
   for (int s = 0; s < n; s++) {
     if (timed && flush_bytes) CU(cudaMemsetAsync(h->d_flush, s & 0xff, flush_bytes, h->st));
     if (timed) CU(cudaEventRecord(h->events[2 * s], h->st));
     if (!h->started) {
-      TRY(issue_column<R>(h, COL_HEAD, false, nullptr, false));
+      TRY(issue_column<Real>(h, COL_HEAD, false, nullptr, false));
       h->started = true;
     } else if (s == 0 && h->last_finalized) {
-      TRY(issue_column<R>(h, COL_MID, false, nullptr, false));
+      TRY(issue_column<Real>(h, COL_MID, false, nullptr, false));
     } else {
-      TRY(issue_column<R>(h, COL_MID, h->do_crp, h->d_norms + (s - 1), false));
+      TRY(issue_column<Real>(h, COL_MID, h->do_crp, h->d_norms + (long)(s - 1) * R, false));
     }
-    TRY(issue_lines<R>(h));
+    TRY(issue_lines<Real>(h));
     h->steps++;
     if (timed && s < n - 1) CU(cudaEventRecord(h->events[2 * s + 1], h->st));
   }
-  TRY(issue_column<R>(h, COL_TAIL, h->do_crp, h->d_norms + (n - 1), false));
+  TRY(issue_column<Real>(h, COL_TAIL, h->do_crp, h->d_norms + (long)(n - 1) * R, false));
   h->last_finalized = true;
   TRY(compute_crp(h));
   if (timed) CU(cudaEventRecord(h->events[2 * n - 1], h->st));
-  std::vector<double> nb(n);
-  CU(cudaMemcpyAsync(nb.data(), h->d_norms, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+  std::vector<double> nb((size_t)n * R);
+  CU(cudaMemcpyAsync(nb.data(), h->d_norms, sizeof(double) * n * R, cudaMemcpyDeviceToHost,
+                     h->st));
   CU(cudaStreamSynchronize(h->st));
   TRY(prof_collect(h));
   TRY(check_status(h));
@@ -528,10 +540,11 @@ template <typename R> int propagate(qd_handle *h, int n, size_t flush_bytes = 0,
     *device_ms = tot;
   }
   const double scale = h->data->r1.dr * h->data->r2.dr;
-  for (int s = 0; s < n; s++) {
+  for (long s = 0; s < (long)n * R; s++) {
     const double v = nb[s] * scale;
     if (!std::isfinite(v))
-      return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d", h->steps - n + s + 1);
+      return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d (run %d)",
+                     h->steps - n + (int)(s / R) + 1, (int)(s % R));
     h->norms_host.push_back(v);
   }
   return QD_OK;
@@ -545,9 +558,50 @@ int upload(qd_handle *h, T *&dst, const T *src, size_t count)
   return QD_OK;
 }
 
-int create(const qd_data *d, qd_handle **out)
+bool same(const double *a, const double *b, size_t n)
 {
-  TRY(validate(d));
+  if (a == b) return true;
+  if (!a || !b) return false;
+  return std::memcmp(a, b, n * sizeof(double)) == 0;
+}
+
+// The runs of a batch share the grid, quadrature, time step, absorbers,
+// precision and flux settings; psi, pot, energies and eta_sq may differ.
+int validate_batch(const qd_data *runs, int n)
+{
+  if (!runs || n < 1) return set_err(QD_ERR_INVALID, "need at least one run");
+  for (int r = 0; r < n; r++) {
+    int rc = validate(&runs[r]);
+    if (rc) return set_err(rc, "run %d: %s", r, g_err.c_str());
+  }
+  const qd_data &a = runs[0];
+  for (int r = 1; r < n; r++) {
+    const qd_data &b = runs[r];
+    const bool ok =
+        b.r1.n == a.r1.n && b.r2.n == a.r2.n && b.r1.dr == a.r1.dr && b.r2.dr == a.r2.dr &&
+        b.r1.mass == a.r1.mass && b.r2.mass == a.r2.mass && same(b.r1.r, a.r1.r, a.r1.n) &&
+        same(b.r2.r, a.r2.r, a.r2.n) && b.theta.n == a.theta.n && b.theta.m == a.theta.m &&
+        same(b.theta.x, a.theta.x, a.theta.n) && same(b.theta.w, a.theta.w, a.theta.n) &&
+        same(b.theta.legendre, a.theta.legendre, (size_t)a.theta.n * (a.theta.m + 1)) &&
+        b.time.time_step == a.time.time_step && b.time.steps == a.time.steps &&
+        b.options.precision == a.options.precision &&
+        same(b.dump1.dump, a.dump1.dump, a.r1.n) && same(b.dump2.dump, a.dump2.dump, a.r2.n) &&
+        b.CRP.calculate_CRP == a.CRP.calculate_CRP &&
+        (!a.CRP.calculate_CRP ||
+         (b.CRP.n_dividing_surface == a.CRP.n_dividing_surface &&
+          b.CRP.n_gradient_points == a.CRP.n_gradient_points &&
+          b.CRP.n_energies == a.CRP.n_energies));
+    if (!ok)
+      return set_err(QD_ERR_INVALID, "run %d differs from run 0 in a field the batch shares "
+                     "(grids, theta, time, options.precision, dumps, CRP settings)", r);
+  }
+  return QD_OK;
+}
+
+int create(const qd_data *runs, int nruns, qd_handle **out)
+{
+  TRY(validate_batch(runs, nruns));
+  const qd_data *d = &runs[0];
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -556,6 +610,8 @@ int create(const qd_data *d, qd_handle **out)
   qd_handle *h = new qd_handle();
   *out = h;
   h->data = const_cast<qd_data *>(d);
+  h->nruns = nruns;
+  for (int r = 0; r < nruns; r++) h->runs.push_back(const_cast<qd_data *>(&runs[r]));
   h->prec = d->options.precision;
   h->n1 = d->r1.n; h->n2 = d->r2.n; h->nth = d->theta.n; h->nl = d->theta.m + 1;
   h->n12 = (long)h->n1 * h->n2;
@@ -575,7 +631,15 @@ int create(const qd_data *d, qd_handle **out)
 
   const long npt = h->n12 * h->nth;
   const bool f64 = h->prec == QD_PREC_FP64;
-  TRY(upload(h, h->d_pot, d->pot, npt));
+  // one potential table for the batch when all runs share pot, else one per run
+  bool shared_pot = true;
+  for (int r = 1; r < nruns && shared_pot; r++) shared_pot = same(runs[r].pot, d->pot, npt);
+  const int npot = shared_pot ? 1 : nruns;
+  h->vrun = shared_pot ? 0 : npt;
+  TRY(h->alloc(h->d_pot, npt * npot));
+  for (int r = 0; r < npot; r++)
+    CU(cudaMemcpyAsync(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt,
+                       cudaMemcpyHostToDevice, h->st));
   TRY(upload(h, h->d_w, d->theta.w, h->nth));
   TRY(upload(h, h->d_leg, d->theta.legendre, (size_t)h->nth * h->nl));
   TRY(h->alloc(h->d_P, (size_t)h->nth * h->nl));
@@ -612,19 +676,19 @@ int create(const qd_data *d, qd_handle **out)
                               h->d_P32, h->d_WP32, h->d_P32lo, h->d_WP32lo, h->st));
   g_launches++;
   if (f64) {
-    TRY(h->alloc(h->d_expV, npt));
+    TRY(h->alloc(h->d_expV, npt * npot));
     TRY(h->alloc(h->d_rot, (size_t)h->n12 * h->nl));
     TRY(h->alloc(h->d_kin, h->n12));
-    CU(launch_setup_tables_fp64(h->n1, h->n2, h->nth, h->nl, h->dt, h->d_pot, h->d_I1,
+    CU(launch_setup_tables_fp64(h->n1, h->n2, h->nth * npot, h->nl, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV, h->d_rot, h->d_kin,
                                 h->st));
   } else {
-    TRY(h->alloc(h->d_expV32, npt));
+    TRY(h->alloc(h->d_expV32, npt * npot));
     TRY(h->alloc(h->d_rc1, (size_t)h->nl * h->n1));
     TRY(h->alloc(h->d_rc2, (size_t)h->nl * h->n2));
     TRY(h->alloc(h->d_kc1, h->n1));
     TRY(h->alloc(h->d_kc2, h->n2));
-    CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth, h->nl, h->dt, h->d_pot, h->d_I1,
+    CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth * npot, h->nl, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV32, h->d_rc1, h->d_rc2,
                                 h->d_kc1, h->d_kc2, h->st));
   }
@@ -633,25 +697,34 @@ int create(const qd_data *d, qd_handle **out)
   void *lp = nullptr;
   {
     unsigned char *b = nullptr;
-    TRY(h->alloc(b, csz * h->n12 * h->nl));
+    TRY(h->alloc(b, csz * h->n12 * h->nl * nruns));
     lp = b;
   }
   h->d_lpsi = lp;
-  TRY(upload(h, h->d_psi_z, reinterpret_cast<const double2 *>(d->psi), npt));
+  TRY(h->alloc(h->d_psi_z, npt * nruns));
+  for (int r = 0; r < nruns; r++)
+    CU(cudaMemcpyAsync(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt,
+                       cudaMemcpyHostToDevice, h->st));
   if (h->do_crp) {
     const size_t nq = (size_t)h->nth * h->n1;
     unsigned char *b = nullptr;
-    TRY(h->alloc(b, csz * nq * (2 * h->h + 1)));
+    TRY(h->alloc(b, csz * nq * (2 * h->h + 1) * nruns));
     h->d_surf = b;
-    TRY(h->alloc(h->d_ring_psi, nq * QD_RING));
-    TRY(h->alloc(h->d_ring_g, nq * QD_RING));
-    TRY(h->alloc(h->d_fai, nq * h->ne));
-    TRY(h->alloc(h->d_dfai, nq * h->ne));
-    CU(cudaMemsetAsync(h->d_fai, 0, sizeof(double2) * nq * h->ne, h->st));
-    CU(cudaMemsetAsync(h->d_dfai, 0, sizeof(double2) * nq * h->ne, h->st));
-    TRY(upload(h, h->d_energies, d->CRP.energies, h->ne));
-    TRY(upload(h, h->d_eta, d->CRP.eta_sq, h->ne));
-    TRY(h->alloc(h->d_crp, h->ne));
+    TRY(h->alloc(h->d_ring_psi, nq * QD_RING * nruns));
+    TRY(h->alloc(h->d_ring_g, nq * QD_RING * nruns));
+    TRY(h->alloc(h->d_fai, nq * h->ne * nruns));
+    TRY(h->alloc(h->d_dfai, nq * h->ne * nruns));
+    CU(cudaMemsetAsync(h->d_fai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
+    CU(cudaMemsetAsync(h->d_dfai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
+    TRY(h->alloc(h->d_energies, (size_t)h->ne * nruns));
+    TRY(h->alloc(h->d_eta, (size_t)h->ne * nruns));
+    for (int r = 0; r < nruns; r++) {
+      CU(cudaMemcpyAsync(h->d_energies + (size_t)r * h->ne, runs[r].CRP.energies,
+                         sizeof(double) * h->ne, cudaMemcpyHostToDevice, h->st));
+      CU(cudaMemcpyAsync(h->d_eta + (size_t)r * h->ne, runs[r].CRP.eta_sq,
+                         sizeof(double) * h->ne, cudaMemcpyHostToDevice, h->st));
+    }
+    TRY(h->alloc(h->d_crp, (size_t)h->ne * nruns));
   }
   const char *path = getenv("QD_COLUMN_PATH");   // "simt" forces the SIMT column pass
   if (!f64 && !(path && std::string(path) == "simt")) {
@@ -665,28 +738,176 @@ int create(const qd_data *d, qd_handle **out)
   return QD_OK;
 }
 
-int get_psi(qd_handle *h, double *psi_out)
+// theta-space psi of every run into d_psi_z (B psi_l and the absorber)
+int stage_psi(qd_handle *h)
 {
+  if (!h->started) return QD_OK;              // d_psi_z still holds the input
+  if (h->prec == QD_PREC_FP64) TRY(issue_column<double>(h, COL_TAIL, false, nullptr, true));
+  else TRY(issue_column<float>(h, COL_TAIL, false, nullptr, true));
+  return QD_OK;
+}
+
+int get_psi(qd_handle *h, int run, double *psi_out)
+{
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
   const long npt = h->n12 * h->nth;
-  if (h->started) {
-    if (h->prec == QD_PREC_FP64) TRY(issue_column<double>(h, COL_TAIL, false, nullptr, true));
-    else TRY(issue_column<float>(h, COL_TAIL, false, nullptr, true));
-  }
-  CU(cudaMemcpyAsync(psi_out, h->d_psi_z, sizeof(double2) * npt, cudaMemcpyDeviceToHost, h->st));
+  TRY(stage_psi(h));
+  CU(cudaMemcpyAsync(psi_out, h->d_psi_z + (long)run * npt, sizeof(double2) * npt,
+                     cudaMemcpyDeviceToHost, h->st));
   CU(cudaStreamSynchronize(h->st));
   return QD_OK;
 }
 
-int get_crp(qd_handle *h, double *crp_out)
+int get_crp(qd_handle *h, int run, double *crp_out)
 {
   if (!h->do_crp) return set_err(QD_ERR_INVALID, "CRP.calculate_CRP is 0");
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
   if (!h->started) {
     for (int e = 0; e < h->ne; e++) crp_out[e] = 0.0;
     return QD_OK;
   }
   TRY(compute_crp(h));
-  CU(cudaMemcpyAsync(crp_out, h->d_crp, sizeof(double) * h->ne, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaMemcpyAsync(crp_out, h->d_crp + (long)run * h->ne, sizeof(double) * h->ne,
+                     cudaMemcpyDeviceToHost, h->st));
   CU(cudaStreamSynchronize(h->st));
+  return QD_OK;
+}
+
+// Energies of the current theta-space state of one run (timeEvol.C:256-360):
+// kinetic from the 2-D DFT of each l-slice, rotational and potential by
+// direct sums; all reductions in FP64.
+int energies(qd_handle *h, int run, double out4[4])
+{
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
+  TRY(stage_psi(h));
+  EnergyParams e{};
+  e.n1 = h->n1; e.n2 = h->n2; e.nth = h->nth; e.nl = h->nl; e.n12 = h->n12;
+  e.psi_z = h->d_psi_z + (long)run * h->n12 * h->nth;
+  e.pot = h->d_pot + (long)run * h->vrun;
+  e.w = h->d_w; e.P = h->d_P; e.WP = h->d_WP;
+  e.T1 = h->d_T1; e.T2 = h->d_T2; e.I1 = h->d_I1; e.I2 = h->d_I2;
+  e.tw1 = h->d_tw1_64; e.tw2 = h->d_tw2_64; e.pl1 = h->pl1; e.pl2 = h->pl2;
+  double *dsum = nullptr;
+  double2 *scratch = nullptr;
+  CU(cudaMalloc(&dsum, 3 * sizeof(double)));
+  cudaError_t err = cudaMalloc(&scratch, sizeof(double2) * h->n12 * h->nl);
+  if (err != cudaSuccess) { cudaFree(dsum); CU(err); }
+  e.sums = dsum;
+  e.scratch = scratch;
+  err = cudaMemsetAsync(dsum, 0, 3 * sizeof(double), h->st);
+  if (err == cudaSuccess) err = launch_energies(e, h->st);
+  double s[3] = {0, 0, 0};
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(s, dsum, sizeof s, cudaMemcpyDeviceToHost, h->st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(h->st);
+  cudaFree(dsum);
+  cudaFree(scratch);
+  CU(err);
+  g_launches += energies_launches();
+  const double dd = h->data->r1.dr * h->data->r2.dr;
+  out4[0] = s[0] * dd / ((double)h->n1 * h->n2);   // kinetic (unnormalised DFT)
+  out4[1] = s[1] * dd;                              // rotational
+  out4[2] = s[2] * dd;                              // potential
+  out4[3] = out4[0] + out4[1] + out4[2];
+  return QD_OK;
+}
+
+// ---- checkpoint / restore ----------------------------------------------------
+constexpr uint64_t CKPT_MAGIC = 0x31544b5044514251ull;   // file tag
+
+struct CkptHeader {
+  uint64_t magic;
+  int32_t prec, nruns, n1, n2, nth, nl, ne, npts;
+  int32_t steps, started, last_finalized, ring_fill, flux_pending;
+  int64_t acc_done;
+};
+
+int checkpoint(qd_handle *h, const char *path)
+{
+  CU(cudaStreamSynchronize(h->st));
+  CkptHeader hd{};
+  hd.magic = CKPT_MAGIC; hd.prec = h->prec; hd.nruns = h->nruns; hd.n1 = h->n1; hd.n2 = h->n2;
+  hd.nth = h->nth; hd.nl = h->nl; hd.ne = h->do_crp ? h->ne : 0; hd.npts = h->npts;
+  hd.steps = h->steps; hd.started = h->started; hd.last_finalized = h->last_finalized;
+  hd.ring_fill = h->ring_fill; hd.flux_pending = h->flux_pending; hd.acc_done = h->acc_done;
+  const size_t csz = h->prec == QD_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  std::vector<std::pair<const void *, size_t>> blocks;
+  const size_t nq = (size_t)h->nth * h->n1;
+  blocks.push_back({h->d_lpsi, csz * h->n12 * h->nl * h->nruns});
+  blocks.push_back({h->d_psi_z, sizeof(double2) * h->n12 * h->nth * h->nruns});
+  if (h->do_crp) {
+    blocks.push_back({h->d_surf, csz * nq * (2 * h->h + 1) * h->nruns});
+    blocks.push_back({h->d_ring_psi, sizeof(double2) * nq * QD_RING * h->nruns});
+    blocks.push_back({h->d_ring_g, sizeof(double2) * nq * QD_RING * h->nruns});
+    blocks.push_back({h->d_fai, sizeof(double2) * nq * h->ne * h->nruns});
+    blocks.push_back({h->d_dfai, sizeof(double2) * nq * h->ne * h->nruns});
+  }
+  FILE *f = fopen(path, "wb");
+  if (!f) return set_err(QD_ERR_IO, "cannot write \"%s\"", path);
+  bool ok = fwrite(&hd, sizeof hd, 1, f) == 1;
+  const uint64_t nnorm = h->norms_host.size();
+  ok = ok && fwrite(&nnorm, sizeof nnorm, 1, f) == 1;
+  ok = ok && (nnorm == 0 || fwrite(h->norms_host.data(), sizeof(double), nnorm, f) == nnorm);
+  std::vector<unsigned char> buf;
+  for (auto &b : blocks) {
+    if (!ok) break;
+    buf.resize(b.second);
+    if (cudaMemcpy(buf.data(), b.first, b.second, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      fclose(f);
+      return set_err(QD_ERR_CUDA, "checkpoint: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    ok = fwrite(buf.data(), 1, b.second, f) == b.second;
+  }
+  if (fclose(f) != 0) ok = false;
+  return ok ? QD_OK : set_err(QD_ERR_IO, "short write to \"%s\"", path);
+}
+
+int restore(qd_handle *h, const char *path)
+{
+  FILE *f = fopen(path, "rb");
+  if (!f) return set_err(QD_ERR_IO, "cannot read \"%s\"", path);
+  CkptHeader hd{};
+  if (fread(&hd, sizeof hd, 1, f) != 1 || hd.magic != CKPT_MAGIC) {
+    fclose(f);
+    return set_err(QD_ERR_IO, "\"%s\" is not a propagator checkpoint", path);
+  }
+  if (hd.prec != h->prec || hd.nruns != h->nruns || hd.n1 != h->n1 || hd.n2 != h->n2 ||
+      hd.nth != h->nth || hd.nl != h->nl || hd.ne != (h->do_crp ? h->ne : 0) ||
+      hd.npts != h->npts) {
+    fclose(f);
+    return set_err(QD_ERR_INVALID, "checkpoint \"%s\" was written for other sizes", path);
+  }
+  uint64_t nnorm = 0;
+  bool ok = fread(&nnorm, sizeof nnorm, 1, f) == 1 && nnorm < (1ull << 40);
+  std::vector<double> norms(ok ? nnorm : 0);
+  ok = ok && (nnorm == 0 || fread(norms.data(), sizeof(double), nnorm, f) == nnorm);
+  const size_t csz = h->prec == QD_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t nq = (size_t)h->nth * h->n1;
+  std::vector<std::pair<void *, size_t>> blocks;
+  blocks.push_back({h->d_lpsi, csz * h->n12 * h->nl * h->nruns});
+  blocks.push_back({h->d_psi_z, sizeof(double2) * h->n12 * h->nth * h->nruns});
+  if (h->do_crp) {
+    blocks.push_back({h->d_surf, csz * nq * (2 * h->h + 1) * h->nruns});
+    blocks.push_back({h->d_ring_psi, sizeof(double2) * nq * QD_RING * h->nruns});
+    blocks.push_back({h->d_ring_g, sizeof(double2) * nq * QD_RING * h->nruns});
+    blocks.push_back({h->d_fai, sizeof(double2) * nq * h->ne * h->nruns});
+    blocks.push_back({h->d_dfai, sizeof(double2) * nq * h->ne * h->nruns});
+  }
+  std::vector<unsigned char> buf;
+  for (auto &b : blocks) {
+    if (!ok) break;
+    buf.resize(b.second);
+    ok = fread(buf.data(), 1, b.second, f) == b.second;
+    if (ok && cudaMemcpy(b.first, buf.data(), b.second, cudaMemcpyHostToDevice) != cudaSuccess) {
+      fclose(f);
+      return set_err(QD_ERR_CUDA, "restore: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+  }
+  fclose(f);
+  if (!ok) return set_err(QD_ERR_IO, "\"%s\" is truncated", path);
+  h->steps = hd.steps; h->started = hd.started; h->last_finalized = hd.last_finalized;
+  h->ring_fill = hd.ring_fill; h->flux_pending = hd.flux_pending; h->acc_done = hd.acc_done;
+  h->norms_host = norms;
   return QD_OK;
 }
 
@@ -704,17 +925,29 @@ int qd_set_device(int32_t device)
   return QD_OK;
 }
 
-int qd_create(const qd_data *data, qd_handle **out)
+int qd_create_batch(const qd_data *runs, int32_t n_runs, qd_handle **out)
 {
   if (!out) return set_err(QD_ERR_INVALID, "out is NULL");
   *out = nullptr;
   qd_handle *h = nullptr;
-  int rc = create(data, &h);
+  int rc = create(runs, n_runs, &h);
   if (rc != QD_OK) {
     delete h;
     return rc;
   }
   *out = h;
+  return QD_OK;
+}
+
+int qd_create(const qd_data *data, qd_handle **out)
+{
+  return qd_create_batch(data, 1, out);
+}
+
+int qd_n_runs(qd_handle *h, int32_t *n_out)
+{
+  if (!h || !n_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  *n_out = h->nruns;
   return QD_OK;
 }
 
@@ -740,34 +973,48 @@ int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes, doubl
   return propagate<float>(h, n_steps, (size_t)flush_bytes, device_ms);
 }
 
-int qd_get_psi(qd_handle *h, double *psi_out)
+int qd_get_psi_run(qd_handle *h, int32_t run, double *psi_out)
 {
   if (!h || !psi_out) return set_err(QD_ERR_INVALID, "NULL argument");
-  return get_psi(h, psi_out);
+  return get_psi(h, run, psi_out);
 }
 
-int qd_get_crp(qd_handle *h, double *crp_out)
+int qd_get_psi(qd_handle *h, double *psi_out) { return qd_get_psi_run(h, 0, psi_out); }
+
+int qd_get_crp_run(qd_handle *h, int32_t run, double *crp_out)
 {
   if (!h || !crp_out) return set_err(QD_ERR_INVALID, "NULL argument");
-  return get_crp(h, crp_out);
+  return get_crp(h, run, crp_out);
 }
+
+int qd_get_crp(qd_handle *h, double *crp_out) { return qd_get_crp_run(h, 0, crp_out); }
 
 int qd_download(qd_handle *h)
 {
   if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
-  TRY(get_psi(h, h->data->psi));
-  if (h->do_crp && h->started) TRY(get_crp(h, h->data->CRP.CRP));
-  h->data->time.steps = h->steps;
+  for (int r = 0; r < h->nruns; r++) {
+    TRY(get_psi(h, r, h->runs[r]->psi));
+    if (h->do_crp && h->started) TRY(get_crp(h, r, h->runs[r]->CRP.CRP));
+    h->runs[r]->time.steps = h->steps;
+  }
+  return QD_OK;
+}
+
+int qd_get_norms_run(qd_handle *h, int32_t run, double *norms_out, int32_t n)
+{
+  if (!h || !norms_out || n < 0) return set_err(QD_ERR_INVALID, "bad argument");
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
+  const size_t avail = h->norms_host.size() / h->nruns;
+  if ((size_t)n > avail)
+    return set_err(QD_ERR_INVALID, "%d norms requested, %zu available", n, avail);
+  for (int32_t s = 0; s < n; s++)
+    norms_out[s] = h->norms_host[(avail - n + s) * h->nruns + run];
   return QD_OK;
 }
 
 int qd_get_norms(qd_handle *h, double *norms_out, int32_t n)
 {
-  if (!h || !norms_out || n < 0) return set_err(QD_ERR_INVALID, "bad argument");
-  if ((size_t)n > h->norms_host.size())
-    return set_err(QD_ERR_INVALID, "%d norms requested, %zu available", n, h->norms_host.size());
-  std::memcpy(norms_out, h->norms_host.data() + (h->norms_host.size() - n), sizeof(double) * n);
-  return QD_OK;
+  return qd_get_norms_run(h, 0, norms_out, n);
 }
 
 int qd_steps(qd_handle *h, int32_t *steps_out)
@@ -793,33 +1040,38 @@ int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written)
   return QD_OK;
 }
 
-int qd_energies(qd_handle *h, double out4[4])
+int qd_energies_run(qd_handle *h, int32_t run, double out4[4])
 {
   if (!h || !out4) return set_err(QD_ERR_INVALID, "NULL argument");
-  return set_err(QD_ERR_UNSUPPORTED, "qd_energies: not available in this build");
+  return energies(h, run, out4);
 }
+
+int qd_energies(qd_handle *h, double out4[4]) { return qd_energies_run(h, 0, out4); }
 
 int qd_checkpoint(qd_handle *h, const char *path)
 {
   if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
-  return set_err(QD_ERR_UNSUPPORTED, "qd_checkpoint: not available in this build");
+  return checkpoint(h, path);
 }
 
 int qd_restore(qd_handle *h, const char *path)
 {
   if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
-  return set_err(QD_ERR_UNSUPPORTED, "qd_restore: not available in this build");
+  return restore(h, path);
 }
 
-int qd_time_evolution(qd_data *data)
+int qd_time_evolution_batch(qd_data *runs, int32_t n_runs)
 {
+  if (!runs || n_runs < 1) return set_err(QD_ERR_INVALID, "need at least one run");
   qd_handle *h = nullptr;
-  TRY(qd_create(data, &h));
-  int rc = qd_propagate(h, data->time.total_steps);
+  TRY(qd_create_batch(runs, n_runs, &h));
+  int rc = qd_propagate(h, runs[0].time.total_steps);
   if (rc == QD_OK) rc = qd_download(h);
   qd_destroy(h);
   return rc;
 }
+
+int qd_time_evolution(qd_data *data) { return qd_time_evolution_batch(data, 1); }
 
 int qd_read_grids(const char *dir, int32_t n, double *x, double *w)
 {

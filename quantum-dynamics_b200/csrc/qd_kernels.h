@@ -18,9 +18,15 @@ enum ColumnMode {
   COL_TAIL = 2,   // lpsi -> B -> dump -> [flux, norm] (-> psi_z if out_z)
 };
 
+// Batches: nruns propagations on the same grid advance together.  Per run r:
+//   lpsi + r * nl * n12, psi_z + r * nth * n12, surf + r * nrows * nth * n1,
+//   expV / expV32 / pot + r * vrun (vrun = 0: one table shared by all runs),
+//   norm_out[r].
 struct ColumnParams {
   int n1, n2, nth, nl;
   long n12;
+  int nruns;
+  long vrun;               // per-run stride of the potential tables (0 = shared)
   void *lpsi;              // complex<R>
   double2 *psi_z;          // theta-space staging (HEAD in / TAIL out)
   const double *P;         // [nth][nl]  P_l(x_k)
@@ -39,28 +45,29 @@ struct ColumnParams {
   void *surf;              // complex<R> [nrows][nth][n1]
   int surf_j0, surf_nrows;
   const double *w;         // quadrature weights
-  double *norm_out;        // accumulate sum_k w_k |psi|^2 (null = skip)
+  double *norm_out;        // [nruns]: accumulate sum_k w_k |psi|^2 (null = skip)
   int out_z;               // TAIL: also write psi_z
 };
 
 struct FluxParams {
-  int n1, nth, npts, h;
-  const void *surf;        // complex<R> [2h+1][nth][n1]
+  int n1, nth, npts, h, nruns;
+  const void *surf;        // complex<R> [run][2h+1][nth][n1]
   double den_dx;           // den * dr2 (Gradient3.F divides by it)
-  double2 *ring_psi, *ring_g;
+  double2 *ring_psi, *ring_g;   // [slot][run][nth][n1]
   int slot;                // ring slot of this step
 };
 
-// psi_s and d psi_s / dr at grid point q = k*n1 + i of the dividing surface
-// from the 2h+1 captured rows: the central differences of Gradient3.F:31-167
-// with the integer coefficients summed in the same order, in FP64.
+// psi_s and d psi_s / dr at point Q = run*nq + k*n1 + i of the dividing
+// surface from the 2h+1 captured rows: the central differences of
+// Gradient3.F:31-167 with the integer coefficients summed in the same order,
+// in FP64.
 template <typename C>
-__device__ __forceinline__ void flux_point(const FluxParams &p, int q)
+__device__ __forceinline__ void flux_point(const FluxParams &p, int Q)
 {
-  // (offset m, coefficient) in Gradient3.F order for h = 1..5
   const int nq = p.nth * p.n1;
-  const C *s = reinterpret_cast<const C *>(p.surf);
+  const int run = Q / nq, q = Q - run * nq;
   const int h = p.h;
+  const C *s = reinterpret_cast<const C *>(p.surf) + (long)run * (2 * h + 1) * nq;
   const double2 v = to_z(s[(long)h * nq + q]);
   double gx = 0.0, gy = 0.0;
 #pragma unroll
@@ -81,7 +88,7 @@ __device__ __forceinline__ void flux_point(const FluxParams &p, int q)
     if (t == 0) { gx = c * dx; gy = c * dy; }   // first term exact (c * d, as Fortran's 0 + c*d)
     else { gx += c * dx; gy += c * dy; }
   }
-  const long o = (long)p.slot * nq + q;
+  const long o = ((long)p.slot * p.nruns + run) * nq + q;
   p.ring_psi[o] = v;
   p.ring_g[o] = make_double2(gx / p.den_dx, gy / p.den_dx);
 }
@@ -89,6 +96,7 @@ __device__ __forceinline__ void flux_point(const FluxParams &p, int q)
 struct LineParams {
   int n1, n2, nl;
   long n12;
+  int nruns;               // slices s = run * nl + l, all of the same n1 x n2
   void *lpsi;              // complex<R>, in place
   const double2 *rot;      // FP64: exp(-i l(l+1)(I1+I2) dt/2) [nl][n12]
   const double2 *kin;      // FP64: exp(-i(T1+T2)dt)/(n1 n2)    [n12]
@@ -105,11 +113,32 @@ struct LineParams {
   int cluster;             // fused slice kernel: CTAs per slice (0 = split kernels)
   FluxParams flux;         // fused slice kernel: flux preparation of the step ...
   int flux_ctas;           // ... by this many extra CTAs (0 = none)
+  int fft_only;            // split kernels: plain forward 2-D DFT, no phases
 };
 
+// energies of one run's theta-space psi (FP64): sums[0] kinetic (before the
+// dr1 dr2 / (n1 n2) factor), sums[1] rotational, sums[2] potential
+struct EnergyParams {
+  int n1, n2, nth, nl;
+  long n12;
+  const double2 *psi_z;    // [nth][n2][n1]
+  const double *pot;       // [nth][n2][n1]
+  const double *w, *P, *WP;
+  const double *T1, *T2, *I1, *I2;
+  const double2 *tw1, *tw2;
+  FftPlan pl1, pl2;
+  double2 *scratch;        // nth * n12
+  double *sums;            // 3
+};
+cudaError_t launch_energies(const EnergyParams &e, cudaStream_t s);
+int energies_launches();
+
+// per run r: energies/eta_sq/crp + r * ne, fai/dfai + r * ne * nq,
+// ring slot t of run r at (t * nruns + r) * nq
 struct AccumParams {
   int nq;                  // nth * n1
   int ne;
+  int nruns;
   int nt;                  // steps in this chunk
   long t0;                 // accumulations done before this chunk
   double dt;
@@ -119,7 +148,7 @@ struct AccumParams {
 };
 
 struct CrpParams {
-  int n1, nth, ne;
+  int n1, nth, ne, nruns;
   const double *w, *eta_sq;
   double dr1_mu2;
   const double2 *fai, *dfai;

@@ -172,6 +172,13 @@ def lib():
         "qd_kernel_times": (C.c_int, [H, c_double_p, C.c_int32, P(C.c_int32)]),
         "qd_checkpoint": (C.c_int, [H, C.c_char_p]),
         "qd_restore": (C.c_int, [H, C.c_char_p]),
+        "qd_create_batch": (C.c_int, [P(QdData), C.c_int32, P(H)]),
+        "qd_time_evolution_batch": (C.c_int, [P(QdData), C.c_int32]),
+        "qd_n_runs": (C.c_int, [H, P(C.c_int32)]),
+        "qd_get_psi_run": (C.c_int, [H, C.c_int32, c_double_p]),
+        "qd_get_crp_run": (C.c_int, [H, C.c_int32, c_double_p]),
+        "qd_get_norms_run": (C.c_int, [H, C.c_int32, c_double_p, C.c_int32]),
+        "qd_energies_run": (C.c_int, [H, C.c_int32, c_double_p]),
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
     }

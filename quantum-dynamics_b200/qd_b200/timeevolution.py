@@ -6,9 +6,10 @@ common/TimeEvolutionMex.C:18-78) -- fields r1, r2, theta, pot, psi, time,
 options, dump1, dump2, CRP -- and, like them, propagate
 `time.total_steps` steps updating `psi`, `time.steps` and `CRP.CRP` in place.
 Both run on the GPU through libqd.so's C ABI; errors the reference reports
-through insist()/mexErrMsgTxt raise `QdError` here.
+through insist()/mexErrMsgTxt raise `QdError` here.  Given a list of structs
+they propagate them as one batch (same grid; see qd_create_batch).
 
-`Propagator` keeps the wavepacket on the device across calls (the C ABI's
+`Propagator` keeps the wavepacket(s) on the device across calls (the C ABI's
 handle API).
 """
 import ctypes as C
@@ -31,12 +32,24 @@ def _check_layout(data):
                          "(the (m+1) x n Matlab matrix, column-major)")
 
 
+def _c_runs(runs):
+    """ctypes array of QdData over a list of structs (keeps the views alive)."""
+    for d in runs:
+        _check_layout(d)
+    views = [_abi.to_c(d) for d in runs]
+    arr = (_abi.QdData * len(runs))(*views)
+    arr._views = views
+    return arr
+
+
 def TimeEvolutionMexCUDA(data):
-    """Propagate `data.time.total_steps` steps on the GPU, in place."""
-    _check_layout(data)
-    d = _abi.to_c(data)
-    check(lib().qd_time_evolution(C.byref(d)))
-    _abi.from_c(d, data)
+    """Propagate `time.total_steps` steps on the GPU, in place.  `data` is one
+    struct or a list of structs propagated together as a batch."""
+    runs = data if isinstance(data, (list, tuple)) else [data]
+    arr = _c_runs(runs)
+    check(lib().qd_time_evolution_batch(arr, len(runs)))
+    for d, c in zip(runs, arr):
+        _abi.from_c(c, d)
     return data
 
 
@@ -45,14 +58,19 @@ TimeEvolutionMex = TimeEvolutionMexCUDA
 
 
 class Propagator:
-    """Device-resident propagation (qd_create / qd_propagate / qd_download)."""
+    """Device-resident propagation of one struct or a batch of structs
+    (qd_create_batch / qd_propagate / qd_download)."""
 
     def __init__(self, data):
-        _check_layout(data)
-        self.data = data
-        self._c = _abi.to_c(data)
+        self.runs = list(data) if isinstance(data, (list, tuple)) else [data]
+        self.data = self.runs[0]
+        self._c = _c_runs(self.runs)
         self._h = C.c_void_p()
-        check(lib().qd_create(C.byref(self._c), C.byref(self._h)))
+        check(lib().qd_create_batch(self._c, len(self.runs), C.byref(self._h)))
+
+    @property
+    def n_runs(self):
+        return len(self.runs)
 
     def propagate(self, n_steps):
         check(lib().qd_propagate(self._h, int(n_steps)))
@@ -65,19 +83,20 @@ class Propagator:
         check(lib().qd_propagate_timed(self._h, int(n_steps), int(flush_bytes), C.byref(ms)))
         return ms.value
 
-    def psi(self):
-        out = np.empty_like(self.data.psi)
-        check(lib().qd_get_psi(self._h, out.ctypes.data_as(_abi.c_double_p)))
+    def psi(self, run=0):
+        out = np.empty_like(self.runs[run].psi)
+        check(lib().qd_get_psi_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p)))
         return out
 
-    def crp(self):
-        out = np.empty(int(self.data.CRP.n_energies))
-        check(lib().qd_get_crp(self._h, out.ctypes.data_as(_abi.c_double_p)))
+    def crp(self, run=0):
+        out = np.empty(int(self.runs[run].CRP.n_energies))
+        check(lib().qd_get_crp_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p)))
         return out
 
-    def norms(self, n):
+    def norms(self, n, run=0):
         out = np.empty(int(n))
-        check(lib().qd_get_norms(self._h, out.ctypes.data_as(_abi.c_double_p), int(n)))
+        check(lib().qd_get_norms_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p),
+                                     int(n)))
         return out
 
     @property
@@ -87,14 +106,16 @@ class Propagator:
         return s.value
 
     def download(self):
-        """Write psi, time.steps and CRP.CRP back into `data`."""
+        """Write psi, time.steps and CRP.CRP back into the struct(s)."""
         check(lib().qd_download(self._h))
-        self.data.time.steps = self.steps
+        for d in self.runs:
+            d.time.steps = self.steps
         return self.data
 
-    def energies(self):
+    def energies(self, run=0):
+        """(E_kin, E_rot, E_pot, E_total) of the current wavepacket, hartree."""
         out = np.empty(4)
-        check(lib().qd_energies(self._h, out.ctypes.data_as(_abi.c_double_p)))
+        check(lib().qd_energies_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p)))
         return out
 
     def checkpoint(self, path):

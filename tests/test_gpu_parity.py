@@ -199,3 +199,87 @@ def test_fp32_c1_full_run_within_pe_budget():
     dP = np.abs(out[QD_PREC_FP32][0] - out[QD_PREC_FP64][0])[sel].max()
     assert dP < FP32_CRP_ABS, dP
     assert np.abs(out[QD_PREC_FP32][1] - out[QD_PREC_FP64][1]).max() < 1e-3
+
+
+def _three_runs(prec, steps=25):
+    # same F + H2 grid, different initial states (v0, j0) -> different psi,
+    # energies and eta^2; the potential table is shared
+    runs = []
+    for v0, j0 in ((0, 0), (0, 2), (1, 0)):
+        d = S.build_case("f+h2", 48, 40, 24, m=23, total_steps=steps, n_energies=13,
+                         n_gradient_points=7, j0=j0, v0=v0, precision=prec)
+        runs.append(d)
+    for d in runs[1:]:
+        d.pot = runs[0].pot
+    return runs
+
+
+@pytest.mark.parametrize("prec", [QD_PREC_FP64, QD_PREC_FP32])
+def test_batch_equals_individual_runs(prec):
+    runs = _three_runs(prec)
+    single = [S.copy_case(d) for d in runs]
+    batch = [S.copy_case(d) for d in runs]
+    for d in single:
+        TimeEvolutionMexCUDA(d)
+    TimeEvolutionMexCUDA(batch)
+    tol = 1e-12 if prec == QD_PREC_FP64 else 1e-6
+    for a, b in zip(single, batch):
+        assert b.time.steps == a.time.steps == 25
+        assert rel(b.psi, a.psi) < tol
+        assert np.abs(b.CRP.CRP - a.CRP.CRP).max() < tol * max(1.0, np.abs(a.CRP.CRP).max())
+
+
+def test_batch_fp64_matches_oracle_per_run():
+    runs = _three_runs(QD_PREC_FP64, steps=20)
+    with Propagator([S.copy_case(d) for d in runs]) as p:
+        p.propagate(20)
+        got = [(p.psi(r), p.crp(r), p.norms(20, r)) for r in range(3)]
+    for r, d in enumerate(runs):
+        a = S.copy_case(d)
+        norms, _ = O.oracle_time_evolution(a, norms=True)
+        assert rel(got[r][0], a.psi) < FP64_PSI_REL
+        assert np.abs(got[r][1] - a.CRP.CRP).max() < FP64_CRP_ABS
+        assert np.abs(got[r][2] - norms).max() < FP64_PSI_REL
+
+
+@pytest.mark.parametrize("prec,tol", [(QD_PREC_FP64, 1e-10), (QD_PREC_FP32, 1e-4)])
+def test_energies_match_oracle(prec, tol):
+    base = S.build_case("f+h2", 48, 40, 24, m=23, total_steps=15, n_energies=5,
+                        precision=prec)
+    a = S.copy_case(base)
+    O.oracle_time_evolution(a)
+    e_ref = O.oracle_energies(a)
+    with Propagator(S.copy_case(base)) as p:
+        p.propagate(15)
+        e = p.energies()
+    assert np.abs(e - e_ref).max() < tol * np.abs(e_ref).max(), (e, e_ref)
+
+
+@pytest.mark.parametrize("prec", [QD_PREC_FP64, QD_PREC_FP32])
+def test_checkpoint_restore_resumes_exactly(prec, tmp_path):
+    base = S.build_case("h+h2", 32, 32, 16, m=15, total_steps=40, n_energies=9,
+                        n_gradient_points=5, precision=prec)
+    path = tmp_path / "state.qdck"
+    with Propagator(S.copy_case(base)) as p:
+        p.propagate(17)
+        p.checkpoint(path)
+        p.propagate(23)
+        psi_a, crp_a = p.psi(), p.crp()
+    with Propagator(S.copy_case(base)) as q:
+        q.restore(path)
+        assert q.steps == 17
+        q.propagate(23)
+        psi_b, crp_b = q.psi(), q.crp()
+        assert q.steps == 40
+    assert np.array_equal(psi_a, psi_b)
+    assert np.array_equal(crp_a, crp_b)
+
+
+@pytest.mark.parametrize("prec,tol", [(QD_PREC_FP64, 1e-10), (QD_PREC_FP32, 1e-5)])
+def test_energies_harmonic_oscillator_kat(prec, tol):
+    from test_oracle import ho_state
+    d = ho_state()
+    d.options.precision = prec
+    with Propagator(d) as p:
+        e = p.energies()
+    assert abs(e[0] - 0.5) < tol and abs(e[2] - 0.5) < tol and abs(e[1]) < tol

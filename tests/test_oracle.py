@@ -141,3 +141,37 @@ def test_oracle_unitary_without_absorbers():
     norms, _ = O.oracle_time_evolution(base, norms=True)
     # with n_l = n_theta the Legendre pair is unitary, so is every phase and FFT
     assert np.abs(norms - norms[0]).max() < 1e-12 * norms[0]
+
+
+def ho_state(n=96, nth=4):
+    """A 2-D harmonic-oscillator ground state (m = 1, omega = 1) in (R, r),
+    independent of theta: the two-dimensional form of the known-answer check
+    in common/fftwinterface.C:132-188 (<T> = <V> = 0.25 per dimension)."""
+    from qd_b200.systems import Struct
+    g = np.linspace(1.0, 21.0, n)
+    dx = g[1] - g[0]
+    x, w = S.gauss_legendre(nth)
+    f = math.pi ** -0.25 * np.exp(-0.5 * (g - 11.0) ** 2)
+    psi = (math.sqrt(0.5) * f[None, None, :] * f[None, :, None]
+           * np.ones((nth, 1, 1))).astype(np.complex128)
+    pot = (0.5 * (g[None, None, :] - 11.0) ** 2 + 0.5 * (g[None, :, None] - 11.0) ** 2
+           ) * np.ones((nth, 1, 1))
+    r1 = Struct(n=n, r=g.copy(), dr=dx, mass=1.0, r0=0.0, k0=0.0, delta=0.0)
+    r2 = Struct(n=n, r=g.copy(), dr=dx, mass=1.0, r0=0.0, k0=0.0, delta=0.0)
+    theta = Struct(n=nth, m=nth - 1, x=x, w=w, legendre=S.legendre_p2(nth - 1, x))
+    return Struct(r1=r1, r2=r2, theta=theta, pot=np.ascontiguousarray(pot),
+                  psi=np.ascontiguousarray(psi),
+                  time=Struct(total_steps=1, time_step=0.01, steps=0),
+                  options=Struct(wave_to_matlab=None, test_name="ho", precision=0,
+                                 steps_to_copy_psi_from_device_to_host=0),
+                  dump1=Struct(dump=None), dump2=Struct(dump=None),
+                  CRP=Struct(n_dividing_surface=1, n_gradient_points=3, n_energies=1,
+                             calculate_CRP=0, energies=np.zeros(1), eta_sq=np.ones(1),
+                             CRP=np.zeros(1)))
+
+
+def test_oracle_energies_harmonic_oscillator_kat():
+    e = O.oracle_energies(ho_state())
+    assert abs(e[0] - 0.5) < 1e-10      # kinetic, two dimensions
+    assert abs(e[1]) < 1e-12            # l = 0 only
+    assert abs(e[2] - 0.5) < 1e-10      # potential
