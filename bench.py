@@ -1,7 +1,7 @@
 """Benchmark: grid-point * steps / s of the split-operator propagator.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0]
+                    [--workload c1|c0|c2j0]
 
 Workload (default c1): F + H2, J = 0, extended-LEPS surface on a
 128 x 128 x 64 Jacobi grid (n_l = 64), complex64 wavefunction with the
@@ -41,6 +41,22 @@ METRIC = "grid-pt*steps/s"
 FLUSH_BYTES = 256 << 20
 
 
+def as_runs(data):
+    """A workload is one run (a data struct) or a batch (a list of them)."""
+    return list(data) if isinstance(data, (list, tuple)) else [data]
+
+
+def grid_points(data):
+    """Grid points of all runs of a workload."""
+    return sum(int(d.r1.n) * int(d.r2.n) * int(d.theta.n) for d in as_runs(data))
+
+
+def copy_workload(data):
+    from qd_b200 import systems as S
+    runs = [S.copy_case(d) for d in as_runs(data)]
+    return runs if isinstance(data, (list, tuple)) else runs[0]
+
+
 def load_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -59,6 +75,10 @@ def build_workload(name, precision):
     elif name == "c0":
         data = S.case_c0(precision=precision)
         desc = "H+H2 J=0 extended-LEPS, 64x64x40 Jacobi grid, n_l=39, dt=10 au, 241 energies"
+    elif name == "c2j0":
+        data = S.case_c2_j0(64, precision=precision)
+        desc = ("batch of 64 F+H2 J=0 propagations, 128x96x64 Jacobi grid, n_l=64, dt=10 au, "
+                "initial (v0,j0) cycling (0,0),(0,1),(0,2),(1,0), 241 energies each")
     else:
         raise SystemExit(f"unknown workload {name}")
     return data, desc
@@ -130,7 +150,8 @@ def cpu_reference_rate(data, max_seconds, steps_cap=None):
     os.environ["OMP_NUM_THREADS"] = str(threads)
     use_ref = O.ref_available()
     run = O.ref_time_evolution if use_ref else O.oracle_time_evolution
-    d = S.copy_case(data)
+    runs = as_runs(data)
+    d = S.copy_case(runs[0])
     d.options.precision = 0
     d.time.total_steps = 1
     t0 = time.perf_counter()
@@ -143,9 +164,10 @@ def cpu_reference_rate(data, max_seconds, steps_cap=None):
     t0 = time.perf_counter()
     run(d)
     dt = time.perf_counter() - t0
-    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    pts = grid_points(runs[0])
+    what = "the same workload" if len(runs) == 1 else f"run 0 of the {len(runs)}-run batch"
     info = {"kind": "reference" if use_ref else "port", "cores": threads,
-            "sample": f"{n} steps (after 1 warm-up step) of the same workload in FP64, "
+            "sample": f"{n} steps (after 1 warm-up step) of {what} in FP64, "
                       f"per-step energies/norm/CRP diagnostics included as in the reference"}
     return pts * n / dt, info
 
@@ -173,7 +195,7 @@ def run_reference(args):
     data, desc = build_workload(args.workload, 0)
     budget = float(os.environ.get("QD_REF_SECONDS", "60"))
     rate, info = cpu_reference_rate(data, budget)
-    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    pts = grid_points(data)
     info["value"] = rate
     info["unit"] = METRIC
     line = {"metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
@@ -197,11 +219,12 @@ def run_ours(args):
     set_device(local)
     prec = QD_PREC_FP64 if args.fp64 else QD_PREC_FP32
     data, desc = build_workload(args.workload, prec)
-    pts = int(data.r1.n) * int(data.r2.n) * int(data.theta.n)
+    runs = as_runs(data)
+    pts = grid_points(data)
     K, W = args.steps, args.warmup
 
     # --- device-resident throughput -------------------------------------------------
-    d = S.copy_case(data)
+    d = copy_workload(data)
     with Propagator(d) as p:
         p.propagate_timed(W, FLUSH_BYTES)
         if dist:
@@ -232,9 +255,10 @@ def run_ours(args):
     value = pts * K * world / (t_max * 1e-3)
 
     # --- end to end through the drop-in entry point -------------------------------
-    e = S.copy_case(data)
-    e.time.total_steps = K
-    e.time.steps = 0
+    e = copy_workload(data)
+    for r in as_runs(e):
+        r.time.total_steps = K
+        r.time.steps = 0
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -245,8 +269,8 @@ def run_ours(args):
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    h2d = data.pot.nbytes + data.psi.nbytes + data.theta.legendre.nbytes
-    d2h = data.psi.nbytes + data.CRP.CRP.nbytes
+    h2d = sum(r.pot.nbytes + r.psi.nbytes for r in runs) + runs[0].theta.legendre.nbytes
+    d2h = sum(r.psi.nbytes + r.CRP.CRP.nbytes for r in runs)
     e2e = {"value": pts * K * world / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
            "seconds": e2e_s, "entry_point": "qd_time_evolution (TimeEvolutionMexCUDA)"}
@@ -258,7 +282,9 @@ def run_ours(args):
 
     # --- roofline of the dominant kernel class ----------------------------------------
     peak, peak_kind = load_peaks()
-    nl, nth, n12 = int(data.theta.m) + 1, int(data.theta.n), int(data.r1.n) * int(data.r2.n)
+    r0 = runs[0]
+    nl, nth = int(r0.theta.m) + 1, int(r0.theta.n)
+    n12 = int(r0.r1.n) * int(r0.r2.n) * len(runs)
     cb = 16 if args.fp64 else 8        # bytes per complex
     alg = {  # algorithmic bytes per launch group
         "column": n12 * (2 * nl * cb + nth * (16 if args.fp64 else 4)),
@@ -306,7 +332,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2j0"])
     ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -336,6 +336,35 @@ def case_c1(**kw):
     return build_case("f+h2", 128, 128, 64, m=63, **kw)
 
 
+def batch_cases(base, states):
+    """Runs of one batch: `base` with the initial diatomic state (v0, j0)
+    replaced per run (psi, CRP.energies, CRP.eta_sq); grid and potential are
+    shared (the same pot array)."""
+    pes = leps_f_h2() if base.system == "f+h2" else leps_h_h2()
+    e_coll = base.CRP.energies - base.CRP.eDiatomic
+    runs = []
+    for v0, j0 in states:
+        d = copy_case(base)
+        d.psi, e_vj, _ = init_wavepacket(d.r1, d.r2, d.theta, j0, v0, pes.diatom)
+        d.CRP.eDiatomic = e_vj
+        d.CRP.energies = np.ascontiguousarray(e_coll + e_vj)
+        d.CRP.eta_sq = eta_sq(d.r1, e_coll)
+        d.CRP.CRP = np.zeros(int(d.CRP.n_energies))
+        d.pot = base.pot
+        runs.append(d)
+    return runs
+
+
+def case_c2_j0(n_runs=64, **kw):
+    """F + H2 J = 0 batch on the 128 x 96 x 64 grid (n_l = 64): n_runs
+    propagations with initial states cycling over (v0, j0) = (0,0), (0,1),
+    (0,2), (1,0)."""
+    kw.setdefault("total_steps", 10000)
+    base = build_case("f+h2", 128, 96, 64, m=63, r=(0.4, 8.0), **kw)
+    states = [((0, 0), (0, 1), (0, 2), (1, 0))[i % 4] for i in range(n_runs)]
+    return batch_cases(base, states)
+
+
 def copy_case(data):
     """Deep copy of the arrays that a propagation mutates (psi, CRP, time)."""
     import copy
