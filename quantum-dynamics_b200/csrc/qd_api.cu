@@ -790,7 +790,7 @@ int energies(qd_handle *h, int run, double out4[4])
   double *dsum = nullptr;
   double2 *scratch = nullptr;
   CU(cudaMalloc(&dsum, 3 * sizeof(double)));
-  cudaError_t err = cudaMalloc(&scratch, sizeof(double2) * h->n12 * h->nl);
+  cudaError_t err = cudaMalloc(&scratch, sizeof(double2) * h->n12 * h->nth);
   if (err != cudaSuccess) { cudaFree(dsum); CU(err); }
   e.sums = dsum;
   e.scratch = scratch;

@@ -242,9 +242,10 @@ def test_batch_fp64_matches_oracle_per_run():
         assert np.abs(got[r][2] - norms).max() < FP64_PSI_REL
 
 
+@pytest.mark.parametrize("m", [23, 17])          # n_l = n_theta and n_l < n_theta
 @pytest.mark.parametrize("prec,tol", [(QD_PREC_FP64, 1e-10), (QD_PREC_FP32, 1e-4)])
-def test_energies_match_oracle(prec, tol):
-    base = S.build_case("f+h2", 48, 40, 24, m=23, total_steps=15, n_energies=5,
+def test_energies_match_oracle(prec, tol, m):
+    base = S.build_case("f+h2", 48, 40, 24, m=m, total_steps=15, n_energies=5,
                         precision=prec)
     a = S.copy_case(base)
     O.oracle_time_evolution(a)
