@@ -215,6 +215,27 @@ int qd_get_crp_run(qd_handle *h, int32_t run, double *crp_out);
 int qd_get_norms_run(qd_handle *h, int32_t run, double *norms_out, int32_t n);
 int qd_energies_run(qd_handle *h, int32_t run, double out4[4]);
 
+/* ---- energies without allocation ----------------------------------------
+ * No counterpart in the reference.  Same result as qd_energies_run, but the
+ * kinetic-energy DFT scratch (n1*n2*n_theta complex128 values) and the three
+ * FP64 sums live in one static device array instead of cudaMalloc'd memory.
+ * It serves callers that cannot allocate device memory at diagnostic time:
+ * a host that sized a large batch to fill the device and handed the rest to
+ * its own memory pool (a cudaMalloc would fail with out-of-memory in the
+ * middle of the run), and monitors that sample energies often while other
+ * streams keep working (cudaFree synchronises the whole device, so the
+ * allocating call stalls them every time).
+ *   - limit: n1*n2*n_theta of one run <= QD_ENERGIES_NOALLOC_MAX_POINTS
+ *     (16 MiB of scratch); larger grids get QD_ERR_INVALID and nothing runs;
+ *   - the first call on each device looks up the scratch address
+ *     (cudaGetSymbolAddress, which may load the module holding the array):
+ *     make that first call before any stream capture;
+ *   - the scratch is shared by every handle on the device, so calls that
+ *     overlap in time (two host threads, or two streams) race on it;
+ *   - the sums are cleared on the handle's stream at every call. */
+#define QD_ENERGIES_NOALLOC_MAX_POINTS 1048576
+int qd_energies_noalloc(qd_handle *h, int32_t run, double out4[4]);
+
 /* ---- setup helpers (the Matlab-side L4 of the reference) --------------- */
 
 /* Gauss-Legendre nodes and weights from a "<n>-LegendreGauss.grids" file in

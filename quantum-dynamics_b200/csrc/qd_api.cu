@@ -1115,3 +1115,79 @@ int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre)
 }
 
 }  // extern "C"
+
+// ---- energies with static scratch (qd_energies_noalloc) ------------------------
+// One file-scope device array holds everything qd_energies_noalloc needs on the
+// device: its first 16 double2 (256 bytes) carry the three FP64 energy sums, the
+// rest the 2-D DFT of up to QD_ENERGIES_NOALLOC_MAX_POINTS theta-space points.
+static __device__ __align__(256) double2 g_energy_scratch[16 + QD_ENERGIES_NOALLOC_MAX_POINTS];
+
+namespace {
+
+constexpr int QD_MAX_DEVICES = 64;
+std::atomic<double2 *> g_energy_scratch_at[QD_MAX_DEVICES];   // per device, set once
+
+// Device address of g_energy_scratch on the current device, looked up on the
+// first call for that device (cudaGetSymbolAddress; two threads racing here
+// both store the same address).
+int energy_scratch(double2 **out)
+{
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= QD_MAX_DEVICES)
+    return set_err(QD_ERR_DEVICE, "qd_energies_noalloc: device %d out of range", dev);
+  double2 *p = g_energy_scratch_at[dev].load();
+  if (!p) {
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_energy_scratch);
+    if (e != cudaSuccess || !p)
+      return set_err(QD_ERR_CUDA, "qd_energies_noalloc: cudaGetSymbolAddress failed: %s",
+                     cudaGetErrorString(e));
+    g_energy_scratch_at[dev].store(p);
+  }
+  *out = p;
+  return QD_OK;
+}
+
+// energies() with the scratch and the sums in g_energy_scratch: no device
+// memory is allocated or freed.
+int energies_noalloc(qd_handle *h, int run, double out4[4])
+{
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
+  const long need = h->n12 * h->nth;
+  if (need > QD_ENERGIES_NOALLOC_MAX_POINTS)
+    return set_err(QD_ERR_INVALID,
+                   "qd_energies_noalloc: %ld grid points per run exceed the static scratch "
+                   "of %d points (use qd_energies_run)", need, QD_ENERGIES_NOALLOC_MAX_POINTS);
+  double2 *base = nullptr;
+  TRY(energy_scratch(&base));
+  TRY(stage_psi(h));
+  EnergyParams e{};
+  e.n1 = h->n1; e.n2 = h->n2; e.nth = h->nth; e.nl = h->nl; e.n12 = h->n12;
+  e.psi_z = h->d_psi_z + (long)run * h->n12 * h->nth;
+  e.pot = h->d_pot + (long)run * h->vrun;
+  e.w = h->d_w; e.P = h->d_P; e.WP = h->d_WP;
+  e.T1 = h->d_T1; e.T2 = h->d_T2; e.I1 = h->d_I1; e.I2 = h->d_I2;
+  e.tw1 = h->d_tw1_64; e.tw2 = h->d_tw2_64; e.pl1 = h->pl1; e.pl2 = h->pl2;
+  e.sums = reinterpret_cast<double *>(base);
+  e.scratch = base + 16;
+  CU(cudaMemsetAsync(e.sums, 0, 3 * sizeof(double), h->st));
+  CU(launch_energies(e, h->st));
+  double s[3] = {0, 0, 0};
+  CU(cudaMemcpyAsync(s, e.sums, sizeof s, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  g_launches += energies_launches();
+  const double dd = h->data->r1.dr * h->data->r2.dr;
+  out4[0] = s[0] * dd / ((double)h->n1 * h->n2);
+  out4[1] = s[1] * dd;
+  out4[2] = s[2] * dd;
+  out4[3] = out4[0] + out4[1] + out4[2];
+  return QD_OK;
+}
+
+}  // namespace
+
+extern "C" int qd_energies_noalloc(qd_handle *h, int32_t run, double out4[4])
+{
+  if (!h || !out4) return set_err(QD_ERR_INVALID, "NULL argument");
+  return energies_noalloc(h, run, out4);
+}
