@@ -66,7 +66,7 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def build_workload(name, precision):
+def build_workload(name, precision, runs=64):
     from qd_b200 import systems as S
     if name == "c1":
         data = S.case_c1(precision=precision)
@@ -76,8 +76,8 @@ def build_workload(name, precision):
         data = S.case_c0(precision=precision)
         desc = "H+H2 J=0 extended-LEPS, 64x64x40 Jacobi grid, n_l=39, dt=10 au, 241 energies"
     elif name == "c2j0":
-        data = S.case_c2_j0(64, precision=precision)
-        desc = ("batch of 64 F+H2 J=0 propagations, 128x96x64 Jacobi grid, n_l=64, dt=10 au, "
+        data = S.case_c2_j0(runs, precision=precision)
+        desc = (f"batch of {runs} F+H2 J=0 propagations, 128x96x64 Jacobi grid, n_l=64, dt=10 au, "
                 "initial (v0,j0) cycling (0,0),(0,1),(0,2),(1,0), 241 energies each")
     else:
         raise SystemExit(f"unknown workload {name}")
@@ -192,7 +192,7 @@ def run_reference(args):
         if dist:
             dist.destroy_process_group()
         return
-    data, desc = build_workload(args.workload, 0)
+    data, desc = build_workload(args.workload, 0, args.runs)
     budget = float(os.environ.get("QD_REF_SECONDS", "60"))
     rate, info = cpu_reference_rate(data, budget)
     pts = grid_points(data)
@@ -218,7 +218,7 @@ def run_ours(args):
     from qd_b200.timeevolution import kernel_launch_count, set_device
     set_device(local)
     prec = QD_PREC_FP64 if args.fp64 else QD_PREC_FP32
-    data, desc = build_workload(args.workload, prec)
+    data, desc = build_workload(args.workload, prec, args.runs)
     runs = as_runs(data)
     pts = grid_points(data)
     K, W = args.steps, args.warmup
@@ -333,6 +333,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2j0"])
+    ap.add_argument("--runs", type=int, default=64, help="runs of the c2j0 batch")
     ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
