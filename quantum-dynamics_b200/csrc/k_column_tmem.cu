@@ -629,7 +629,7 @@ cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode
   t.status = tc_status_ptr(plan);
   t.renorm = plan.renorm;
   t.nnorm = plan.nth < plan.S ? plan.nth : plan.S;
-  const long ntiles = (p.n12 + TPTS - 1) / TPTS;
+  const long ntiles = (p.n12 + TPTS - 1) / TPTS * p.nruns;   // tiles of all runs
   const int grid = (int)(ntiles < plan.grid ? ntiles : plan.grid);
   switch (plan.S) {
     case 16: launch_mode<16>(grid, plan.smem_bytes, s, p, t, mode); break;

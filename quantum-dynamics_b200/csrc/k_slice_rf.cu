@@ -1,0 +1,320 @@
+// k_slice_rf.cu -- the l-space part of one complex64 split-operator step,
+//     psi_l <- Rot(dt/2) IFFT2 [exp(-i(T1+T2)dt)/(n1 n2)] FFT2 Rot(dt/2) psi_l
+// (evolution_dt, timeEvol.C:625-635; the FFTW 2-D DFT pair of
+// fftwinterface.C:70-76; phase tables timeEvol.C:465-517), one l-slice per
+// CTA, with every 1-D transform done as two register passes.
+//
+// A length N = A*B transform (n = a + A b, k = c + B d) is
+//   pass 1, one item per a:  B-point DFT over b in registers, times W_N^{a c}
+//   pass 2, one item per c:  A-point DFT over a in registers -> X[c + B d]
+// so a 2-D transform costs two shared-memory round trips per dimension
+// instead of one per radix stage.  The slice lives in shared memory in ONE
+// padded layout for the whole step, every pass works in place, and only
+// six barriers separate the seven passes:
+//   P1  global -> regs: Rot/2, row pass 1 (B1-pt), twiddle      -> smem
+//   P2  row pass 2 (A1-pt)                                       in place
+//   P3  column pass 1 (B2-pt), twiddle                           in place
+//   P4  column pass 2 (A2-pt), kinetic phase, inverse column
+//       pass 1 (A2-pt), twiddle                                  in place
+//   P5  inverse column pass 2 (B2-pt)                            in place
+//   P6  inverse row pass 1 (A1-pt over a block), twiddle         in place
+//   P7  inverse row pass 2 (B1-pt), Rot/2 -> global
+// Row layout: block c (c < B1) holds slots 0..A1-1 at s + (A1+1) c; row
+// stride RS = N1 + B1 (= 8 mod 16 complex).  With this padding every warp
+// access of every pass touches each shared-memory bank at most twice (the
+// minimum for 8-byte elements), and global loads and stores are whole
+// 64- or 128-byte segments.  The forward row transform leaves frequency
+// k = c + B1 d at slot d of block c; the inverse row transform reads that
+// order directly (its decomposition is the transposed one, A = B1, B = A1).
+//
+// Radix-16 and radix-12 DFTs are 4x4 and 4x3 compositions whose internal
+// twiddles are compensated constants (value + residual), like the radix-8
+// and radix-3 butterflies, so no fixed-point rounding bias enters the norm.
+#include "qd_kernels.h"
+
+namespace {
+
+// ---- compile-time twiddles exp(SGN 2 pi i E / N) --------------------------
+// cos(2 pi a / 48) as (magnitude code, sign); a in [0, 48), a multiple of 3 or 4.
+// codes: 0 -> 0, 1 -> 1, 2 -> 1/2, 3 -> 1/sqrt2, 4 -> sqrt3/2, 5 -> cos(pi/8), 6 -> sin(pi/8)
+__host__ __device__ constexpr int kcode(int a)
+{
+  const int r = a % 24 <= 12 ? a % 24 : 24 - a % 24;    // |cos| is even in a and 24-periodic
+  return r == 0 ? 1 : r == 3 ? 5 : r == 4 ? 4 : r == 6 ? 3 : r == 8 ? 2 : r == 9 ? 6 : r == 12 ? 0
+                                                                                               : -1;
+}
+__host__ __device__ constexpr int ksign(int a)
+{
+  return (a % 48 > 12 && a % 48 < 36) ? -1 : 1;
+}
+
+template <int CODE> __device__ __forceinline__ float kmag(float x)
+{
+  if constexpr (CODE == 1) return x;
+  else if constexpr (CODE == 2) return 0.5f * x;
+  else if constexpr (CODE == 3) return fmaf(x, 7.07106769e-01f, x * 1.21016175e-08f);
+  else if constexpr (CODE == 4) return fmaf(x, 8.66025388e-01f, x * 1.55436251e-08f);
+  else if constexpr (CODE == 5) return fmaf(x, 9.23879504e-01f, x * 2.83074897e-08f);
+  else if constexpr (CODE == 6) return fmaf(x, 3.82683426e-01f, x * 6.22335072e-09f);
+  else return 0.f;
+}
+
+// x * cos(2 pi A / 48)
+template <int A> __device__ __forceinline__ float kcos(float x)
+{
+  static_assert(kcode(A) >= 0, "angle not in the table");
+  const float v = kmag<kcode(A)>(x);
+  return ksign(A) < 0 ? -v : v;
+}
+
+template <int N, int E, int SGN> __device__ __forceinline__ float2 twk(float2 z)
+{
+  static_assert(48 % N == 0, "N must divide 48");
+  constexpr int a = (E % N) * (48 / N);
+  constexpr int as = (a + 36) % 48;                     // sin(t) = cos(t - pi/2)
+  if constexpr (a == 0) {
+    return z;
+  } else {
+    float re, im;
+    if constexpr (kcode(as) == 0) {                     // sin = 0
+      re = kcos<a>(z.x);
+      im = kcos<a>(z.y);
+    } else if constexpr (kcode(a) == 0) {               // cos = 0
+      re = SGN > 0 ? -kcos<as>(z.y) : kcos<as>(z.y);
+      im = SGN > 0 ? kcos<as>(z.x) : -kcos<as>(z.x);
+    } else {
+      re = SGN > 0 ? kcos<a>(z.x) - kcos<as>(z.y) : kcos<a>(z.x) + kcos<as>(z.y);
+      im = SGN > 0 ? kcos<as>(z.x) + kcos<a>(z.y) : kcos<a>(z.y) - kcos<as>(z.x);
+    }
+    return make_float2(re, im);
+  }
+}
+
+// ---- DFTs in registers, natural order in and out --------------------------
+template <int N, int SGN> struct Dft;
+template <int SGN> struct Dft<2, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { SmallDFT<2, float2>::run(v, SGN, nullptr, 0); }
+};
+template <int SGN> struct Dft<3, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { SmallDFT<3, float2>::run(v, SGN, nullptr, 0); }
+};
+template <int SGN> struct Dft<4, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { SmallDFT<4, float2>::run(v, SGN, nullptr, 0); }
+};
+template <int SGN> struct Dft<8, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { SmallDFT<8, float2>::run(v, SGN, nullptr, 0); }
+};
+
+// N = 4 Q: n = p + 4 q, Q-point DFTs over q, twiddles W_N^{p c}, 4-point
+// DFTs over p, X[c + Q d]
+template <int N, int Q, int SGN> struct Dft4xQ {
+  template <int P, int C> static __device__ __forceinline__ void tw(float2 (&u)[4][Q])
+  {
+    if constexpr (C < Q) {
+      u[P][C] = twk<N, P * C, SGN>(u[P][C]);
+      tw<P, C + 1>(u);
+    } else if constexpr (P + 1 < 4) {
+      tw<P + 1, 0>(u);
+    }
+  }
+  static __device__ __forceinline__ void run(float2 *v)
+  {
+    float2 u[4][Q];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) u[p][q] = v[p + 4 * q];
+      Dft<Q, SGN>::run(u[p]);
+    }
+    tw<1, 1>(u);
+#pragma unroll
+    for (int c = 0; c < Q; c++) {
+      float2 s[4] = {u[0][c], u[1][c], u[2][c], u[3][c]};
+      Dft<4, SGN>::run(s);
+#pragma unroll
+      for (int d = 0; d < 4; d++) v[c + Q * d] = s[d];
+    }
+  }
+};
+template <int SGN> struct Dft<12, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { Dft4xQ<12, 3, SGN>::run(v); }
+};
+template <int SGN> struct Dft<16, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { Dft4xQ<16, 4, SGN>::run(v); }
+};
+
+template <int N1, int N2, int NT> struct RfShape {
+  static constexpr int A1 = N1 == 64 ? 8 : 16;        // row pass 2 radix (B1 = 8)
+  static constexpr int B1 = N1 / A1;
+  static constexpr int A2 = N2 / 8;                   // column pass 2 radix (B2 = 8)
+  static constexpr int B2 = 8;
+  static constexpr int RS = N1 + B1;                  // padded row stride (complex)
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)N2 * RS + N1 + N2);
+  static_assert(B1 == 8 && RS % 16 == 8, "row layout");
+  static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
+};
+
+__device__ __forceinline__ float2 rot_at(const float2 *r1, float2 rj, int i)
+{ return cmul(r1[i], rj); }
+
+template <int N1, int N2, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
+{
+  using Sh = RfShape<N1, N2, NT>;
+  constexpr int A1 = Sh::A1, B1 = Sh::B1, A2 = Sh::A2, B2 = Sh::B2, RS = Sh::RS;
+  extern __shared__ float4 smem4[];
+  float2 *S = reinterpret_cast<float2 *>(smem4);    // [N2][RS]
+  float2 *r1 = S + N2 * RS;                          // rc1[l][0..N1)
+  float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
+  const int tid = threadIdx.x;
+  if ((int)blockIdx.x >= p.nruns * p.nl) {           // extra CTAs: flux preparation
+    const int q = ((int)blockIdx.x - p.nruns * p.nl) * NT + tid;
+    if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
+    return;
+  }
+  const int sl = blockIdx.x, l = sl % p.nl;          // slice = run * nl + l
+  float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
+  const float2 *tw1 = reinterpret_cast<const float2 *>(p.tw1);
+  const float2 *tw2 = reinterpret_cast<const float2 *>(p.tw2);
+  const float2 *rc2 = p.rc2 + l * N2;
+  for (int e = tid; e < N1; e += NT) r1[e] = __ldg(p.rc1 + l * N1 + e);
+  for (int e = tid; e < N2; e += NT) t2[e] = __ldg(tw2 + e);
+  __syncthreads();
+
+  // P1: items (j, a); elements i = a + A1 b from global
+  {
+    const int a = tid % A1;
+    float2 w[B1];
+#pragma unroll
+    for (int c = 0; c < B1; c++) w[c] = __ldg(tw1 + a * c);
+#pragma unroll 2
+    for (int e = tid; e < N2 * A1; e += NT) {
+      const int j = e / A1;
+      const float2 rj = __ldg(rc2 + j);
+      float2 v[B1];
+#pragma unroll
+      for (int b = 0; b < B1; b++) v[b] = g[j * N1 + a + A1 * b];
+#pragma unroll
+      for (int b = 0; b < B1; b++) v[b] = cmul(v[b], rot_at(r1, rj, a + A1 * b));
+      Dft<B1, -1>::run(v);
+#pragma unroll
+      for (int c = 0; c < B1; c++) S[j * RS + a + (A1 + 1) * c] = c ? cmul(v[c], w[c]) : v[c];
+    }
+  }
+  __syncthreads();
+  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
+  for (int e = tid; e < N2 * B1; e += NT) {
+    const int j = e / B1, c = e % B1;
+    float2 *blk = S + j * RS + (A1 + 1) * c;
+    float2 v[A1];
+#pragma unroll
+    for (int a = 0; a < A1; a++) v[a] = blk[a];
+    Dft<A1, -1>::run(v);
+#pragma unroll
+    for (int d = 0; d < A1; d++) blk[d] = v[d];
+  }
+  __syncthreads();
+  // column passes on physical column pc of counter q (frequency k(q))
+  // P3: items (q, a'): rows a' + A2 b'
+  for (int e = tid; e < N1 * A2; e += NT) {
+    const int q = e % N1, ap = e / N1;
+    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + ap * RS;
+    float2 v[B2];
+#pragma unroll
+    for (int b = 0; b < B2; b++) v[b] = col[A2 * b * RS];
+    Dft<B2, -1>::run(v);
+#pragma unroll
+    for (int c = 0; c < B2; c++) col[A2 * c * RS] = c ? cmul(v[c], t2[ap * c]) : v[c];
+  }
+  __syncthreads();
+  // P4: items (q, c'): rows a' + A2 c'; forward pass 2, kinetic phase, inverse pass 1
+  for (int e = tid; e < N1 * B2; e += NT) {
+    const int q = e % N1, cp = e / N1;
+    const int k = (q / A1) + B1 * (q % A1);
+    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + A2 * cp * RS;
+    const float2 k1 = __ldg(p.kc1 + k);
+    float2 v[A2];
+#pragma unroll
+    for (int a = 0; a < A2; a++) v[a] = col[a * RS];
+    Dft<A2, -1>::run(v);
+#pragma unroll
+    for (int d = 0; d < A2; d++)
+      v[d] = cmul(v[d], cscale2(cmul(k1, __ldg(p.kc2 + cp + B2 * d)), p.kscale, p.kscale_lo));
+    Dft<A2, +1>::run(v);
+#pragma unroll
+    for (int cc = 0; cc < A2; cc++) col[cc * RS] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
+  }
+  __syncthreads();
+  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d''
+  for (int e = tid; e < N1 * A2; e += NT) {
+    const int q = e % N1, cc = e / N1;
+    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + cc * RS;
+    float2 v[B2];
+#pragma unroll
+    for (int a = 0; a < B2; a++) v[a] = col[A2 * a * RS];
+    Dft<B2, +1>::run(v);
+#pragma unroll
+    for (int d = 0; d < B2; d++) col[A2 * d * RS] = v[d];
+  }
+  __syncthreads();
+  // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
+  {
+    const int bk = tid % B1;
+    float2 w[A1];
+#pragma unroll
+    for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
+    for (int e = tid; e < N2 * B1; e += NT) {
+      const int j = e / B1;
+      float2 *blk = S + j * RS + (A1 + 1) * bk;
+      float2 v[A1];
+#pragma unroll
+      for (int s = 0; s < A1; s++) v[s] = blk[s];
+      Dft<A1, +1>::run(v);
+#pragma unroll
+      for (int c = 0; c < A1; c++) blk[c] = c ? cmul(v[c], w[c]) : v[c];
+    }
+  }
+  __syncthreads();
+  // P7: items (j, c'): slot c' of every block -> i = c' + A1 d', Rot/2, store
+#pragma unroll 2
+  for (int e = tid; e < N2 * A1; e += NT) {
+    const int j = e / A1, c = e % A1;
+    const float2 rj = __ldg(rc2 + j);
+    float2 v[B1];
+#pragma unroll
+    for (int b = 0; b < B1; b++) v[b] = S[j * RS + c + (A1 + 1) * b];
+    Dft<B1, +1>::run(v);
+#pragma unroll
+    for (int d = 0; d < B1; d++)
+      g[j * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
+  }
+}
+
+template <int N1, int N2, int NT> cudaError_t launch_rf(const LineParams &p, cudaStream_t s)
+{
+  constexpr size_t sm = RfShape<N1, N2, NT>::SMEM;
+  cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)(p.nruns * p.nl + p.flux_ctas);
+  k_slice_rf<N1, N2, NT><<<grid, NT, sm, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int slice_rf_threads(int n1, int n2)
+{
+  if (n1 == 64 && n2 == 64) return 256;
+  if (n1 == 128 && n2 == 96) return 256;
+  if (n1 == 128 && n2 == 128) return 512;
+  return 0;
+}
+
+cudaError_t launch_slice_rf(const LineParams &p, cudaStream_t s)
+{
+  if (p.n1 == 64 && p.n2 == 64) return launch_rf<64, 64, 256>(p, s);
+  if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256>(p, s);
+  if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512>(p, s);
+  return cudaErrorInvalidValue;
+}

@@ -125,7 +125,7 @@ struct qd_handle {
   double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
   float2 *d_expV32 = nullptr;
   float2 *d_rc1 = nullptr, *d_rc2 = nullptr, *d_kc1 = nullptr, *d_kc2 = nullptr;
-  int slice_cluster = 0;          // fused slice kernel: CTAs per l-slice (0 = split kernels)
+  int slice_cluster = 0;          // l-space kernel (LineParams::cluster code)
   double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
   void *d_lpsi = nullptr;
@@ -375,8 +375,10 @@ LineParams line_params(qd_handle *h, bool f32)
 }
 
 // Autotuner of the complex64 l-space pass: time the fused slice kernel with
-// 1, 2 and 4 CTAs per slice (and the split kernels) on a scratch wavepacket
-// and keep the fastest.  QD_SLICE_CLUSTER=0|1|2|4 forces a choice.
+// 1, 2 and 4 CTAs per slice, the register-FFT slice kernel and the split
+// kernels on a scratch wavepacket
+// and keep the fastest.  QD_SLICE_CLUSTER=0|1|2|4|8 forces a choice (8 = the
+// register-FFT kernel).
 int tune_slice(qd_handle *h)
 {
   h->slice_cluster = 0;
@@ -397,7 +399,7 @@ int tune_slice(qd_handle *h)
   LineParams p = line_params(h, true);
   p.lpsi = scratch;
   float best = 1e30f;
-  for (int cl : {0, 1, 2, 4}) {
+  for (int cl : {0, 1, 2, 4, SLICE_RF}) {
     if (cl > 0 && !slice_cluster_ok(h->n1, h->n2, cl)) continue;
     p.cluster = cl;
     bool ok = true;
@@ -429,8 +431,10 @@ template <typename R> int issue_lines(qd_handle *h)
   if (fused_flux) {
     p.flux = flux_params(h);
     const int nq = h->nth * h->n1 * h->nruns;
-    const int ctas = (nq + 511) / 512;                // 512 threads per slice CTA
-    p.flux_ctas = (ctas + p.cluster - 1) / p.cluster * p.cluster;
+    const int nt = slice_threads(h->n1, h->n2, p.cluster);
+    const int ctas = (nq + nt - 1) / nt;
+    const int cl = p.cluster == SLICE_RF ? 1 : p.cluster;   // whole clusters
+    p.flux_ctas = (ctas + cl - 1) / cl * cl;
   }
   TRY(prof_mark(h, -1));
   if (p.cluster > 0) {

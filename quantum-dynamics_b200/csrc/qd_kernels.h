@@ -110,7 +110,8 @@ struct LineParams {
   FftPlan pl1, pl2;
   int rows_per_cta;        // rows kernels
   int cols_per_cta;        // column kernel
-  int cluster;             // fused slice kernel: CTAs per slice (0 = split kernels)
+  int cluster;             // l-space pass: 0 = split kernels, 1/2/4 = cluster kernel with
+                           // that many CTAs per slice, SLICE_RF = register-FFT kernel
   FluxParams flux;         // fused slice kernel: flux preparation of the step ...
   int flux_ctas;           // ... by this many extra CTAs (0 = none)
   int fft_only;            // split kernels: plain forward 2-D DFT, no phases
@@ -174,7 +175,11 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
                                      cudaStream_t s);
 // fused slice kernel (FP32): CTAs per slice it can run with for these sizes
 // (0 if none), its launch, and the smem bytes it needs
+constexpr int SLICE_RF = 8;    // LineParams::cluster value of the register-FFT slice kernel
 int slice_cluster_ok(int n1, int n2, int cluster);
+int slice_rf_threads(int n1, int n2);        // threads per CTA, 0 if the shape is not built
+int slice_threads(int n1, int n2, int cluster);
+cudaError_t launch_slice_rf(const LineParams &p, cudaStream_t s);
 cudaError_t launch_slice(const LineParams &p, cudaStream_t s);
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const double *w,
                                      const double *legendre, double *P, double *WP,

@@ -164,22 +164,46 @@ def test_fp32_tensor_core_and_simt_agree(monkeypatch):
 
 @pytest.mark.parametrize("shape", [(64, 64, 32), (128, 128, 64), (128, 96, 64), (48, 40, 24)])
 def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
-    # fused slice kernel with 1, 2, 4 CTAs per slice (where they fit) against
-    # the three-kernel split pass
+    # fused slice kernel with 1, 2, 4 CTAs per slice and the register-FFT slice
+    # kernel (8), where they are built, against the three-kernel split pass;
+    # the flux preparation rides in the fused launches, so P(E) is compared too
     n1, n2, nth = shape
     base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=8, n_energies=5,
                         n_gradient_points=5, r=(0.5, 9.0))
     out = {}
-    for cl in ("0", "1", "2", "4"):
+    for cl in ("0", "1", "2", "4", "8"):
         monkeypatch.setenv("QD_SLICE_CLUSTER", cl)
         d = S.copy_case(base)
         d.options.precision = QD_PREC_FP32
         with Propagator(d) as p:
             p.propagate(8)
-            out[cl] = p.psi()
+            out[cl] = (p.psi(), p.crp())
     ref = out["0"]
-    for cl, psi in out.items():
-        assert rel(psi, ref) < 2e-5, cl
+    for cl, (psi, crp) in out.items():
+        assert rel(psi, ref[0]) < 2e-5, cl
+        assert np.abs(crp - ref[1]).max() < 1e-6, cl
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 32), (128, 96, 64)])
+def test_fp32_register_fft_slice_batch_matches_fp64(shape, monkeypatch):
+    # the register-FFT slice kernel on a 3-run batch (flux preparation in its
+    # extra CTAs) against the FP64 plain form of the same runs, 40 steps
+    n1, n2, nth = shape
+    base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=40, n_energies=9,
+                        n_gradient_points=5, r=(0.5, 9.0))
+    runs = S.batch_cases(base, [(0, 0), (0, 1), (1, 0)])
+    monkeypatch.setenv("QD_SLICE_CLUSTER", "8")
+    got = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        rs = [S.copy_case(r) for r in runs]
+        for r in rs:
+            r.options.precision = prec
+        with Propagator(rs) as p:
+            p.propagate(40)
+            got[prec] = [(p.psi(i), p.crp(i)) for i in range(len(rs))]
+    for (a, ca), (b, cb) in zip(got[QD_PREC_FP32], got[QD_PREC_FP64]):
+        assert rel(a, b) < 1e-4
+        assert np.abs(ca - cb).max() < FP32_CRP_ABS
 
 
 def test_fp32_c1_full_run_within_pe_budget():
