@@ -193,20 +193,9 @@ __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint
 
 constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4 share a TMEM lane quarter)
 
-// sum over the 2*NG threads that hold one complex point (Re/Im rows x column
-// groups); `slot` is an [NG][TPTS] smem array.  Includes a CTA barrier.
-__device__ __forceinline__ float point_sum(float part, float *slot, int grp, int pt, bool is_im)
-{
-  part += __shfl_xor_sync(0xffffffffu, part, 1);
-  if (!is_im) slot[grp * TPTS + pt] = part;
-  __syncthreads();
-  float s = 0.f;
-#pragma unroll
-  for (int g = 0; g < NG; g++) s += slot[g * TPTS + pt];
-  return s;
-}
-
-template <int S, int MODE>
+// EX: exact shape -- n_l = n_theta = S, n12 and n1 multiples of the tile, so
+// every point and column of a tile is valid and a tile lies in one grid row j.
+template <int S, int MODE, bool EX>
 __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev t)
 {
   constexpr int mode = MODE;
@@ -220,9 +209,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   unsigned char *B1 = base;                     // hi | mid | lo
   unsigned char *B2 = B1 + 3 * B_BYTES;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 3 * B_BYTES);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
-  double *red = reinterpret_cast<double *>(mbar + 4);
-  float *xch = reinterpret_cast<float *>(red + 32);      // [4 exchanges][NG][TPTS]
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
+  float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *wk = xch + 4 * NG * TPTS;                        // [S] w_k (float), 0 beyond n_theta
   float *linv = wk + S;                                   // [S] 1/(l+1/2)
 
@@ -232,6 +220,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   const int c0 = grp * H;                        // first K/N column of this thread
   const int pt = row >> 1;                       // complex point within tile
   const bool is_im = row & 1;
+  const int comp = is_im ? 1 : 0;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -273,37 +262,41 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   uint32_t ph1 = 0, ph2 = 0;
   bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
 
-  float2 *surf = reinterpret_cast<float2 *>(p.surf);
+  // 32-bit tile arithmetic: the host checks n12 * n_l * 2 * n_runs < 2^31
+  const int n12 = (int)p.n12, n1 = p.n1;
+  const int nl = p.nl, nth = p.nth;
+  const int tpr = (n12 + TPTS - 1) / TPTS;      // tiles per run
+  const int ntiles = tpr * p.nruns;
+  const int stride = 2 * n12;                   // floats between orders l (or k) of a point
   const float *lsrc = reinterpret_cast<const float *>(p.lpsi);
   float *ldst = reinterpret_cast<float *>(p.lpsi);
-  const long tpr = (p.n12 + TPTS - 1) / TPTS;        // tiles per run
-  const long ntiles = tpr * p.nruns;
-  const long n12 = p.n12;
-  const int nl = p.nl, nth = p.nth;
-  const int comp = is_im ? 1 : 0;
+  float *surf = reinterpret_cast<float *>(p.surf);
+  double *psiz = reinterpret_cast<double *>(p.psi_z);
   const float2 *expv = p.expV32;
+  const float ysg = is_im ? 1.f : -1.f;         // out = mine e.x + ysg other e.y
 
   float a[H];
-#define QD_PREFETCH_A(tl)                                                              \
-  do {                                                                                 \
-    const long rr = (tl) / tpr, qq = ((tl) - rr * tpr) * TPTS + pt;                    \
-    const bool ok = (tl) < ntiles && qq < n12;                                         \
-    const float *src = lsrc + 2 * rr * nl * n12;                                       \
-    _Pragma("unroll") for (int u = 0; u < H; u++) {                                    \
-      const int l = c0 + u;                                                            \
-      a[u] = (ok && l < nl) ? __ldg(src + 2 * ((long)l * n12 + qq) + comp) : 0.f;      \
-    }                                                                                  \
+#define QD_PREFETCH_A(tl)                                                            \
+  do {                                                                               \
+    const int rr = (tl) / tpr, qq = ((tl) - rr * tpr) * TPTS + pt;                   \
+    const bool ok = EX || ((tl) < ntiles && qq < n12);                               \
+    const float *src = lsrc + (size_t)rr * nl * stride + (size_t)c0 * stride + 2 * qq + comp; \
+    _Pragma("unroll") for (int u = 0; u < H; u++) {                                  \
+      if (EX) a[u] = (tl) < ntiles ? __ldg(src + u * stride) : 0.f;                   \
+      else a[u] = (ok && c0 + u < nl) ? __ldg(src + u * stride) : 0.f;               \
+    }                                                                                \
   } while (0)
-  if (mode != COL_HEAD) QD_PREFETCH_A((long)blockIdx.x);
+  if (mode != COL_HEAD) QD_PREFETCH_A((int)blockIdx.x);
 
-  for (long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const int run = (int)(tile / tpr);
-    const long q = (tile - (long)run * tpr) * TPTS + pt;
-    const bool qok = q < n12;
-    const long voff = (long)run * p.vrun, zoff = (long)run * nth * n12;
-    float2 *surf_r = surf + (long)run * p.surf_nrows * nth * p.n1;
-    float *ldst_r = ldst + 2 * (long)run * nl * n12;
-    const int j = qok ? (int)(q / p.n1) : 0, i = qok ? (int)(q % p.n1) : 0;
+  for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const int run = tile / tpr;
+    const int q0 = (tile - run * tpr) * TPTS;
+    const int q = q0 + pt;
+    const bool qok = EX || q < n12;
+    int j, i;
+    if (EX) { j = q0 / n1; i = q0 - j * n1 + pt; }
+    else { j = qok ? q / n1 : 0; i = qok ? q - (q / n1) * n1 : 0; }
+    const size_t voff = (size_t)run * p.vrun;
     float2 ev[H];
     float sc = 1.f;
 
@@ -327,10 +320,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
         mma_commit(mb1);
       }
       if (mode == COL_MID) {                    // V phase of the tile, in flight during GEMM1
+        const float2 *ep = expv + voff + (size_t)c0 * n12 + q;
 #pragma unroll
         for (int u = 0; u < H; u++) {
-          const int k = c0 + u;
-          ev[u] = (qok && k < nth) ? __ldg(expv + voff + (long)k * n12 + q) : make_float2(1.f, 0.f);
+          float2 e = make_float2(1.f, 0.f);
+          if (EX || (qok && c0 + u < nth)) e = __ldg(ep + u * n12);
+          ev[u] = make_float2(e.x, e.y * ysg);
         }
       }
       float n_l = 0.f;
@@ -339,7 +334,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
-      // pass 1 over D: theta-space norm of the column -> isometry scale
+      // theta-space norm of the GEMM1 output -> isometry scale
       float nt_part = 0.f;
 #pragma unroll
       for (int u = 0; u < H; u += 4) {
@@ -348,16 +343,26 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
         nt_part += wk[c0 + u] * v0 * v0 + wk[c0 + u + 1] * v1 * v1 +
                    wk[c0 + u + 2] * v2 * v2 + wk[c0 + u + 3] * v3 * v3;
       }
-      const float n_t = point_sum(nt_part, xch + NG * TPTS, grp, pt, is_im);
+      nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
+      if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
+      __syncthreads();
+      float n_t = 0.f;
+#pragma unroll
+      for (int g = 0; g < NG; g++) n_t += xch[NG * TPTS + g * TPTS + pt];
       sc = (t.renorm && n_t > 0.f) ? sqrtf(n_l / n_t) : 1.f;
     }
 
-    // ---- theta-space operations (pass 2), A2 into TMEM --------------------------------
-    float nt2_part = 0.f;
-    const float dd = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) * sc : sc;
-    const bool flux_row = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
-                          j < p.surf_j0 + p.surf_nrows;
+    // ---- theta-space operations, A2 into TMEM ----------------------------------------
+    // tsum: this thread's share of sum_k w_k |psi_k|^2 of its point after the
+    // absorber; |exp(-i V dt)| = 1, so it is also the theta norm of GEMM2's input
     float tsum = 0.f;
+    const float dd = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) * sc : sc;
+    bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
+                j < p.surf_j0 + p.surf_nrows;
+    float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
+                       : nullptr;
+    double *zrow = (mode != COL_HEAD && p.out_z) ? psiz + 2 * ((size_t)run * nth * n12 + q) + comp
+                                                 : nullptr;
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
       float v[4];
@@ -367,18 +372,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
         for (int x = 0; x < 4; x++) {
           const int k = c0 + u + x;
           const float mine = v[x] * dd;
-          const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-          const float re = is_im ? other : mine, im = is_im ? mine : other;
-          if (!is_im) {
-            tsum += wk[k] * (re * re + im * im);
-            if (qok && k < nth) {
-              if (flux_row) surf_r[((long)(j - p.surf_j0) * nth + k) * p.n1 + i] = make_float2(re, im);
-              if (p.out_z) p.psi_z[zoff + (long)k * n12 + q] = make_double2(re, im);
-            }
+          tsum += wk[k] * mine * mine;
+          if (EX || (qok && k < nth)) {
+            if (frow) srow[(size_t)2 * k * n1] = mine;
+            if (zrow) zrow[(size_t)2 * k * n12] = mine;
           }
           if (mode == COL_MID) {
-            const float2 e = ev[u + x];
-            v[x] = is_im ? re * e.y + im * e.x : re * e.x - im * e.y;
+            const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
+            v[x] = fmaf(other, ev[u + x].y, mine * ev[u + x].x);
           } else {
             v[x] = mine;
           }
@@ -389,8 +390,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           const int k = c0 + u + x;
           float val = 0.f;
           if (qok && k < nth) {
-            const long g = (long)k * n12 + q;
-            const double2 z = p.psi_z[zoff + g];
+            const size_t g = (size_t)k * n12 + q;
+            const double2 z = p.psi_z[(size_t)run * nth * n12 + g];
             double s, c;
             sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
             double2 f = make_double2(c, -s);
@@ -402,40 +403,38 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
             val = (float)(is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y);
           }
           v[x] = val;
+          tsum += wk[k] * val * val;
         }
       }
-      if (mode != COL_TAIL) {
-        put4_tmem(my_hi + u, my_lo + u, v[0], v[1], v[2], v[3]);
-        nt2_part += wk[c0 + u] * v[0] * v[0] + wk[c0 + u + 1] * v[1] * v[1] +
-                    wk[c0 + u + 2] * v[2] * v[2] + wk[c0 + u + 3] * v[3] * v[3];
-      }
+      if (mode != COL_TAIL) put4_tmem(my_hi + u, my_lo + u, v[0], v[1], v[2], v[3]);
     }
-    if (p.norm_out && mode != COL_HEAD) {        // this tile's share of its run's norm
-      const double s = block_sum(qok ? (double)tsum : 0.0, red);
-      if (tid == 0) atomicAdd(p.norm_out + run, s);
+    // per-point theta norm (both components, both column groups)
+    tsum += __shfl_xor_sync(0xffffffffu, tsum, 1);
+    if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = tsum;
+    if (mode != COL_TAIL) tmem_wait_st();
+    tc_fence_before();
+    __syncthreads();
+    float n_t2 = 0.f;
+#pragma unroll
+    for (int g = 0; g < NG; g++) n_t2 += xch[2 * NG * TPTS + g * TPTS + pt];
+    if (p.norm_out && mode != COL_HEAD) {       // this tile's share of its run's norm
+      double s = (grp == 0 && !is_im && qok) ? (double)n_t2 : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
     }
     if (mode == COL_TAIL) {
-      QD_PREFETCH_A(tile + gridDim.x);
-      tc_fence_before();
-      __syncthreads();
+      QD_PREFETCH_A(tile + (int)gridDim.x);
       continue;
     }
 
     // ---- GEMM2: D = A2 * B2 -------------------------------------------------------------
-    tmem_wait_st();
-    tc_fence_before();
-    nt2_part += __shfl_xor_sync(0xffffffffu, nt2_part, 1);
-    if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = nt2_part;
-    __syncthreads();
     if (tid == 0) {
       tc_fence_after();
       gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
       mma_commit(mb2);
     }
-    float n_t2 = 0.f;
-#pragma unroll
-    for (int g = 0; g < NG; g++) n_t2 += xch[2 * NG * TPTS + g * TPTS + pt];
-    if (mode != COL_HEAD) QD_PREFETCH_A(tile + gridDim.x);   // next tile's loads fly during GEMM2
+    if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
@@ -444,25 +443,33 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     for (int u = 0; u < H; u += 4) {
       float v0, v1, v2, v3;
       tmem_ld4(my_d + u, v0, v1, v2, v3);
-      no_part += (c0 + u < t.nnorm ? v0 * v0 * linv[c0 + u] : 0.f) +
-                 (c0 + u + 1 < t.nnorm ? v1 * v1 * linv[c0 + u + 1] : 0.f) +
-                 (c0 + u + 2 < t.nnorm ? v2 * v2 * linv[c0 + u + 2] : 0.f) +
-                 (c0 + u + 3 < t.nnorm ? v3 * v3 * linv[c0 + u + 3] : 0.f);
+      if (EX) {
+        no_part += v0 * v0 * linv[c0 + u] + v1 * v1 * linv[c0 + u + 1] +
+                   v2 * v2 * linv[c0 + u + 2] + v3 * v3 * linv[c0 + u + 3];
+      } else {
+        no_part += (c0 + u < t.nnorm ? v0 * v0 * linv[c0 + u] : 0.f) +
+                   (c0 + u + 1 < t.nnorm ? v1 * v1 * linv[c0 + u + 1] : 0.f) +
+                   (c0 + u + 2 < t.nnorm ? v2 * v2 * linv[c0 + u + 2] : 0.f) +
+                   (c0 + u + 3 < t.nnorm ? v3 * v3 * linv[c0 + u + 3] : 0.f);
+      }
     }
-    const float n_o = point_sum(no_part, xch + 3 * NG * TPTS, grp, pt, is_im);
+    no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
+    if (!is_im) xch[3 * NG * TPTS + grp * TPTS + pt] = no_part;
+    __syncthreads();
+    float n_o = 0.f;
+#pragma unroll
+    for (int g = 0; g < NG; g++) n_o += xch[3 * NG * TPTS + g * TPTS + pt];
     const float sc2 = (t.renorm && n_o > 0.f) ? sqrtf(n_t2 / n_o) : 1.f;
+    float *dst = ldst + (size_t)run * nl * stride + (size_t)c0 * stride + 2 * q + comp;
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
       float v[4];
       tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
 #pragma unroll
-      for (int x = 0; x < 4; x++) {
-        const int l = c0 + u + x;
-        if (qok && l < nl) ldst_r[2 * ((long)l * n12 + q) + comp] = v[x] * sc2;
-      }
+      for (int x = 0; x < 4; x++)
+        if (EX || (qok && c0 + u + x < nl)) dst[(u + x) * stride] = v[x] * sc2;
     }
     tc_fence_before();
-    __syncthreads();
   }
 #undef QD_PREFETCH_A
 
@@ -476,26 +483,45 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   }
 }
 
-template <int S> cudaError_t set_smem_attr(int bytes)
+template <int S, bool EX> cudaError_t set_smem_attr_ex(int bytes)
 {
-  cudaError_t e = cudaFuncSetAttribute(k_column_tc<S, COL_HEAD>,
+  cudaError_t e = cudaFuncSetAttribute(k_column_tc<S, COL_HEAD, EX>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_column_tc<S, COL_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes);
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_MID, EX>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_column_tc<S, COL_TAIL>,
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_TAIL, EX>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
+}
+template <int S> cudaError_t set_smem_attr(int bytes)
+{
+  cudaError_t e = set_smem_attr_ex<S, false>(bytes);
+  if constexpr (S == 64) {
+    if (e == cudaSuccess) e = set_smem_attr_ex<S, true>(bytes);
+  }
+  return e;
+}
+
+template <int S, bool EX>
+void launch_mode_ex(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
+                    int mode)
+{
+  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD, EX><<<grid, NTHREADS, smem, s>>>(p, t);
+  else if (mode == COL_MID) k_column_tc<S, COL_MID, EX><<<grid, NTHREADS, smem, s>>>(p, t);
+  else k_column_tc<S, COL_TAIL, EX><<<grid, NTHREADS, smem, s>>>(p, t);
 }
 
 template <int S>
 void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
                  int mode)
 {
-  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD><<<grid, NTHREADS, smem, s>>>(p, t);
-  else if (mode == COL_MID) k_column_tc<S, COL_MID><<<grid, NTHREADS, smem, s>>>(p, t);
-  else k_column_tc<S, COL_TAIL><<<grid, NTHREADS, smem, s>>>(p, t);
+  const bool ex = S == 64 && p.nl == S && p.nth == S && p.n12 % TPTS == 0 && p.n1 % TPTS == 0;
+  if constexpr (S == 64) {
+    if (ex) { launch_mode_ex<S, true>(grid, smem, s, p, t, mode); return; }
+  }
+  launch_mode_ex<S, false>(grid, smem, s, p, t, mode);
 }
 
 template <int S> constexpr int smem_bytes_for()
