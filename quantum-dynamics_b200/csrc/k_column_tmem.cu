@@ -9,16 +9,18 @@
 //   GEMM2  D[128 x S] = A2[128 x S] * B2[S x S]    B2[k][l] = (l+1/2) w_k P_l(x_k)
 // The 128 GEMM rows are the real and imaginary parts of the 64 complex
 // points (row 2p = Re, 2p+1 = Im), so the complex-by-real transform is one
-// real GEMM.  FP32 accuracy from TF32 units by split products
-//   A*B ~ Ahi*(Bhi + Bmid + Blo) + Alo*Bhi,   A = Ahi + Alo,  Ahi = tf32(A),
-// with the constant Legendre matrices carried to ~2^-33 in three TF32 terms.
+// real GEMM.  FP32 accuracy from TF32 units by split products (3xTF32)
+//   A*B ~ Ahi*Bhi + Ahi*Blo + Alo*Bhi,   A = Ahi + Alo,  Ahi = tf32(A),
+// with the constant Legendre matrices split the same way on the host.
 //
 // Data placement: the A operands live in tensor memory (written by the
-// threads with tcgen05.st; each thread owns one TMEM lane = one GEMM row), the
-// constant B images in shared memory (K-major, 128-byte swizzle, built once
-// on the host), the accumulator in TMEM.  Shared memory is thus only the B
-// images, so two CTAs run on each SM and overlap each other's load / MMA /
-// epilogue phases.  TMEM per CTA: [Ahi | Alo | D], S columns each.
+// threads with tcgen05.st; each thread owns one TMEM lane = one GEMM row and
+// a quarter of its columns), the constant B images in shared memory (K-major,
+// 128-byte swizzle, built once on the host), the accumulator in TMEM.  The
+// tile's exp(-i V dt) values are staged into shared memory by asynchronous
+// copies issued while the previous tile finishes.  512 threads per CTA, two
+// CTAs per SM overlap each other's load / MMA / epilogue phases.  TMEM per
+// CTA: [Ahi | Alo | D], S columns each.
 //
 // Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
 // smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
@@ -45,7 +47,7 @@ namespace {
 
 constexpr int TPTS = 64;          // complex grid points per tile
 constexpr int MROWS = 128;        // GEMM rows per tile
-constexpr int NTHREADS = 256;
+constexpr int NTHREADS = 512;
 constexpr int MAXS = 64;          // max padded n_l / n_theta handled here
 constexpr uint32_t TMEM_COLS = 256;
 constexpr long WAIT_LIMIT = 1L << 22;   // mbarrier polls before giving up
@@ -123,6 +125,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase)
   return false;
 }
 
+__device__ __forceinline__ void cp16_zfill(void *dst, const void *src, bool valid)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;"
+               :: "r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -172,17 +180,17 @@ __device__ __forceinline__ void mma_tf32_ts(uint32_t dtmem, uint32_t atmem, uint
 }
 
 // D = A * B over K = S, A in TMEM columns [ahi, ahi+S) and [alo, alo+S), B at
-// b (hi | mid | lo, b_bytes apart): the small split terms first, main last
+// b (hi | lo, b_bytes apart): the small split terms first, main last
 template <int S>
 __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint32_t alo,
                                               uint32_t b, int b_bytes)
 {
   constexpr uint32_t idesc = make_idesc(S);
 #pragma unroll 1
-  for (int term = 0; term < 4; term++) {
-    // term 0: Ahi*Blo, 1: Ahi*Bmid, 2: Alo*Bhi, 3: Ahi*Bhi
-    const uint32_t a = term == 2 ? alo : ahi;
-    const uint32_t bt = b + (term == 0 ? 2 * b_bytes : term == 1 ? b_bytes : 0);
+  for (int term = 0; term < 3; term++) {
+    // term 0: Ahi*Blo, 1: Alo*Bhi, 2: Ahi*Bhi
+    const uint32_t a = term == 1 ? alo : ahi;
+    const uint32_t bt = b + (term == 0 ? b_bytes : 0);
 #pragma unroll
     for (int kk = 0; kk < S; kk += 8) {
       const uint32_t boff = (uint32_t)((kk >> 5) * S * 128 + ((kk & 31) >> 3) * 32);
@@ -191,7 +199,7 @@ __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint
   }
 }
 
-constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4 share a TMEM lane quarter)
+constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share a TMEM lane quarter)
 
 // EX: exact shape -- n_l = n_theta = S, n12 and n1 multiples of the tile, so
 // every point and column of a tile is valid and a tile lies in one grid row j.
@@ -206,13 +214,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   extern __shared__ unsigned char smem_raw[];
   const uint32_t base_u = smem_u32(smem_raw);
   unsigned char *base = smem_raw + ((1024u - (base_u & 1023u)) & 1023u);
-  unsigned char *B1 = base;                     // hi | mid | lo
-  unsigned char *B2 = B1 + 3 * B_BYTES;
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 3 * B_BYTES);
+  unsigned char *B1 = base;                     // hi | lo
+  unsigned char *B2 = B1 + 2 * B_BYTES;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 2 * B_BYTES);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *wk = xch + 4 * NG * TPTS;                        // [S] w_k (float), 0 beyond n_theta
   float *linv = wk + S;                                   // [S] 1/(l+1/2)
+  float2 *evs = reinterpret_cast<float2 *>(linv + S);     // [S][TPTS] exp(-i V dt) of a tile
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int row = (warp & 3) * 32 + lane;        // TMEM lane == GEMM row
@@ -233,9 +242,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb3));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    // the B images (6 * B_BYTES, a multiple of 16) by bulk asynchronous copies
+    // the B images (4 * B_BYTES, a multiple of 16) by bulk asynchronous copies
     // from this GPU's global memory into this CTA's shared memory
-    constexpr uint32_t total = 6 * B_BYTES, chunk = 16384;
+    constexpr uint32_t total = 4 * B_BYTES, chunk = 16384;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                  :: "r"(mb3), "r"(total) : "memory");
     const char *src = reinterpret_cast<const char *>(t.mats);
@@ -286,7 +295,23 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       else a[u] = (ok && c0 + u < nl) ? __ldg(src + u * stride) : 0.f;               \
     }                                                                                \
   } while (0)
+  // exp(-i V dt) of tile tl into evs, 16-byte asynchronous copies (zero-filled
+  // past n_theta and past the grid; n12 is even, so a copy never straddles it)
+#define QD_STAGE_EV(tl)                                                              \
+  do {                                                                               \
+    if ((tl) < ntiles) {                                                             \
+      const int rr = (tl) / tpr, qb = ((tl) - rr * tpr) * TPTS;                      \
+      const float2 *eb = expv + (size_t)rr * p.vrun + qb;                            \
+      for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
+        const int k = x / (TPTS / 2), c2 = 2 * (x % (TPTS / 2));                     \
+        const bool okv = k < nth && qb + c2 < n12;                                   \
+        cp16_zfill(&evs[k * TPTS + c2], okv ? eb + (size_t)k * n12 + c2 : expv, okv); \
+      }                                                                              \
+    }                                                                                \
+    asm volatile("cp.async.commit_group;" ::: "memory");                             \
+  } while (0)
   if (mode != COL_HEAD) QD_PREFETCH_A((int)blockIdx.x);
+  if (mode == COL_MID) QD_STAGE_EV((int)blockIdx.x);
 
   for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
     const int run = tile / tpr;
@@ -297,7 +322,6 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     if (EX) { j = q0 / n1; i = q0 - j * n1 + pt; }
     else { j = qok ? q / n1 : 0; i = qok ? q - (q / n1) * n1 : 0; }
     const size_t voff = (size_t)run * p.vrun;
-    float2 ev[H];
     float sc = 1.f;
 
     if (mode != COL_HEAD) {
@@ -319,15 +343,6 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
         gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
         mma_commit(mb1);
       }
-      if (mode == COL_MID) {                    // V phase of the tile, in flight during GEMM1
-        const float2 *ep = expv + voff + (size_t)c0 * n12 + q;
-#pragma unroll
-        for (int u = 0; u < H; u++) {
-          float2 e = make_float2(1.f, 0.f);
-          if (EX || (qok && c0 + u < nth)) e = __ldg(ep + u * n12);
-          ev[u] = make_float2(e.x, e.y * ysg);
-        }
-      }
       float n_l = 0.f;
 #pragma unroll
       for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
@@ -345,6 +360,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       }
       nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
       if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
+      if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
       __syncthreads();
       float n_t = 0.f;
 #pragma unroll
@@ -379,7 +395,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           }
           if (mode == COL_MID) {
             const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-            v[x] = fmaf(other, ev[u + x].y, mine * ev[u + x].x);
+            const float2 e = evs[k * TPTS + pt];
+            v[x] = fmaf(other * ysg, e.y, mine * e.x);
           } else {
             v[x] = mine;
           }
@@ -427,6 +444,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       QD_PREFETCH_A(tile + (int)gridDim.x);
       continue;
     }
+    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: D = A2 * B2 -------------------------------------------------------------
     if (tid == 0) {
@@ -472,8 +490,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     tc_fence_before();
   }
 #undef QD_PREFETCH_A
+#undef QD_STAGE_EV
 
   if (failed && lane == 0) atomicExch(t.status, 1);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -526,7 +546,8 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 
 template <int S> constexpr int smem_bytes_for()
 {
-  return 1024 + 6 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4;
+  return 1024 + 4 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
+         S * TPTS * 8;
 }
 
 // P_l(x_k) for l = 0..lmax by the recurrence of LegendreP2.m:9-21 (FP64)
@@ -578,17 +599,14 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const 
   }
   const int nka = (S + 31) / 32;
   const int bb = nka * S * 128;
-  std::vector<unsigned char> img(6 * (size_t)bb, 0);
-  unsigned char *b1 = img.data(), *b2 = b1 + 3 * bb;
-  auto put = [&](unsigned char *img3, int r, int k, double val) {
+  std::vector<unsigned char> img(4 * (size_t)bb, 0);
+  unsigned char *b1 = img.data(), *b2 = b1 + 2 * bb;
+  auto put = [&](unsigned char *img2, int r, int k, double val) {     // hi | lo
     const float h = tf32_round_host((float)val);
-    const double r1 = val - (double)h;
-    const float m = tf32_round_host((float)r1);
-    const float l = tf32_round_host((float)(r1 - (double)m));
+    const float l = tf32_round_host((float)(val - (double)h));
     const uint32_t off = sw128_off(r, k, S);
-    std::memcpy(img3 + off, &h, 4);
-    std::memcpy(img3 + bb + off, &m, 4);
-    std::memcpy(img3 + 2 * bb + off, &l, 4);
+    std::memcpy(img2 + off, &h, 4);
+    std::memcpy(img2 + bb + off, &l, 4);
   };
   const int lrows = renorm ? nth : nl;          // orders formed by GEMM2
   for (int k = 0; k < nth; k++) {

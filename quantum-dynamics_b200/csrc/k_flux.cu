@@ -4,10 +4,11 @@
 //                  Gradient3.F:31-167 (3..11 points, same coefficient order),
 //                  from the surface rows captured by the column pass; stored
 //                  in FP64 in a history ring (one slot per step).
-//   k_flux_accum   phi_E += sum_t dt e^{iE t} psi_s(t), dphi_E likewise
-//                  (PsiTimeToPsiEnergyOnSurface, CRPAux.F:4-31, with the
-//                  e^{iEt} recurrence of timeEvol.C:807-817 evaluated
-//                  directly): a complex FP64 GEMM over a chunk of steps.
+//   k_flux_phase   the factors dt e^{iE t} of a chunk of steps (the e^{iEt}
+//                  recurrence of timeEvol.C:807-817 evaluated directly, FP64)
+//   k_flux_gemm    phi_E += sum_t dt e^{iE t} psi_s(t), dphi_E likewise
+//                  (PsiTimeToPsiEnergyOnSurface, CRPAux.F:4-31): a
+//                  register-tiled complex FP64 GEMM over the chunk.
 //   k_crp          P(E) = Im(sum_k w_k sum_i conj(phi) dphi) / eta^2 dr1/mu2
 //                  (CalculateCRP, CRPAux.F:34-66), warp-shuffle reduction.
 #include "qd_kernels.h"
@@ -22,50 +23,106 @@ __global__ void k_flux_prep(FluxParams p)
   if (q < p.nruns * p.nth * p.n1) flux_point<C>(p, q);
 }
 
-constexpr int EB = 8;          // energies per CTA
 constexpr int TMAX = 128;      // max steps per chunk
 
-__global__ void __launch_bounds__(256) k_flux_accum(AccumParams p)
+// phase[run][e][t] = dt e^{i E_e (t0 + t + 1) dt} of this chunk, FP64
+__global__ void __launch_bounds__(256) k_flux_phase(AccumParams p)
 {
-  __shared__ double2 ph[EB][TMAX];
-  const int e0 = blockIdx.y * EB;
-  const int run = blockIdx.z;
-  const double *energies = p.energies + (long)run * p.ne;
-  for (int x = threadIdx.x; x < EB * p.nt; x += blockDim.x) {
-    const int e = x / p.nt, t = x % p.nt;
-    double2 c = make_double2(0.0, 0.0);
-    if (e0 + e < p.ne) {
-      const double edt = energies[e0 + e] * p.dt;
-      double sn, cs;
-      sincos(edt * (double)(p.t0 + t + 1), &sn, &cs);
-      c = make_double2(p.dt * cs, p.dt * sn);
-    }
-    ph[e][t] = c;
+  const int n = p.nruns * p.ne * p.nt;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+    const int t = x % p.nt, re = x / p.nt;                 // re = run * ne + e
+    double sn, cs;
+    sincos(p.energies[re] * p.dt * (double)(p.t0 + t + 1), &sn, &cs);
+    p.phase[(size_t)re * TMAX + t] = make_double2(p.dt * cs, p.dt * sn);
   }
-  __syncthreads();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= p.nq) return;
-  double2 a[EB], b[EB];
-#pragma unroll
-  for (int e = 0; e < EB; e++) { a[e] = make_double2(0, 0); b[e] = make_double2(0, 0); }
-  for (int t = 0; t < p.nt; t++) {
-    const long o = ((long)t * p.nruns + run) * p.nq + q;
-    const double2 zp = p.ring_psi[o];
-    const double2 zg = p.ring_g[o];
-#pragma unroll
-    for (int e = 0; e < EB; e++) {
-      const double2 c = ph[e][t];
-      a[e].x += c.x * zp.x - c.y * zp.y; a[e].y += c.x * zp.y + c.y * zp.x;
-      b[e].x += c.x * zg.x - c.y * zg.y; b[e].y += c.x * zg.y + c.y * zg.x;
+}
+
+// phi[e][q] += sum_t phase[e][t] psi_s[t][q] (and dphi with the gradient), a
+// complex FP64 GEMM per run.  CTA tile: GE energies x GQ surface points x
+// {psi_s, d psi_s}; each thread owns 4 energies x 4 columns (2 points x 2
+// fields) in registers.  KT steps of phases and history are staged in shared
+// memory by asynchronous copies into two buffers, so the next KT steps load
+// while the current ones are multiplied; the history is read from HBM once
+// per energy tile.
+constexpr int GE = 64, GQ = 32, KT = 10;
+
+__device__ __forceinline__ void cp16(void *dst, const void *src, bool valid)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;                 // 0: fill the 16 bytes with zeros
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" :: "r"(d), "l"(src), "r"(n)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(256) k_flux_gemm(AccumParams p)
+{
+  __shared__ double2 As[2][GE][KT + 1];         // phases (padded rows)
+  __shared__ double2 Bs[2][KT][2 * GQ];         // cols 0..GQ-1 psi_s, GQ..2GQ-1 gradient
+  const int tid = threadIdx.x;
+  const int te = tid >> 4, tc = tid & 15;       // 16 energy groups x 16 column groups
+  const int e0 = blockIdx.x * GE, q0 = blockIdx.y * GQ, run = blockIdx.z;
+  const double2 *ph = p.phase + ((size_t)run * p.ne) * TMAX;
+  auto stage = [&](int buf, int t0) {
+    for (int x = tid; x < GE * KT; x += 256) {
+      const int e = x / KT, t = x % KT;
+      const bool ok = e0 + e < p.ne && t0 + t < p.nt;
+      cp16(&As[buf][e][t], ok ? ph + (size_t)(e0 + e) * TMAX + t0 + t : ph, ok);
     }
+    for (int x = tid; x < KT * 2 * GQ; x += 256) {
+      const int t = x / (2 * GQ), c = x % (2 * GQ), q = q0 + (c % GQ);
+      const bool ok = t0 + t < p.nt && q < p.nq;
+      const size_t o = ok ? ((size_t)(t0 + t) * p.nruns + run) * p.nq + q : 0;
+      cp16(&Bs[buf][t][c], (c < GQ ? p.ring_psi : p.ring_g) + o, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0.0, 0.0);
+  const int nchunk = (p.nt + KT - 1) / KT;
+  stage(0, 0);
+  for (int ch = 0; ch < nchunk; ch++) {
+    const int buf = ch & 1;
+    if (ch + 1 < nchunk) {
+      stage(buf ^ 1, (ch + 1) * KT);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int k = 0; k < KT; k++) {             // rows past nt were zero-filled
+      double2 a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[buf][te + 16 * i][k];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[buf][k][tc + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          acc[i][j].x = fma(a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
+          acc[i][j].y = fma(a[i].x, b[j].y, fma(a[i].y, b[j].x, acc[i][j].y));
+        }
+    }
+    __syncthreads();                            // buffer free for the stage after next
   }
 #pragma unroll
-  for (int e = 0; e < EB; e++) {
-    if (e0 + e >= p.ne) break;
-    const long o = ((long)run * p.ne + e0 + e) * p.nq + q;
-    double2 f = p.fai[o], df = p.dfai[o];
-    f.x += a[e].x; f.y += a[e].y; df.x += b[e].x; df.y += b[e].y;
-    p.fai[o] = f; p.dfai[o] = df;
+  for (int i = 0; i < 4; i++) {
+    const int e = e0 + te + 16 * i;
+    if (e >= p.ne) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int c = tc + 16 * j, q = q0 + (c % GQ);
+      if (q >= p.nq) continue;
+      double2 *dst = (c < GQ ? p.fai : p.dfai) + ((size_t)run * p.ne + e) * p.nq + q;
+      double2 f = *dst;
+      f.x += acc[i][j].x;
+      f.y += acc[i][j].y;
+      *dst = f;
+    }
   }
 }
 
@@ -101,8 +158,10 @@ cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 {
   if (p.nt <= 0) return cudaSuccess;
   if (p.nt > TMAX) return cudaErrorInvalidValue;
-  dim3 grid((p.nq + 255) / 256, (p.ne + EB - 1) / EB, p.nruns);
-  k_flux_accum<<<grid, 256, 0, s>>>(p);
+  const int n = p.nruns * p.ne * p.nt;
+  k_flux_phase<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, s>>>(p);
+  dim3 grid((p.ne + GE - 1) / GE, (p.nq + GQ - 1) / GQ, p.nruns);
+  k_flux_gemm<<<grid, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -111,3 +170,5 @@ cudaError_t launch_crp(const CrpParams &p, cudaStream_t s)
   k_crp<<<p.nruns * p.ne, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
+
+int flux_accum_launches() { return 2; }

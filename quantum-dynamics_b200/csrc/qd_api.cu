@@ -132,6 +132,7 @@ struct qd_handle {
   double2 *d_psi_z = nullptr;
   void *d_surf = nullptr;
   double2 *d_ring_psi = nullptr, *d_ring_g = nullptr, *d_fai = nullptr, *d_dfai = nullptr;
+  double2 *d_phase = nullptr;     // chunk phase factors [run][E][128]
   double *d_energies = nullptr, *d_eta = nullptr, *d_crp = nullptr;
   double *d_norms = nullptr;
   int norms_cap = 0;
@@ -338,9 +339,10 @@ int after_flux_prep(qd_handle *h)
     a.nruns = h->nruns;
     a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
     a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+    a.phase = h->d_phase;
     TRY(prof_mark(h, -1));
     CU(launch_flux_accum(a, h->st));
-    g_launches++;
+    g_launches += flux_accum_launches();
     TRY(prof_mark(h, PROF_ACCUM));
     h->acc_done += h->ring_fill;
     h->ring_fill = 0;
@@ -457,8 +459,9 @@ int flush_accum(qd_handle *h)
   a.nruns = h->nruns;
   a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
   a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+  a.phase = h->d_phase;
   CU(launch_flux_accum(a, h->st));
-  g_launches++;
+  g_launches += flux_accum_launches();
   h->acc_done += h->ring_fill;
   h->ring_fill = 0;
   return QD_OK;
@@ -718,6 +721,7 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     TRY(h->alloc(h->d_ring_g, nq * QD_RING * nruns));
     TRY(h->alloc(h->d_fai, nq * h->ne * nruns));
     TRY(h->alloc(h->d_dfai, nq * h->ne * nruns));
+    TRY(h->alloc(h->d_phase, (size_t)h->ne * 128 * nruns));
     CU(cudaMemsetAsync(h->d_fai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
     CU(cudaMemsetAsync(h->d_dfai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
     TRY(h->alloc(h->d_energies, (size_t)h->ne * nruns));

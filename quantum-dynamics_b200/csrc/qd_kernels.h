@@ -146,7 +146,9 @@ struct AccumParams {
   const double *energies;
   const double2 *ring_psi, *ring_g;
   double2 *fai, *dfai;
+  double2 *phase;          // workspace [nruns][ne][128] for the chunk's e^{iEt} factors
 };
+int flux_accum_launches();
 
 struct CrpParams {
   int n1, nth, ne, nruns;
