@@ -28,8 +28,10 @@
 // isometries per grid column in the quadrature norms -- B (l -> theta)
 // whenever n_l <= n_theta (Gauss quadrature is exact to degree 2 n_theta - 1),
 // F (theta -> l) when its output is taken over all n_theta orders -- so each
-// column's output is rescaled to the exactly known input norm:
-//   sum_k w_k |psi_theta|^2 = sum_l |psi_l|^2/(l+1/2).
+// column's output is rescaled to the exactly known norm
+//   sum_k w_k |psi_theta|^2 = sum_l |psi_l|^2/(l+1/2)
+// (times the absorber squared).  The state is kept in the orthonormal basis
+// psi'_l = psi_l/sqrt(l+1/2), where these norms are plain sums of squares.
 // For n_l < n_theta, GEMM2 also forms the orders n_l..n_theta-1 (rows from the
 // same three-term recurrence) for the norm only; they are not stored.  This
 // fixes the magnitude only; shape and phase stay as computed.
@@ -203,6 +205,17 @@ constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share
 
 // EX: exact shape -- n_l = n_theta = S, n12 and n1 multiples of the tile, so
 // every point and column of a tile is valid and a tile lies in one grid row j.
+//
+// Orthonormal representation.  The l-space state is kept as
+// psi'_l = psi_l / sqrt(l+1/2) and theta values as sqrt(w_k) psi(theta_k), so
+// both transforms use the same matrix Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k)
+// (B: D1 = Q psi', F: psi' = Q^T A2) and every norm is a plain sum of squares.
+// Renormalisation.  The column output is rescaled to the norm the exact
+// transform pair would give, dd^2 * sum_l |psi'_l|^2 per grid column (dd =
+// absorber); the theta-space intermediate needs its own scale only where it
+// leaves the kernel (flux rows, psi_z, the last step of a call: the "slow"
+// tiles), elsewhere GEMM2 runs on V * D1 unscaled and one factor
+// dd sqrt(n_l / n_out) at the store does both.
 template <int S, int MODE, bool EX>
 __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev t)
 {
@@ -219,9 +232,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 2 * B_BYTES);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
-  float *wk = xch + 4 * NG * TPTS;                        // [S] w_k (float), 0 beyond n_theta
-  float *linv = wk + S;                                   // [S] 1/(l+1/2)
-  float2 *evs = reinterpret_cast<float2 *>(linv + S);     // [S][TPTS] exp(-i V dt) of a tile
+  float *sw = xch + 4 * NG * TPTS;                        // [S] sqrt(w_k), 0 beyond n_theta
+  float *rsw = sw + S;                                    // [S] 1/sqrt(w_k)
+  float2 *evs = reinterpret_cast<float2 *>(rsw + S);      // [S][TPTS] exp(-i V dt) of a tile
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int row = (warp & 3) * 32 + lane;        // TMEM lane == GEMM row
@@ -256,8 +269,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     }
   }
   for (int i = tid; i < S; i += NTHREADS) {
-    wk[i] = i < p.nth ? (float)p.w[i] : 0.f;
-    linv[i] = (float)(1.0 / (i + 0.5));
+    const double w = i < p.nth ? p.w[i] : 0.0;
+    sw[i] = (float)sqrt(w);
+    rsw[i] = w > 0.0 ? (float)(1.0 / sqrt(w)) : 0.f;
   }
   tc_fence_before();
   __syncthreads();
@@ -282,7 +296,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   float *surf = reinterpret_cast<float *>(p.surf);
   double *psiz = reinterpret_cast<double *>(p.psi_z);
   const float2 *expv = p.expV32;
-  const float ysg = is_im ? 1.f : -1.f;         // out = mine e.x + ysg other e.y
+  const float ysg = is_im ? 1.f : -1.f;         // V z: mine e.x + ysg other e.y
 
   float a[H];
 #define QD_PREFETCH_A(tl)                                                            \
@@ -322,63 +336,63 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     if (EX) { j = q0 / n1; i = q0 - j * n1 + pt; }
     else { j = qok ? q / n1 : 0; i = qok ? q - (q / n1) * n1 : 0; }
     const size_t voff = (size_t)run * p.vrun;
-    float sc = 1.f;
+    const float ddv = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) : 1.f;
+    const bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
+                      j < p.surf_j0 + p.surf_nrows;
+    // slow tiles form the scaled theta-space state (EX: frow is uniform per tile)
+    const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow;
+    float n_l = 0.f, sc = 1.f;
 
     if (mode != COL_HEAD) {
-      // ---- A1 = psi_l tile into TMEM, its l-space norm, GEMM1 ----------------------
+      // ---- A1 = psi'_l tile into TMEM, its norm, GEMM1 --------------------------------
       float nl_part = 0.f;
 #pragma unroll
       for (int u = 0; u < H; u += 4) {
         put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
-        nl_part += a[u] * a[u] * linv[c0 + u] + a[u + 1] * a[u + 1] * linv[c0 + u + 1] +
-                   a[u + 2] * a[u + 2] * linv[c0 + u + 2] + a[u + 3] * a[u + 3] * linv[c0 + u + 3];
+        nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
+                  fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
       }
       tmem_wait_st();
       tc_fence_before();
       nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
       if (!is_im) xch[grp * TPTS + pt] = nl_part;
+      if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
       __syncthreads();
       if (tid == 0) {
         tc_fence_after();
         gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
         mma_commit(mb1);
       }
-      float n_l = 0.f;
 #pragma unroll
       for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
-      // theta-space norm of the GEMM1 output -> isometry scale
-      float nt_part = 0.f;
+      if (slow) {                               // theta norm of GEMM1 -> isometry scale
+        float nt_part = 0.f;
 #pragma unroll
-      for (int u = 0; u < H; u += 4) {
-        float v0, v1, v2, v3;
-        tmem_ld4(my_d + u, v0, v1, v2, v3);
-        nt_part += wk[c0 + u] * v0 * v0 + wk[c0 + u + 1] * v1 * v1 +
-                   wk[c0 + u + 2] * v2 * v2 + wk[c0 + u + 3] * v3 * v3;
+        for (int u = 0; u < H; u += 4) {
+          float v0, v1, v2, v3;
+          tmem_ld4(my_d + u, v0, v1, v2, v3);
+          nt_part = fmaf(v0, v0, fmaf(v1, v1, fmaf(v2, v2, fmaf(v3, v3, nt_part))));
+        }
+        nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
+        if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
+        __syncthreads();
+        float n_t = 0.f;
+#pragma unroll
+        for (int g = 0; g < NG; g++) n_t += xch[NG * TPTS + g * TPTS + pt];
+        sc = (t.renorm && n_t > 0.f) ? sqrtf(n_l / n_t) : 1.f;
       }
-      nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
-      if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
-      if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
-      __syncthreads();
-      float n_t = 0.f;
-#pragma unroll
-      for (int g = 0; g < NG; g++) n_t += xch[NG * TPTS + g * TPTS + pt];
-      sc = (t.renorm && n_t > 0.f) ? sqrtf(n_l / n_t) : 1.f;
     }
 
     // ---- theta-space operations, A2 into TMEM ----------------------------------------
-    // tsum: this thread's share of sum_k w_k |psi_k|^2 of its point after the
-    // absorber; |exp(-i V dt)| = 1, so it is also the theta norm of GEMM2's input
-    float tsum = 0.f;
-    const float dd = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) * sc : sc;
-    bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
-                j < p.surf_j0 + p.surf_nrows;
-    float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
-                       : nullptr;
+    float tsum = 0.f;                           // this thread's share of sum_k |theta'_k|^2
+    const float sin_ = sc * ddv;                // slow tiles: scaled theta values
     double *zrow = (mode != COL_HEAD && p.out_z) ? psiz + 2 * ((size_t)run * nth * n12 + q) + comp
                                                  : nullptr;
+    float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
+                       : nullptr;
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
       float v[4];
@@ -387,18 +401,19 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #pragma unroll
         for (int x = 0; x < 4; x++) {
           const int k = c0 + u + x;
-          const float mine = v[x] * dd;
-          tsum += wk[k] * mine * mine;
-          if (EX || (qok && k < nth)) {
-            if (frow) srow[(size_t)2 * k * n1] = mine;
-            if (zrow) zrow[(size_t)2 * k * n12] = mine;
+          float mine = v[x];
+          if (slow) {
+            mine *= sin_;
+            tsum = fmaf(mine, mine, tsum);
+            if (EX || (qok && k < nth)) {
+              if (srow) srow[(size_t)2 * k * n1] = mine * rsw[k];
+              if (zrow) zrow[(size_t)2 * k * n12] = mine * rsw[k];
+            }
           }
           if (mode == COL_MID) {
             const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
             const float2 e = evs[k * TPTS + pt];
             v[x] = fmaf(other * ysg, e.y, mine * e.x);
-          } else {
-            v[x] = mine;
           }
         }
       } else {
@@ -417,25 +432,32 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
               sincos(0.5 * atan2(-s, c), &sh, &ch);
               f = make_double2(ch, sh);
             }
-            val = (float)(is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y);
+            val = (float)((is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y) * sqrt(p.w[k]));
           }
           v[x] = val;
-          tsum += wk[k] * val * val;
+          tsum = fmaf(val, val, tsum);
         }
       }
       if (mode != COL_TAIL) put4_tmem(my_hi + u, my_lo + u, v[0], v[1], v[2], v[3]);
     }
-    // per-point theta norm (both components, both column groups)
-    tsum += __shfl_xor_sync(0xffffffffu, tsum, 1);
-    if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = tsum;
+    // target norm of the column output (and the step norm of the point)
+    float target;
+    if (slow || mode == COL_HEAD) {
+      tsum += __shfl_xor_sync(0xffffffffu, tsum, 1);
+      if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = tsum;
+    }
     if (mode != COL_TAIL) tmem_wait_st();
     tc_fence_before();
     __syncthreads();
-    float n_t2 = 0.f;
+    if (slow || mode == COL_HEAD) {
+      target = 0.f;
 #pragma unroll
-    for (int g = 0; g < NG; g++) n_t2 += xch[2 * NG * TPTS + g * TPTS + pt];
+      for (int g = 0; g < NG; g++) target += xch[2 * NG * TPTS + g * TPTS + pt];
+    } else {
+      target = ddv * ddv * n_l;
+    }
     if (p.norm_out && mode != COL_HEAD) {       // this tile's share of its run's norm
-      double s = (grp == 0 && !is_im && qok) ? (double)n_t2 : 0.0;
+      double s = (grp == 0 && !is_im && qok) ? (double)target : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
@@ -446,7 +468,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     }
     if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
-    // ---- GEMM2: D = A2 * B2 -------------------------------------------------------------
+    // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
       tc_fence_after();
       gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
@@ -462,13 +484,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       float v0, v1, v2, v3;
       tmem_ld4(my_d + u, v0, v1, v2, v3);
       if (EX) {
-        no_part += v0 * v0 * linv[c0 + u] + v1 * v1 * linv[c0 + u + 1] +
-                   v2 * v2 * linv[c0 + u + 2] + v3 * v3 * linv[c0 + u + 3];
+        no_part = fmaf(v0, v0, fmaf(v1, v1, fmaf(v2, v2, fmaf(v3, v3, no_part))));
       } else {
-        no_part += (c0 + u < t.nnorm ? v0 * v0 * linv[c0 + u] : 0.f) +
-                   (c0 + u + 1 < t.nnorm ? v1 * v1 * linv[c0 + u + 1] : 0.f) +
-                   (c0 + u + 2 < t.nnorm ? v2 * v2 * linv[c0 + u + 2] : 0.f) +
-                   (c0 + u + 3 < t.nnorm ? v3 * v3 * linv[c0 + u + 3] : 0.f);
+        no_part += (c0 + u < t.nnorm ? v0 * v0 : 0.f) + (c0 + u + 1 < t.nnorm ? v1 * v1 : 0.f) +
+                   (c0 + u + 2 < t.nnorm ? v2 * v2 : 0.f) + (c0 + u + 3 < t.nnorm ? v3 * v3 : 0.f);
       }
     }
     no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
@@ -477,7 +496,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     float n_o = 0.f;
 #pragma unroll
     for (int g = 0; g < NG; g++) n_o += xch[3 * NG * TPTS + g * TPTS + pt];
-    const float sc2 = (t.renorm && n_o > 0.f) ? sqrtf(n_t2 / n_o) : 1.f;
+    float so;
+    if (t.renorm) so = n_o > 0.f ? sqrtf(target / n_o) : 1.f;
+    else so = (slow || mode == COL_HEAD) ? 1.f : ddv;
     float *dst = ldst + (size_t)run * nl * stride + (size_t)c0 * stride + 2 * q + comp;
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
@@ -485,7 +506,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
 #pragma unroll
       for (int x = 0; x < 4; x++)
-        if (EX || (qok && c0 + u + x < nl)) dst[(u + x) * stride] = v[x] * sc2;
+        if (EX || (qok && c0 + u + x < nl)) dst[(u + x) * stride] = v[x] * so;
     }
     tc_fence_before();
   }
@@ -547,7 +568,7 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 template <int S> constexpr int smem_bytes_for()
 {
   return 1024 + 4 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
-         S * TPTS * 8;
+         S * TPTS * 8;   // B images, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
 
 // P_l(x_k) for l = 0..lmax by the recurrence of LegendreP2.m:9-21 (FP64)
@@ -609,11 +630,14 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const 
     std::memcpy(img2 + bb + off, &l, 4);
   };
   const int lrows = renorm ? nth : nl;          // orders formed by GEMM2
+  // both images hold Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k) (orthonormal basis)
   for (int k = 0; k < nth; k++) {
-    for (int l = 0; l < nl; l++) put(b1, k, l, legendre[l + (long)k * nl]);   // B1: row k, K = l
-    for (int l = 0; l < lrows; l++) {
+    const double swk = std::sqrt(w[k]);
+    for (int l = 0; l < nl; l++)                                              // B1: row k, K = l
+      put(b1, k, l, swk * std::sqrt(l + 0.5) * legendre[l + (long)k * nl]);
+    for (int l = 0; l < lrows; l++) {                                         // B2: row l, K = k
       const double P = l < nl ? legendre[l + (long)k * nl] : Pext[(size_t)k * nth + l];
-      put(b2, l, k, (l + 0.5) * w[k] * P);                                     // B2: row l, K = k
+      put(b2, l, k, swk * std::sqrt(l + 0.5) * P);
     }
   }
   void *d = nullptr;

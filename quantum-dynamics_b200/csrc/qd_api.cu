@@ -821,14 +821,18 @@ int energies(qd_handle *h, int run, double out4[4])
 }
 
 // ---- checkpoint / restore ----------------------------------------------------
-constexpr uint64_t CKPT_MAGIC = 0x31544b5044514251ull;   // file tag
+constexpr uint64_t CKPT_MAGIC = 0x32544b5044514251ull;   // file tag, layout version 2
 
 struct CkptHeader {
   uint64_t magic;
   int32_t prec, nruns, n1, n2, nth, nl, ne, npts;
   int32_t steps, started, last_finalized, ring_fill, flux_pending;
+  int32_t basis;               // l-space representation: 0 psi_l, 1 psi_l / sqrt(l+1/2)
   int64_t acc_done;
 };
+
+// The complex64 tensor-core column pass keeps psi_l in the orthonormal basis.
+int lspace_basis(const qd_handle *h) { return h->prec == QD_PREC_FP32 && h->use_tc ? 1 : 0; }
 
 int checkpoint(qd_handle *h, const char *path)
 {
@@ -838,6 +842,7 @@ int checkpoint(qd_handle *h, const char *path)
   hd.nth = h->nth; hd.nl = h->nl; hd.ne = h->do_crp ? h->ne : 0; hd.npts = h->npts;
   hd.steps = h->steps; hd.started = h->started; hd.last_finalized = h->last_finalized;
   hd.ring_fill = h->ring_fill; hd.flux_pending = h->flux_pending; hd.acc_done = h->acc_done;
+  hd.basis = lspace_basis(h);
   const size_t csz = h->prec == QD_PREC_FP64 ? sizeof(double2) : sizeof(float2);
   std::vector<std::pair<const void *, size_t>> blocks;
   const size_t nq = (size_t)h->nth * h->n1;
@@ -884,6 +889,11 @@ int restore(qd_handle *h, const char *path)
       hd.npts != h->npts) {
     fclose(f);
     return set_err(QD_ERR_INVALID, "checkpoint \"%s\" was written for other sizes", path);
+  }
+  if (hd.basis != lspace_basis(h)) {
+    fclose(f);
+    return set_err(QD_ERR_INVALID, "checkpoint \"%s\" was written by another column-pass kernel "
+                   "(l-space basis %d, this handle %d)", path, hd.basis, lspace_basis(h));
   }
   uint64_t nnorm = 0;
   bool ok = fread(&nnorm, sizeof nnorm, 1, f) == 1 && nnorm < (1ull << 40);
