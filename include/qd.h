@@ -247,6 +247,46 @@ int qd_read_grids(const char *dir, int32_t n, double *x, double *w);
  * recurrence of common/LegendreP2.m:9-21, computed in FP64 on the GPU. */
 int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre);
 
+/* ---- potential on the Jacobi grid (H3/H3PESJacobi.m:5-27) --------------- */
+
+/* A PES in the convention of the reference's PES MEX functions
+ * (FH2/HSW/HSWMex.C:29-90, called as H3PES(r12, r23, r13) by
+ * H3/H3PESJacobi.m:25): V[m] = V(r12[m], r23[m], r13[m]) for n points,
+ * internuclear distances in bohr (atom 1 = the atom, 2 3 = the diatom), V in
+ * hartree.  Return 0 on success; any other value aborts with QD_ERR_PES. */
+typedef int (*qd_pes_fn)(int64_t n, const double *r12, const double *r23, const double *r13,
+                         double *V, void *ctx);
+
+/* pot_out (n1 x n2 x n_theta, the layout of qd_data.pot) on the Jacobi grid
+ * R = r1.r, r = r2.r, cos(theta) = theta.x: r23 = r,
+ * r12 = sqrt((f2 r)^2 + R^2 - 2 f2 r R cos), r13 = sqrt((f3 r)^2 + R^2 + 2 f3 r R cos),
+ * f2 = masses[2]/(masses[1]+masses[2]), f3 = 1 - f2.  Points with any distance
+ * <= rmin get vmax; if cap, V is also capped at vmax.  One callback for all
+ * other points, on the calling thread. */
+int qd_potential_jacobi(const qd_radial *R, const qd_radial *r, const qd_angle *theta,
+                        const double masses[3], qd_pes_fn pes, void *ctx, double vmax,
+                        double rmin, int32_t cap, double *pot_out);
+
+/* Extended-LEPS surface V = De(BC) + Q_AB + Q_BC + Q_AC
+ * - sqrt(J_AB^2 + J_BC^2 + J_AC^2 - J_AB J_BC - J_BC J_AC - J_AC J_AB), per pair
+ * Q, J = (De (y-2) +- pf (y+2)) y / 2, y = exp(-beta (r - re)),
+ * pf = De (1 - sato)/(1 + sato) / 2 (the algebra of ClH2/G3/clh2g3v.F:88-101).
+ * No counterpart in the reference's propagator; evaluated on the GPU in FP64. */
+typedef struct qd_leps_pair {
+  double de;      /* hartree */
+  double beta;    /* 1/bohr */
+  double re;      /* bohr */
+  double sato;
+} qd_leps_pair;
+typedef struct qd_leps {
+  qd_leps_pair ab;  /* atom - diatom atom 2 (r12) */
+  qd_leps_pair bc;  /* the diatom (r23)           */
+  qd_leps_pair ac;  /* atom - diatom atom 3 (r13) */
+} qd_leps;
+int qd_potential_leps(const qd_radial *R, const qd_radial *r, const qd_angle *theta,
+                      const double masses[3], const qd_leps *leps, double vmax, double rmin,
+                      int32_t cap, double *pot_out);
+
 #ifdef __cplusplus
 }
 #endif

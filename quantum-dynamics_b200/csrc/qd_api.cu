@@ -104,6 +104,14 @@ bool all_finite(const double *a, size_t n)
 
 }  // namespace
 
+// error reporting for the other translation units of the library (qd_err.h)
+int qd_set_error(int code, const char *msg)
+{
+  g_err = msg;
+  return code;
+}
+void qd_count_launches(int n) { g_launches += n; }
+
 struct qd_handle {
   qd_data *data = nullptr;        // run 0 (holds the fields shared by the batch)
   std::vector<qd_data *> runs;    // all runs of the batch

@@ -64,6 +64,19 @@ class QdData(C.Structure):
                 ("CRP", QdCrp)]
 
 
+PES_FN = C.CFUNCTYPE(C.c_int, C.c_int64, c_double_p, c_double_p, c_double_p, c_double_p,
+                     C.c_void_p)
+
+
+class QdLepsPair(C.Structure):
+    _fields_ = [("de", C.c_double), ("beta", C.c_double), ("re", C.c_double),
+                ("sato", C.c_double)]
+
+
+class QdLeps(C.Structure):
+    _fields_ = [("ab", QdLepsPair), ("bc", QdLepsPair), ("ac", QdLepsPair)]
+
+
 def _ptr(a):
     """double* into a C-contiguous float64 numpy array (None -> NULL)."""
     if a is None:
@@ -182,6 +195,12 @@ def lib():
         "qd_energies_noalloc": (C.c_int, [H, C.c_int32, c_double_p]),
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
+        "qd_potential_jacobi": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
+                                          PES_FN, C.c_void_p, C.c_double, C.c_double,
+                                          C.c_int32, c_double_p]),
+        "qd_potential_leps": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
+                                        P(QdLeps), C.c_double, C.c_double, C.c_int32,
+                                        c_double_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

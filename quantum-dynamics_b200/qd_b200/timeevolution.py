@@ -168,3 +168,62 @@ def kernel_launch_count():
 def set_device(device):
     """CUDA device for the calling thread's later library calls."""
     check(lib().qd_set_device(int(device)))
+
+
+def _grid_structs(R, r, x):
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    a, b, t = _abi.QdRadial(), _abi.QdRadial(), _abi.QdAngle()
+    a.n, a.r = R.size, R.ctypes.data_as(_abi.c_double_p)
+    b.n, b.r = r.size, r.ctypes.data_as(_abi.c_double_p)
+    t.n, t.x = x.size, x.ctypes.data_as(_abi.c_double_p)
+    return (a, b, t), (R, r, x)
+
+
+def potential_jacobi(R, r, x, masses, pes, vmax=2.5, rmin=0.4, cap=True):
+    """V on the Jacobi grid (shape (n_theta, n_r, n_R)) through the PES
+    callback convention of the reference's PES MEX functions: `pes(r12, r23,
+    r13)` gets the three internuclear distances of every point with all of them
+    > rmin (one call) and returns V; the others get vmax (H3/H3PESJacobi.m)."""
+    (a, b, t), keep = _grid_structs(R, r, x)
+    m = np.ascontiguousarray(masses, dtype=np.float64)
+    out = np.empty((t.n, b.n, a.n))
+
+    def cb(n, p12, p23, p13, pv, ctx):
+        try:
+            r12 = np.ctypeslib.as_array(p12, (n,))
+            r23 = np.ctypeslib.as_array(p23, (n,))
+            r13 = np.ctypeslib.as_array(p13, (n,))
+            np.ctypeslib.as_array(pv, (n,))[:] = pes(r12, r23, r13)
+            return 0
+        except Exception:
+            return 1
+    fn = _abi.PES_FN(cb)
+    check(lib().qd_potential_jacobi(C.byref(a), C.byref(b), C.byref(t),
+                                    m.ctypes.data_as(_abi.c_double_p), fn, None, vmax, rmin,
+                                    1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
+    return out
+
+
+def leps_params(pes):
+    """qd_leps of a systems.LEPS surface (atomic units)."""
+    p = _abi.QdLeps()
+    for name in ("ab", "bc", "ac"):
+        d = getattr(pes, name)
+        q = getattr(p, name)
+        q.de, q.beta, q.re, q.sato = d.de, d.beta, d.re, d.sato
+    return p
+
+
+def potential_leps_gpu(R, r, x, masses, pes, vmax=2.5, rmin=0.4, cap=True):
+    """The extended-LEPS surface `pes` (a systems.LEPS) on the Jacobi grid,
+    evaluated on the GPU in FP64 (qd_potential_leps)."""
+    (a, b, t), keep = _grid_structs(R, r, x)
+    m = np.ascontiguousarray(masses, dtype=np.float64)
+    out = np.empty((t.n, b.n, a.n))
+    p = leps_params(pes)
+    check(lib().qd_potential_leps(C.byref(a), C.byref(b), C.byref(t),
+                                  m.ctypes.data_as(_abi.c_double_p), C.byref(p), vmax, rmin,
+                                  1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
+    return out

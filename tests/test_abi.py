@@ -88,3 +88,40 @@ def test_struct_layout_matches_header():
     assert C.sizeof(_abi.QdAngle) == 32
     assert C.sizeof(_abi.QdTime) == 24
     assert C.sizeof(_abi.QdCrp) == 40
+
+
+def _jacobi_grid():
+    x, _ = S.gauss_legendre(12)
+    R = np.linspace(0.5, 12.0, 20)
+    r = np.linspace(0.4, 8.0, 16)
+    m = np.array([18.9984, 1.00783, 1.00783]) * S.AMU_ME
+    return R, r, x, m
+
+
+def test_pes_callback_matches_jacobi_mapping(qdlib):
+    # the host PES callback path (no GPU): same points, same values as the
+    # restatement of H3PESJacobi.m in systems.potential_on_grid
+    from qd_b200.timeevolution import potential_jacobi
+    R, r, x, m = _jacobi_grid()
+    pes = S.leps_f_h2()
+    got = potential_jacobi(R, r, x, m, pes)
+    ref = S.potential_on_grid(R, r, x, m, pes)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
+    uncapped = potential_jacobi(R, r, x, m, pes, cap=False)
+    assert uncapped.max() > 2.5 and np.array_equal(np.minimum(uncapped, 2.5), got)
+
+
+def test_pes_callback_errors(qdlib):
+    from qd_b200.timeevolution import potential_jacobi
+    from qd_b200._abi import QdError, QD_ERR_PES
+    R, r, x, m = _jacobi_grid()
+
+    def raises(r12, r23, r13):
+        raise RuntimeError("no surface here")
+    with pytest.raises(QdError) as e:
+        potential_jacobi(R, r, x, m, raises)
+    assert e.value.code == QD_ERR_PES
+    with pytest.raises(QdError) as e:
+        potential_jacobi(R, r, x, m, lambda a, b, c: np.full(a.shape, np.nan))
+    assert e.value.code == QD_ERR_PES

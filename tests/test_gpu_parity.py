@@ -308,3 +308,23 @@ def test_energies_harmonic_oscillator_kat(prec, tol):
     with Propagator(d) as p:
         e = p.energies()
     assert abs(e[0] - 0.5) < tol and abs(e[2] - 0.5) < tol and abs(e[1]) < tol
+
+
+@pytest.mark.parametrize("system", ["h+h2", "f+h2"])
+def test_leps_potential_on_gpu(system):
+    # the device LEPS evaluation against the host restatement of
+    # H3PESJacobi.m + the LEPS algebra (systems.potential_on_grid)
+    from qd_b200.timeevolution import potential_leps_gpu
+    x, _ = S.gauss_legendre(40)
+    R = np.linspace(0.5, 12.0, 64)
+    r = np.linspace(0.4, 8.0, 64)
+    amu = (1.00783, 1.00783, 1.00783) if system == "h+h2" else (18.9984, 1.00783, 1.00783)
+    m = np.array(amu) * S.AMU_ME
+    pes = S.leps_h_h2() if system == "h+h2" else S.leps_f_h2()
+    for cap in (True, False):
+        got = potential_leps_gpu(R, r, x, m, pes, cap=cap)
+        ref = S.potential_on_grid(R, r, x, m, pes) if cap else None
+        if cap:
+            assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
+        else:
+            assert np.array_equal(np.minimum(got, 2.5), potential_leps_gpu(R, r, x, m, pes))
