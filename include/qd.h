@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define QD_ABI_VERSION 1
+#define QD_ABI_VERSION 2
 
 /* status codes */
 #define QD_OK               0
@@ -120,8 +120,23 @@ typedef struct qd_crp {
   double       *CRP;                /* out: P(E), n_energies                 */
 } qd_crp;
 
+/* Centrifugal-sudden block (J, K).  No counterpart in the reference, whose
+ * propagator is the J = 0 one; zero-initialised it is exactly that.  For a
+ * block (J, K) the angular basis is the normalised associated Legendre
+ * functions of order K, j = K .. K + m: theta.legendre holds
+ * L[l][k] = Pbar_{K+l}^K(x_k) / sqrt(l + 1/2) (so the reference's transform
+ * pair, B with L and F with (l+1/2) w_k L, stays an identity on the basis;
+ * qd_cs_legendre builds it), the rotational phase uses j(j+1) with j = K + l,
+ * and pot already contains the centrifugal term (J(J+1) - 2K^2)/(2 mu_R R^2)
+ * (the caller's to add, as it adds any potential). */
+typedef struct qd_cs {
+  int32_t J;
+  int32_t K;
+} qd_cs;
+
 /* The whole Matlab struct handed to TimeEvolutionMex / TimeEvolutionMexCUDA
- * (common/TimeEvolutionMex.C:28-70). */
+ * (common/TimeEvolutionMex.C:28-70), followed by the centrifugal-sudden block
+ * indices (zero for the reference's J = 0 propagation). */
 typedef struct qd_data {
   qd_radial   r1;       /* R, atom - diatom distance                         */
   qd_radial   r2;       /* r, diatom bond length                             */
@@ -132,6 +147,7 @@ typedef struct qd_data {
   qd_options  options;
   qd_dump     dump1, dump2;
   qd_crp      CRP;
+  qd_cs       cs;
 } qd_data;
 
 /* ---- library ---------------------------------------------------------- */
@@ -201,10 +217,12 @@ int qd_restore(qd_handle *h, const char *path);
 
 /* ---- batches: many propagations in the same launches ------------------- */
 
-/* runs[0..n_runs) share r1, r2, theta, time.time_step, time.steps,
+/* runs[0..n_runs) share r1, r2, theta.n/x/w, time.time_step, time.steps,
  * options.precision, the absorbers and the CRP settings (surface, stencil,
- * number of energies); psi, pot, CRP.energies and CRP.eta_sq may differ per
- * run (one potential table is kept when all pot arrays are equal).  All runs
+ * number of energies); psi, pot, theta.m/legendre, cs, CRP.energies and
+ * CRP.eta_sq may differ per run (one potential table is kept when all pot
+ * arrays are equal; runs with fewer angular functions are padded with empty
+ * l-slices).  All runs
  * advance together; results per run.  No counterpart in the reference, whose
  * MEX propagates one wavepacket per call. */
 int qd_create_batch(const qd_data *runs, int32_t n_runs, qd_handle **out);
@@ -246,6 +264,13 @@ int qd_read_grids(const char *dir, int32_t n, double *x, double *w);
 /* theta.legendre = P_l(x_k), (m+1) x n column-major, by the three-term
  * recurrence of common/LegendreP2.m:9-21, computed in FP64 on the GPU. */
 int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre);
+
+/* theta.legendre of centrifugal-sudden block K: L[l][k] =
+ * Pbar_{K+l}^K(x_k) / sqrt(l + 1/2), l = 0..m, with Pbar_j^K the associated
+ * Legendre function normalised to one on [-1, 1] (no Condon-Shortley phase),
+ * by the standard three-term recurrence in j, FP64 on the host.  K = 0 gives
+ * P_l(x_k), the reference's matrix. */
+int qd_cs_legendre(int32_t n, int32_t K, int32_t m, const double *x, double *legendre);
 
 /* ---- potential on the Jacobi grid (H3/H3PESJacobi.m:5-27) --------------- */
 

@@ -11,6 +11,11 @@
  * FFT: FFTW 3.3.4 (the reference's dependency, not vendored) is replaced by
  * an unnormalised mixed-radix DFT with the same sign convention
  * (FFTW_FORWARD = exp(-2 pi i jk/n), FFTW_BACKWARD = exp(+...)).
+ *
+ * One extension beyond the reference: for a centrifugal-sudden block
+ * (qd_data.cs, zero for the reference's J = 0 case) the rotational phase and
+ * energy use j = K + l; the angular basis and the centrifugal potential come
+ * in through theta.legendre and pot like any other input.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -334,7 +339,8 @@ static void setup_exp_irot_dt_2(qdo_state *s)
       for (int i = 0; i < n1; i++) {
         /* exp(l(l+1)(I1+I2) * Complex(0,-dt/2)): the real part of the product
            is l(l+1)(I1+I2)*0 = 0 and exp(0) = 1 */
-        const double x = l * (l + 1) * (s->one2mr21[i] + s->one2mr22[j]);
+        const double jr = (double)(s->d->cs.K + l);   /* j = K + l (centrifugal sudden) */
+        const double x = jr * (jr + 1) * (s->one2mr21[i] + s->one2mr22[j]);
         s->exp_irot_dt_2[i + (long)n1 * (j + (long)n2 * l)] = ref_expi(x * -dt2);
       }
 }
@@ -422,7 +428,8 @@ static double rotational_energy_lpsi(qdo_state *s)
         cplx c = p[i + (long)n1 * j];
         sl += (c.re * c.re + c.im * c.im) * (s->one2mr21[i] + s->one2mr22[j]);
       }
-    sum += sl * l * (l + 1) / (l + 0.5);
+    const double jr = (double)(s->d->cs.K + l);
+    sum += sl * jr * (jr + 1) / (l + 0.5);
   }
   return sum * s->d->r1.dr * s->d->r2.dr;
 }

@@ -82,8 +82,11 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
   C *lpsi = reinterpret_cast<C *>(p.lpsi) + (long)run * p.nl * p.n12;
   const long zoff = (long)run * p.nth * p.n12;      // psi_z of this run
   const long voff = (long)run * p.vrun;             // potential tables of this run
-  const R *P = MatSel<R>::P(p);
-  const R *WP = MatSel<R>::WP(p);
+  const long soff = p.run_set ? p.run_set[run] * p.set_stride : 0;   // angular basis of the run
+  const R *P = MatSel<R>::P(p) + soff;
+  const R *WP = MatSel<R>::WP(p) + soff;
+  const R *Plo = MatSel<R>::Plo(p) ? MatSel<R>::Plo(p) + soff : nullptr;
+  const R *WPlo = MatSel<R>::WPlo(p) ? MatSel<R>::WPlo(p) + soff : nullptr;
 
   if (mode == COL_HEAD) {
     for (int e = threadIdx.x; e < p.nth * TP; e += blockDim.x) {
@@ -116,7 +119,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
     }
     __syncthreads();
     // psi_theta(k) = sum_l P[k][l] psi_l(l)
-    contract<R, C>(P, MatSel<R>::Plo(p), p.nl, false, A, p.nl, B, p.nth, TP);
+    contract<R, C>(P, Plo, p.nl, false, A, p.nl, B, p.nth, TP);
   }
   __syncthreads();
 
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
   }
 
   // psi_l(l) = sum_k WP[k][l] psi_theta(k)
-  contract<R, C>(WP, MatSel<R>::WPlo(p), p.nl, true, B, p.nth, A, p.nl, TP);
+  contract<R, C>(WP, WPlo, p.nl, true, B, p.nth, A, p.nl, TP);
   __syncthreads();
   for (int e = threadIdx.x; e < p.nl * TP; e += blockDim.x) {
     const int l = e / TP, t = e % TP;

@@ -137,7 +137,10 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 struct TcDev {
-  const float4 *mats;    // B1 hi|mid|lo, B2 hi|mid|lo images
+  const float4 *mats;    // image sets (B1 hi|lo, B2 hi|lo), set_bytes apart
+  uint32_t set_bytes;
+  const int *run_set;    // image set of each run (null: set 0)
+  const int *run_nl;     // orders stored per run (null: n_l)
   int *status;           // device status word (0 = ok)
   int renorm;            // per-column isometry rescaling on
   int nnorm;             // orders l < nnorm enter the GEMM2 output norm
@@ -249,24 +252,36 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
                  :: "r"(smem_u32(tmem_slot)), "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  // this CTA's tiles: a contiguous range, so that it meets few run boundaries
+  const int n12 = (int)p.n12, n1 = p.n1;
+  const int tpr = (n12 + TPTS - 1) / TPTS;      // tiles per run
+  const int ntiles = tpr * p.nruns;
+  const int tbeg = (int)(((long)blockIdx.x * ntiles) / gridDim.x);
+  const int tend = (int)(((long)(blockIdx.x + 1) * ntiles) / gridDim.x);
   const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
+  // the B images of set `st` (4 * B_BYTES, a multiple of 16) by bulk
+  // asynchronous copies from this GPU's global memory into this CTA's shared
+  // memory, completing on mbar[3]
+#define QD_LOAD_IMAGES(st)                                                             \
+  do {                                                                                 \
+    constexpr uint32_t total = 4 * B_BYTES, chunk = 16384;                             \
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"              \
+                 :: "r"(mb3), "r"(total) : "memory");                                  \
+    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes; \
+    for (uint32_t off = 0; off < total; off += chunk) {                                \
+      const uint32_t n = total - off < chunk ? total - off : chunk;                    \
+      asm volatile(                                                                    \
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" \
+          :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
+    }                                                                                  \
+  } while (0)
+  int loaded = tbeg < tend && t.run_set ? t.run_set[tbeg / tpr] : 0;   // image set in smem
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb3));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    // the B images (4 * B_BYTES, a multiple of 16) by bulk asynchronous copies
-    // from this GPU's global memory into this CTA's shared memory
-    constexpr uint32_t total = 4 * B_BYTES, chunk = 16384;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(mb3), "r"(total) : "memory");
-    const char *src = reinterpret_cast<const char *>(t.mats);
-    for (uint32_t off = 0; off < total; off += chunk) {
-      const uint32_t n = total - off < chunk ? total - off : chunk;
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-          :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");
-    }
+    QD_LOAD_IMAGES(loaded);
   }
   for (int i = tid; i < S; i += NTHREADS) {
     const double w = i < p.nth ? p.w[i] : 0.0;
@@ -282,14 +297,11 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   const uint32_t my_hi = Ahi + lane_base + c0, my_lo = Alo + lane_base + c0;
   const uint32_t my_d = D + lane_base + c0;
   const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
-  uint32_t ph1 = 0, ph2 = 0;
+  uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
   bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
 
   // 32-bit tile arithmetic: the host checks n12 * n_l * 2 * n_runs < 2^31
-  const int n12 = (int)p.n12, n1 = p.n1;
   const int nl = p.nl, nth = p.nth;
-  const int tpr = (n12 + TPTS - 1) / TPTS;      // tiles per run
-  const int ntiles = tpr * p.nruns;
   const int stride = 2 * n12;                   // floats between orders l (or k) of a point
   const float *lsrc = reinterpret_cast<const float *>(p.lpsi);
   float *ldst = reinterpret_cast<float *>(p.lpsi);
@@ -302,10 +314,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #define QD_PREFETCH_A(tl)                                                            \
   do {                                                                               \
     const int rr = (tl) / tpr, qq = ((tl) - rr * tpr) * TPTS + pt;                   \
-    const bool ok = EX || ((tl) < ntiles && qq < n12);                               \
+    const bool ok = EX || ((tl) < tend && qq < n12);                                 \
     const float *src = lsrc + (size_t)rr * nl * stride + (size_t)c0 * stride + 2 * qq + comp; \
     _Pragma("unroll") for (int u = 0; u < H; u++) {                                  \
-      if (EX) a[u] = (tl) < ntiles ? __ldg(src + u * stride) : 0.f;                   \
+      if (EX) a[u] = (tl) < tend ? __ldg(src + u * stride) : 0.f;                     \
       else a[u] = (ok && c0 + u < nl) ? __ldg(src + u * stride) : 0.f;               \
     }                                                                                \
   } while (0)
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   // past n_theta and past the grid; n12 is even, so a copy never straddles it)
 #define QD_STAGE_EV(tl)                                                              \
   do {                                                                               \
-    if ((tl) < ntiles) {                                                             \
+    if ((tl) < tend) {                                                               \
       const int rr = (tl) / tpr, qb = ((tl) - rr * tpr) * TPTS;                      \
       const float2 *eb = expv + (size_t)rr * p.vrun + qb;                            \
       for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
@@ -324,11 +336,19 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     }                                                                                \
     asm volatile("cp.async.commit_group;" ::: "memory");                             \
   } while (0)
-  if (mode != COL_HEAD) QD_PREFETCH_A((int)blockIdx.x);
-  if (mode == COL_MID) QD_STAGE_EV((int)blockIdx.x);
+  if (mode != COL_HEAD) QD_PREFETCH_A(tbeg);
+  if (mode == COL_MID) QD_STAGE_EV(tbeg);
 
-  for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+  for (int tile = tbeg; tile < tend && !failed; tile++) {
     const int run = tile / tpr;
+    const int set = t.run_set ? t.run_set[run] : 0;
+    if (set != loaded) {                        // a run with another angular basis
+      if (tid == 0) QD_LOAD_IMAGES(set);        // earlier MMAs have all completed
+      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+      ph3 ^= 1;
+      loaded = set;
+    }
+    const int nlr = t.run_nl ? t.run_nl[run] : nl;   // orders stored for this run
     const int q0 = (tile - run * tpr) * TPTS;
     const int q = q0 + pt;
     const bool qok = EX || q < n12;
@@ -463,10 +483,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
     }
     if (mode == COL_TAIL) {
-      QD_PREFETCH_A(tile + (int)gridDim.x);
+      QD_PREFETCH_A(tile + 1);
       continue;
     }
-    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
+    if (mode == COL_MID) QD_STAGE_EV(tile + 1);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
@@ -474,7 +494,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
       mma_commit(mb2);
     }
-    if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
+    if (mode != COL_HEAD) QD_PREFETCH_A(tile + 1);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
@@ -506,12 +526,13 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
 #pragma unroll
       for (int x = 0; x < 4; x++)
-        if (EX || (qok && c0 + u + x < nl)) dst[(u + x) * stride] = v[x] * so;
+        if ((EX || qok) && c0 + u + x < nlr) dst[(u + x) * stride] = v[x] * so;
     }
     tc_fence_before();
   }
 #undef QD_PREFETCH_A
 #undef QD_STAGE_EV
+#undef QD_LOAD_IMAGES
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
@@ -571,57 +592,58 @@ template <int S> constexpr int smem_bytes_for()
          S * TPTS * 8;   // B images, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
 
-// P_l(x_k) for l = 0..lmax by the recurrence of LegendreP2.m:9-21 (FP64)
-std::vector<double> legendre_rows(int nth, int lmax, const double *x)
-{
-  std::vector<double> P((size_t)nth * (lmax + 1));
-  for (int k = 0; k < nth; k++) {
-    double p0 = 1.0, p1 = x[k];
-    P[(size_t)k * (lmax + 1)] = 1.0;
-    if (lmax >= 1) P[(size_t)k * (lmax + 1) + 1] = x[k];
-    for (int l = 2; l <= lmax; l++) {
-      const double p2 = (2.0 - 1.0 / l) * x[k] * p1 - (1.0 - 1.0 / l) * p0;
-      P[(size_t)k * (lmax + 1) + l] = p2;
-      p0 = p1;
-      p1 = p2;
-    }
-  }
-  return P;
-}
-
 }  // namespace
 
-int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const double *w,
-                   const double *x, cudaStream_t s)
+int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const *leg,
+                   const int *nl_set, const double *w, cudaStream_t s)
 {
   const int S = pad16(nl > nth ? nl : nth);
   if (S > MAXS) return QD_ERR_UNSUPPORTED;
-  // Extra orders l = n_l .. n_theta-1 for the GEMM2 norm, and a check that the
-  // quadrature makes the transform pair an isometry (else no rescaling).
-  bool renorm = nl <= nth;
-  std::vector<double> Pext;
-  if (renorm) {
-    Pext = legendre_rows(nth, nth - 1, x);
-    for (int k = 0; k < nth && renorm; k++)
-      for (int l = 0; l < nl; l++)
-        if (std::fabs(Pext[(size_t)k * nth + l] - legendre[l + (long)k * nl]) >
-            1e-10 * (1.0 + std::fabs(legendre[l + (long)k * nl]))) {
-          renorm = false;
-          break;
-        }
-    for (int l = 0; l < nth && renorm; l++)
-      for (int l2 = 0; l2 < nth; l2++) {
+  // Q[k][l] = sqrt(w_k) sqrt(l+1/2) L[l][k] per angular set; the transform pair
+  // is an isometry per grid column when Q has orthonormal columns, and GEMM2
+  // then also forms an orthonormal completion of them (modified Gram-Schmidt
+  // against the unit vectors, twice) so that its output norm is exact.
+  std::vector<std::vector<double>> Q(nsets), Qx(nsets);
+  bool renorm = true;
+  for (int t = 0; t < nsets; t++) {
+    const int m = nl_set[t];
+    Q[t].assign((size_t)nth * m, 0.0);
+    for (int k = 0; k < nth; k++)
+      for (int l = 0; l < m; l++)
+        Q[t][(size_t)l * nth + k] = std::sqrt(w[k]) * std::sqrt(l + 0.5) * leg[t][l + (long)k * m];
+    if (m > nth) { renorm = false; continue; }
+    for (int l = 0; l < m && renorm; l++)
+      for (int l2 = 0; l2 < m; l2++) {
         double g = 0.0;
-        for (int k = 0; k < nth; k++)
-          g += w[k] * Pext[(size_t)k * nth + l] * Pext[(size_t)k * nth + l2];
-        g *= (l2 + 0.5);
+        for (int k = 0; k < nth; k++) g += Q[t][(size_t)l * nth + k] * Q[t][(size_t)l2 * nth + k];
         if (std::fabs(g - (l == l2 ? 1.0 : 0.0)) > 1e-9) { renorm = false; break; }
       }
+    if (!renorm) continue;
+    std::vector<double> basis = Q[t];                // columns, each nth long
+    int have = m;
+    for (int c = 0; c < nth && have < nth; c++) {
+      std::vector<double> v(nth, 0.0);
+      v[c] = 1.0;
+      for (int pass = 0; pass < 2; pass++)
+        for (int b = 0; b < have; b++) {
+          double d = 0.0;
+          for (int k = 0; k < nth; k++) d += basis[(size_t)b * nth + k] * v[k];
+          for (int k = 0; k < nth; k++) v[k] -= d * basis[(size_t)b * nth + k];
+        }
+      double nv = 0.0;
+      for (int k = 0; k < nth; k++) nv += v[k] * v[k];
+      if (nv < 1e-2) continue;
+      nv = 1.0 / std::sqrt(nv);
+      for (int k = 0; k < nth; k++) basis.push_back(v[k] * nv);
+      have++;
+    }
+    if (have < nth) renorm = false;
+    Qx[t] = basis;                                     // nth columns: Q, then the completion
   }
   const int nka = (S + 31) / 32;
   const int bb = nka * S * 128;
-  std::vector<unsigned char> img(4 * (size_t)bb, 0);
-  unsigned char *b1 = img.data(), *b2 = b1 + 2 * bb;
+  const size_t set_bytes = 4 * (size_t)bb;
+  std::vector<unsigned char> img(set_bytes * nsets, 0);
   auto put = [&](unsigned char *img2, int r, int k, double val) {     // hi | lo
     const float h = tf32_round_host((float)val);
     const float l = tf32_round_host((float)(val - (double)h));
@@ -629,15 +651,14 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const 
     std::memcpy(img2 + off, &h, 4);
     std::memcpy(img2 + bb + off, &l, 4);
   };
-  const int lrows = renorm ? nth : nl;          // orders formed by GEMM2
-  // both images hold Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k) (orthonormal basis)
-  for (int k = 0; k < nth; k++) {
-    const double swk = std::sqrt(w[k]);
-    for (int l = 0; l < nl; l++)                                              // B1: row k, K = l
-      put(b1, k, l, swk * std::sqrt(l + 0.5) * legendre[l + (long)k * nl]);
-    for (int l = 0; l < lrows; l++) {                                         // B2: row l, K = k
-      const double P = l < nl ? legendre[l + (long)k * nl] : Pext[(size_t)k * nth + l];
-      put(b2, l, k, swk * std::sqrt(l + 0.5) * P);
+  for (int t = 0; t < nsets; t++) {
+    unsigned char *b1 = img.data() + t * set_bytes, *b2 = b1 + 2 * bb;
+    const int m = nl_set[t];
+    const int rows2 = renorm ? nth : m;                  // output orders formed by GEMM2
+    const std::vector<double> &q2 = renorm ? Qx[t] : Q[t];
+    for (int k = 0; k < nth; k++) {
+      for (int l = 0; l < m; l++) put(b1, k, l, Q[t][(size_t)l * nth + k]);   // B1: row k, K = l
+      for (int l = 0; l < rows2; l++) put(b2, l, k, q2[(size_t)l * nth + k]); // B2: row l, K = k
     }
   }
   void *d = nullptr;
@@ -652,6 +673,8 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, const double *legendre, const 
     return QD_ERR_CUDA;
   }
   plan.nth = nth; plan.nl = nl; plan.S = S; plan.renorm = renorm ? 1 : 0;
+  plan.nsets = nsets;
+  plan.set_bytes = set_bytes;
   plan.mats = d;
   plan.mats_bytes = img.size();
   int dev = 0, sms = 148;
@@ -694,6 +717,9 @@ cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode
 {
   TcDev t;
   t.mats = reinterpret_cast<const float4 *>(plan.mats);
+  t.set_bytes = (uint32_t)plan.set_bytes;
+  t.run_set = p.run_set;
+  t.run_nl = p.run_nl;
   t.status = tc_status_ptr(plan);
   t.renorm = plan.renorm;
   t.nnorm = plan.nth < plan.S ? plan.nth : plan.S;

@@ -20,7 +20,7 @@ __global__ void __launch_bounds__(256) k_e_pot_rot(EnergyParams e)
       spot += e.w[k] * (z.x * z.x + z.y * z.y) * e.pot[(long)k * e.n12 + q];
     }
     const double I = e.I1[i] + e.I2[j];
-    for (int l = 1; l < e.nl; l++) {
+    for (int l = e.K == 0 ? 1 : 0; l < e.nl; l++) {   // j(j+1) = 0 only for j = 0
       double2 c = make_double2(0.0, 0.0);
       for (int k = 0; k < e.nth; k++) {
         const double2 z = e.psi_z[(long)k * e.n12 + q];
@@ -28,7 +28,8 @@ __global__ void __launch_bounds__(256) k_e_pot_rot(EnergyParams e)
         c.x += z.x * wp;
         c.y += z.y * wp;
       }
-      srot += (c.x * c.x + c.y * c.y) * I * l * (l + 1) / (l + 0.5);
+      const double jr = (double)(e.K + l);           // j = K + l (centrifugal sudden)
+      srot += (c.x * c.x + c.y * c.y) * I * jr * (jr + 1) / (l + 0.5);
     }
   }
   srot = block_sum(srot, red);

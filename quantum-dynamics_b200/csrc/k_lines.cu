@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(256) k_rows(LineParams p, int dir)
   const int rb = p.rows_per_cta;
   C *bufA = reinterpret_cast<C *>(smem);
   C *bufB = bufA + rb * p.n1;
-  const int sl = blockIdx.y, l = sl % p.nl;     // slice = run * nl + l
+  const int sl = blockIdx.y, l = rot_row(p, sl);  // slice = run * nl + l
   const int j0 = blockIdx.x * rb;
   const int nrows = min(rb, p.n2 - j0);
   C *slice = reinterpret_cast<C *>(p.lpsi) + (long)sl * p.n12 + (long)j0 * p.n1;

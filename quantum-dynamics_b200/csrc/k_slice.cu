@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(NT, 1) k_slice(LineParams p)
     if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int sl = blockIdx.x / CL, l = sl % p.nl;   // slice = run * nl + l
+  const int sl = blockIdx.x / CL, l = rot_row(p, sl);   // slice = run * nl + l
   const int nrow = n2 / CL, ncol = n1 / CL;
   const int rs = n1 + n1 / 8;
   const int bufsz = slice_buf_elems(n1, n2, CL);
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(NT, 2) k_slice_ct(LineParams p)
     if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int sl = blockIdx.x / CL, l = sl % p.nl;   // slice = run * nl + l
+  const int sl = blockIdx.x / CL, l = rot_row(p, sl);   // slice = run * nl + l
   float2 *tw1 = sm, *tw2 = sm + N1;
   float2 *X = tw2 + N2, *Y = X + BUF;
   const float2 *gtw1 = reinterpret_cast<const float2 *>(p.tw1);

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int sl = blockIdx.x, l = sl % p.nl;          // slice = run * nl + l
+  const int sl = blockIdx.x, l = rot_row(p, sl);     // slice = run * nl + l; l = table row
   float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
   const float2 *tw1 = reinterpret_cast<const float2 *>(p.tw1);
   const float2 *tw2 = reinterpret_cast<const float2 *>(p.tw2);

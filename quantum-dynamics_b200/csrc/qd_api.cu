@@ -10,6 +10,7 @@
 // with the E-accumulation GEMM every QD_RING steps and P(E) at the end of a
 // call.  The l-space wavepacket stays on the device between calls.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -118,8 +119,13 @@ struct qd_handle {
   int nruns = 1;
   long vrun = 0;                  // per-run stride of the potential tables (0 = shared)
   int prec = QD_PREC_FP64;
-  int n1 = 0, n2 = 0, nth = 0, nl = 0;
+  int n1 = 0, n2 = 0, nth = 0, nl = 0;      // nl: angular functions of the layout (max over runs)
   long n12 = 0;
+  // angular bases: runs with equal theta.legendre share a set; a
+  // centrifugal-sudden run has j = K + l
+  int nsets = 1, jrows = 0;
+  std::vector<int> run_set, run_k, run_nl;
+  int *d_run_set = nullptr, *d_run_k = nullptr, *d_run_nl = nullptr;
   int npts = 0, h = 0, surf_j0 = 0, ne = 0;
   bool do_crp = false, have_dump = false;
   double dt = 0;
@@ -218,6 +224,9 @@ int validate(const qd_data *d)
                    n1, n2);
   if (d->options.precision != QD_PREC_FP64 && d->options.precision != QD_PREC_FP32)
     return set_err(QD_ERR_INVALID, "options.precision = %d", d->options.precision);
+  if (d->cs.K < 0 || d->cs.J < d->cs.K)
+    return set_err(QD_ERR_INVALID, "centrifugal-sudden block J = %d, K = %d: need 0 <= K <= J",
+                   d->cs.J, d->cs.K);
   const size_t npt = (size_t)n1 * n2 * nth;
   if (!all_finite(d->pot, npt)) return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
   if (!all_finite(d->psi, 2 * npt)) return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
@@ -319,6 +328,7 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   p.do_flux = flux ? 1 : 0;
   p.surf = h->d_surf; p.surf_j0 = h->surf_j0; p.surf_nrows = 2 * h->h + 1;
   p.w = h->d_w; p.norm_out = norm_out; p.out_z = out_z ? 1 : 0;
+  p.run_set = h->d_run_set; p.set_stride = (long)h->nth * h->nl; p.run_nl = h->d_run_nl;
   cudaError_t e;
   TRY(prof_mark(h, -1));
   if (sizeof(R) == 4 && h->use_tc) e = launch_column_tc(h->tc, p, mode, h->st);
@@ -381,6 +391,7 @@ LineParams line_params(qd_handle *h, bool f32)
   if (!f32) { p.tw1 = h->d_tw1_64; p.tw2 = h->d_tw2_64; }
   else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
   p.pl1 = h->pl1; p.pl2 = h->pl2;
+  p.run_k = h->d_run_k; p.jrows = h->jrows;
   return p;
 }
 
@@ -595,9 +606,8 @@ int validate_batch(const qd_data *runs, int n)
     const bool ok =
         b.r1.n == a.r1.n && b.r2.n == a.r2.n && b.r1.dr == a.r1.dr && b.r2.dr == a.r2.dr &&
         b.r1.mass == a.r1.mass && b.r2.mass == a.r2.mass && same(b.r1.r, a.r1.r, a.r1.n) &&
-        same(b.r2.r, a.r2.r, a.r2.n) && b.theta.n == a.theta.n && b.theta.m == a.theta.m &&
+        same(b.r2.r, a.r2.r, a.r2.n) && b.theta.n == a.theta.n &&
         same(b.theta.x, a.theta.x, a.theta.n) && same(b.theta.w, a.theta.w, a.theta.n) &&
-        same(b.theta.legendre, a.theta.legendre, (size_t)a.theta.n * (a.theta.m + 1)) &&
         b.time.time_step == a.time.time_step && b.time.steps == a.time.steps &&
         b.options.precision == a.options.precision &&
         same(b.dump1.dump, a.dump1.dump, a.r1.n) && same(b.dump2.dump, a.dump2.dump, a.r2.n) &&
@@ -608,7 +618,8 @@ int validate_batch(const qd_data *runs, int n)
           b.CRP.n_energies == a.CRP.n_energies));
     if (!ok)
       return set_err(QD_ERR_INVALID, "run %d differs from run 0 in a field the batch shares "
-                     "(grids, theta, time, options.precision, dumps, CRP settings)", r);
+                     "(grids, theta nodes and weights, time, options.precision, dumps, CRP "
+                     "settings)", r);
   }
   return QD_OK;
 }
@@ -628,8 +639,35 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   h->nruns = nruns;
   for (int r = 0; r < nruns; r++) h->runs.push_back(const_cast<qd_data *>(&runs[r]));
   h->prec = d->options.precision;
-  h->n1 = d->r1.n; h->n2 = d->r2.n; h->nth = d->theta.n; h->nl = d->theta.m + 1;
+  h->n1 = d->r1.n; h->n2 = d->r2.n; h->nth = d->theta.n;
   h->n12 = (long)h->n1 * h->n2;
+  // angular sets: runs with the same theta.m and theta.legendre share one
+  std::vector<const qd_data *> set_of;
+  h->nl = 0;
+  h->jrows = 0;
+  bool any_k = false;
+  for (int r = 0; r < nruns; r++) {
+    const qd_data &a = runs[r];
+    const int nlr = a.theta.m + 1;
+    int sidx = -1;
+    for (size_t t = 0; t < set_of.size() && sidx < 0; t++)
+      if (set_of[t]->theta.m == a.theta.m &&
+          same(set_of[t]->theta.legendre, a.theta.legendre, (size_t)h->nth * nlr))
+        sidx = (int)t;
+    if (sidx < 0) {
+      sidx = (int)set_of.size();
+      set_of.push_back(&a);
+    }
+    h->run_set.push_back(sidx);
+    h->run_k.push_back(a.cs.K);
+    h->run_nl.push_back(nlr);
+    h->nl = std::max(h->nl, nlr);
+    h->jrows = std::max(h->jrows, a.cs.K + nlr);
+    any_k = any_k || a.cs.K != 0;
+  }
+  h->nsets = (int)set_of.size();
+  if ((long)h->n12 * h->nl * 2 * nruns >= (1L << 31) || (long)h->n12 * h->nth * nruns >= (1L << 31))
+    return set_err(QD_ERR_UNSUPPORTED, "batch too large for 32-bit tile offsets");
   h->dt = d->time.time_step;
   h->steps = d->time.steps;
   h->have_dump = d->dump1.dump && d->dump2.dump;
@@ -656,13 +694,29 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     CU(cudaMemcpyAsync(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt,
                        cudaMemcpyHostToDevice, h->st));
   TRY(upload(h, h->d_w, d->theta.w, h->nth));
-  TRY(upload(h, h->d_leg, d->theta.legendre, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_P, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_WP, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_P32, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_WP32, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_P32lo, (size_t)h->nth * h->nl));
-  TRY(h->alloc(h->d_WP32lo, (size_t)h->nth * h->nl));
+  // each set's legendre matrix padded to nl functions (zero rows beyond its own)
+  const size_t sstride = (size_t)h->nth * h->nl;
+  std::vector<double> legpad(sstride * h->nsets, 0.0);
+  std::vector<std::vector<double>> set_leg(h->nsets);
+  std::vector<int> set_nl(h->nsets);
+  for (int t = 0; t < h->nsets; t++) {
+    const int m1 = set_of[t]->theta.m + 1;
+    set_nl[t] = m1;
+    set_leg[t].assign(set_of[t]->theta.legendre, set_of[t]->theta.legendre + (size_t)h->nth * m1);
+    for (int k = 0; k < h->nth; k++)
+      for (int l = 0; l < m1; l++)
+        legpad[t * sstride + (size_t)k * h->nl + l] = set_leg[t][l + (size_t)k * m1];
+  }
+  TRY(upload(h, h->d_leg, legpad.data(), legpad.size()));
+  TRY(h->alloc(h->d_P, sstride * h->nsets));
+  TRY(h->alloc(h->d_WP, sstride * h->nsets));
+  TRY(h->alloc(h->d_P32, sstride * h->nsets));
+  TRY(h->alloc(h->d_WP32, sstride * h->nsets));
+  TRY(h->alloc(h->d_P32lo, sstride * h->nsets));
+  TRY(h->alloc(h->d_WP32lo, sstride * h->nsets));
+  if (h->nsets > 1) TRY(upload(h, h->d_run_set, h->run_set.data(), nruns));
+  if (any_k) TRY(upload(h, h->d_run_k, h->run_k.data(), nruns));
+  TRY(upload(h, h->d_run_nl, h->run_nl.data(), nruns));
   std::vector<double> T1, I1, T2, I2;
   radial_tables(d->r1, T1, I1);
   radial_tables(d->r2, T2, I2);
@@ -687,23 +741,27 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     TRY(upload(h, dim == 0 ? h->d_tw1_64 : h->d_tw2_64, z.data(), n));
     TRY(upload(h, dim == 0 ? h->d_tw1_32 : h->d_tw2_32, f.data(), n));
   }
-  CU(launch_legendre_matrices(h->nth, h->nl, nullptr, h->d_w, h->d_leg, h->d_P, h->d_WP,
-                              h->d_P32, h->d_WP32, h->d_P32lo, h->d_WP32lo, h->st));
-  g_launches++;
+  for (int t = 0; t < h->nsets; t++) {
+    const size_t o = t * sstride;
+    CU(launch_legendre_matrices(h->nth, h->nl, nullptr, h->d_w, h->d_leg + o, h->d_P + o,
+                                h->d_WP + o, h->d_P32 + o, h->d_WP32 + o, h->d_P32lo + o,
+                                h->d_WP32lo + o, h->st));
+    g_launches++;
+  }
   if (f64) {
     TRY(h->alloc(h->d_expV, npt * npot));
-    TRY(h->alloc(h->d_rot, (size_t)h->n12 * h->nl));
+    TRY(h->alloc(h->d_rot, (size_t)h->n12 * h->jrows));
     TRY(h->alloc(h->d_kin, h->n12));
-    CU(launch_setup_tables_fp64(h->n1, h->n2, h->nth * npot, h->nl, h->dt, h->d_pot, h->d_I1,
+    CU(launch_setup_tables_fp64(h->n1, h->n2, h->nth * npot, h->jrows, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV, h->d_rot, h->d_kin,
                                 h->st));
   } else {
     TRY(h->alloc(h->d_expV32, npt * npot));
-    TRY(h->alloc(h->d_rc1, (size_t)h->nl * h->n1));
-    TRY(h->alloc(h->d_rc2, (size_t)h->nl * h->n2));
+    TRY(h->alloc(h->d_rc1, (size_t)h->jrows * h->n1));
+    TRY(h->alloc(h->d_rc2, (size_t)h->jrows * h->n2));
     TRY(h->alloc(h->d_kc1, h->n1));
     TRY(h->alloc(h->d_kc2, h->n2));
-    CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth * npot, h->nl, h->dt, h->d_pot, h->d_I1,
+    CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth * npot, h->jrows, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV32, h->d_rc1, h->d_rc2,
                                 h->d_kc1, h->d_kc2, h->st));
   }
@@ -744,8 +802,10 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   }
   const char *path = getenv("QD_COLUMN_PATH");   // "simt" forces the SIMT column pass
   if (!f64 && !(path && std::string(path) == "simt")) {
-    int rc = tc_plan_create(h->tc, h->nth, h->nl, d->theta.legendre, d->theta.w, d->theta.x,
-                            h->st);
+    std::vector<const double *> lp(h->nsets);
+    for (int t = 0; t < h->nsets; t++) lp[t] = set_leg[t].data();
+    int rc = tc_plan_create(h->tc, h->nth, h->nl, h->nsets, lp.data(), set_nl.data(),
+                            d->theta.w, h->st);
     if (rc == QD_OK) h->use_tc = true;
     else if (rc != QD_ERR_UNSUPPORTED) return rc;
   }
@@ -800,7 +860,8 @@ int energies(qd_handle *h, int run, double out4[4])
   e.n1 = h->n1; e.n2 = h->n2; e.nth = h->nth; e.nl = h->nl; e.n12 = h->n12;
   e.psi_z = h->d_psi_z + (long)run * h->n12 * h->nth;
   e.pot = h->d_pot + (long)run * h->vrun;
-  e.w = h->d_w; e.P = h->d_P; e.WP = h->d_WP;
+  const long soff = (long)h->run_set[run] * h->nth * h->nl;
+  e.w = h->d_w; e.P = h->d_P + soff; e.WP = h->d_WP + soff; e.K = h->run_k[run];
   e.T1 = h->d_T1; e.T2 = h->d_T2; e.I1 = h->d_I1; e.I2 = h->d_I2;
   e.tw1 = h->d_tw1_64; e.tw2 = h->d_tw2_64; e.pl1 = h->pl1; e.pl2 = h->pl2;
   double *dsum = nullptr;
@@ -1191,7 +1252,8 @@ int energies_noalloc(qd_handle *h, int run, double out4[4])
   e.n1 = h->n1; e.n2 = h->n2; e.nth = h->nth; e.nl = h->nl; e.n12 = h->n12;
   e.psi_z = h->d_psi_z + (long)run * h->n12 * h->nth;
   e.pot = h->d_pot + (long)run * h->vrun;
-  e.w = h->d_w; e.P = h->d_P; e.WP = h->d_WP;
+  const long soff = (long)h->run_set[run] * h->nth * h->nl;
+  e.w = h->d_w; e.P = h->d_P + soff; e.WP = h->d_WP + soff; e.K = h->run_k[run];
   e.T1 = h->d_T1; e.T2 = h->d_T2; e.I1 = h->d_I1; e.I2 = h->d_I2;
   e.tw1 = h->d_tw1_64; e.tw2 = h->d_tw2_64; e.pl1 = h->pl1; e.pl2 = h->pl2;
   e.sums = reinterpret_cast<double *>(base);

@@ -47,6 +47,11 @@ struct ColumnParams {
   const double *w;         // quadrature weights
   double *norm_out;        // [nruns]: accumulate sum_k w_k |psi|^2 (null = skip)
   int out_z;               // TAIL: also write psi_z
+  // per-run angular basis: the P/WP matrices of run r start at
+  // run_set[r] * set_stride (null: one set); run r stores l < run_nl[r]
+  const int *run_set;
+  long set_stride;
+  const int *run_nl;
 };
 
 struct FluxParams {
@@ -115,7 +120,21 @@ struct LineParams {
   FluxParams flux;         // fused slice kernel: flux preparation of the step ...
   int flux_ctas;           // ... by this many extra CTAs (0 = none)
   int fft_only;            // split kernels: plain forward 2-D DFT, no phases
+  // centrifugal-sudden blocks: slice l of run r has j = run_k[r] + l (null: j = l);
+  // the rotational tables have jrows rows
+  const int *run_k;
+  int jrows;
 };
+
+// rotational-table row of slice sl = run * nl + l, clamped to the table (the
+// padded l-slices of runs with fewer angular functions hold zeros)
+__device__ __forceinline__ int rot_row(const LineParams &p, int sl)
+{
+  const int l = sl % p.nl;
+  if (!p.run_k) return l;
+  const int j = p.run_k[sl / p.nl] + l;
+  return j < p.jrows ? j : p.jrows - 1;
+}
 
 // energies of one run's theta-space psi (FP64): sums[0] kinetic (before the
 // dr1 dr2 / (n1 n2) factor), sums[1] rotational, sums[2] potential
@@ -130,6 +149,7 @@ struct EnergyParams {
   FftPlan pl1, pl2;
   double2 *scratch;        // nth * n12
   double *sums;            // 3
+  int K;                   // centrifugal-sudden block: j = K + l in E_rot
 };
 cudaError_t launch_energies(const EnergyParams &e, cudaStream_t s);
 int energies_launches();

@@ -57,11 +57,15 @@ class QdCrp(C.Structure):
                 ("energies", c_double_p), ("eta_sq", c_double_p), ("CRP", c_double_p)]
 
 
+class QdCs(C.Structure):
+    _fields_ = [("J", C.c_int32), ("K", C.c_int32)]
+
+
 class QdData(C.Structure):
     _fields_ = [("r1", QdRadial), ("r2", QdRadial), ("theta", QdAngle),
                 ("pot", c_double_p), ("psi", c_double_p), ("time", QdTime),
                 ("options", QdOptions), ("dump1", QdDump), ("dump2", QdDump),
-                ("CRP", QdCrp)]
+                ("CRP", QdCrp), ("cs", QdCs)]
 
 
 PES_FN = C.CFUNCTYPE(C.c_int, C.c_int64, c_double_p, c_double_p, c_double_p, c_double_p,
@@ -136,6 +140,9 @@ def to_c(data):
     d.CRP.energies = _ptr(crp.energies); d.CRP.eta_sq = _ptr(crp.eta_sq)
     d.CRP.CRP = _ptr(crp.CRP)
     keep += [crp.energies, crp.eta_sq, crp.CRP]
+    cs = getattr(data, "cs", None)
+    d.cs.J = int(getattr(cs, "J", 0)) if cs is not None else 0
+    d.cs.K = int(getattr(cs, "K", 0)) if cs is not None else 0
     d._keep = keep
     return d
 
@@ -195,6 +202,7 @@ def lib():
         "qd_energies_noalloc": (C.c_int, [H, C.c_int32, c_double_p]),
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
+        "qd_cs_legendre": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, c_double_p, c_double_p]),
         "qd_potential_jacobi": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
                                           PES_FN, C.c_void_p, C.c_double, C.c_double,
                                           C.c_int32, c_double_p]),

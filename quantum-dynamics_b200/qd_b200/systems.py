@@ -365,6 +365,81 @@ def case_c2_j0(n_runs=64, **kw):
     return batch_cases(base, states)
 
 
+def cs_legendre(x, K, m):
+    """theta.legendre of centrifugal-sudden block K: column l (l = 0..m) is
+    Pbar_{K+l}^K(x_k) / sqrt(l + 1/2), Pbar_j^K the associated Legendre
+    function normalised to one on [-1, 1] (no Condon-Shortley phase), so that
+    the reference's transform pair (B with L, F with (l+1/2) w_k L) is the
+    identity on the basis.  K = 0 is legendre_p2 itself.  Shape (n, m+1)."""
+    if K == 0:
+        return legendre_p2(m, x)
+    x = np.asarray(x, dtype=np.float64)
+    s = np.sqrt(1.0 - x * x)
+    p0 = np.full(x.size, math.sqrt(0.5))
+    for mm in range(1, K + 1):                        # Pbar_K^K
+        p0 = p0 * math.sqrt((2 * mm + 1) / (2 * mm)) * s
+    v = np.zeros((x.size, m + 1))
+    v[:, 0] = p0
+    if m >= 1:
+        p1 = math.sqrt(2 * K + 3) * x * p0            # Pbar_{K+1}^K
+        v[:, 1] = p1
+    for l in range(2, m + 1):
+        j = K + l
+        a = math.sqrt((4 * j * j - 1) / (j * j - K * K))
+        b = math.sqrt(((j - 1) ** 2 - K * K) / (4 * (j - 1) ** 2 - 1))
+        v[:, l] = a * (x * v[:, l - 1] - b * v[:, l - 2])
+    v /= np.sqrt(np.arange(m + 1) + 0.5)[None, :]
+    return np.ascontiguousarray(v)
+
+
+def cs_case(base, J, K, v0, j0, j_max=None):
+    """The run of centrifugal-sudden block (J, K) with initial diatom state
+    (v0, j0), built from a J = 0 case `base`: angular basis Pbar_j^K for
+    j = K .. j_max (n_j = j_max - K + 1), the centrifugal term
+    (J(J+1) - 2K^2)/(2 mu_R R^2) added to the potential, and the initial packet
+    g(R) phi_{v0 j0}(r) Pbar_{j0}^K(theta) (zero when K > j0: no such state)."""
+    pes = leps_f_h2() if base.system == "f+h2" else leps_h_h2()
+    if j_max is None:
+        j_max = int(base.theta.m)
+    d = copy_case(base)
+    m = j_max - K
+    th = Struct(**vars(base.theta))
+    th.m = m
+    th.legendre = cs_legendre(th.x, K, m)
+    d.theta = th
+    d.cs = Struct(J=J, K=K)
+    R = base.r1.r
+    cent = (J * (J + 1) - 2 * K * K) / (2 * base.r1.mass * R * R)
+    d.pot = np.ascontiguousarray(base.pot + cent[None, None, :])
+    g = (1.0 / (math.pi * base.r1.delta ** 2)) ** 0.25 * np.exp(
+        -(R - base.r1.r0) ** 2 / (2 * base.r1.delta ** 2) - 1j * base.r1.k0 * R)
+    e_vj, phi = diatom_vibrot(base.r2, pes.diatom, j0, v0)
+    if K <= j0:
+        ang = cs_legendre(th.x, K, j0 - K)[:, j0 - K] * math.sqrt(j0 - K + 0.5)
+    else:
+        ang = np.zeros(th.x.size)
+    d.psi = np.ascontiguousarray((ang[:, None, None] * phi[None, :, None] *
+                                  g[None, None, :]).astype(np.complex128))
+    e_coll = base.CRP.energies - base.CRP.eDiatomic
+    d.CRP.eDiatomic = e_vj
+    d.CRP.energies = np.ascontiguousarray(e_coll + e_vj)
+    d.CRP.eta_sq = eta_sq(base.r1, e_coll)
+    d.CRP.CRP = np.zeros(int(base.CRP.n_energies))
+    return d
+
+
+def case_c2(n_runs=64, **kw):
+    """The batched F + H2 configuration on the 128 x 96 x 64 grid: centrifugal-
+    sudden blocks J in (0, 5, 10, 15, 20), K = 0 .. min(J, 4) (n_j = 64 - K),
+    crossed with the initial states (v0, j0) = (0,0), (0,1), (0,2), (1,0), in
+    that order, the first n_runs of them."""
+    kw.setdefault("total_steps", 10000)
+    base = build_case("f+h2", 128, 96, 64, m=63, r=(0.4, 8.0), **kw)
+    combos = [(J, K, v0, j0) for J in (0, 5, 10, 15, 20) for K in range(min(J, 4) + 1)
+              for (v0, j0) in ((0, 0), (0, 1), (0, 2), (1, 0))]
+    return [cs_case(base, *c) for c in combos[:n_runs]]
+
+
 def copy_case(data):
     """Deep copy of the arrays that a propagation mutates (psi, CRP, time)."""
     import copy

@@ -24,7 +24,7 @@ def test_exports_every_declared_symbol(qdlib):
     assert len(names) >= 19
     for n in names:
         assert hasattr(qdlib, n), n
-    assert qdlib.qd_abi_version() == 1
+    assert qdlib.qd_abi_version() == 2
 
 
 def test_read_grids_matches_python_reader(qdlib):
@@ -125,3 +125,19 @@ def test_pes_callback_errors(qdlib):
     with pytest.raises(QdError) as e:
         potential_jacobi(R, r, x, m, lambda a, b, c: np.full(a.shape, np.nan))
     assert e.value.code == QD_ERR_PES
+
+
+@pytest.mark.parametrize("K", [0, 1, 3])
+def test_cs_legendre_matches_host(qdlib, K):
+    x, w = S.gauss_legendre(24)
+    m = 23 - K
+    out = np.empty((24, m + 1))
+    _abi.check(qdlib.qd_cs_legendre(24, K, m, x.ctypes.data_as(_abi.c_double_p),
+                                    out.ctypes.data_as(_abi.c_double_p)))
+    ref = S.cs_legendre(x, K, m)
+    if K == 0:
+        assert np.array_equal(out, S.legendre_p2(m, x))
+    assert np.abs(out - ref).max() < 1e-13
+    # the reference's transform pair is the identity on the basis
+    Q = np.sqrt(w)[:, None] * np.sqrt(np.arange(m + 1) + 0.5)[None, :] * out
+    assert np.abs(Q.T @ Q - np.eye(m + 1)).max() < 1e-12

@@ -328,3 +328,54 @@ def test_leps_potential_on_gpu(system):
             assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
         else:
             assert np.array_equal(np.minimum(got, 2.5), potential_leps_gpu(R, r, x, m, pes))
+
+
+def _cs_base(n1=32, n2=32, nth=16, steps=30, **kw):
+    return S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=steps, n_energies=9,
+                        n_gradient_points=5, r=(0.5, 9.0), **kw)
+
+
+def test_cs_block_fp64_matches_oracle():
+    # centrifugal-sudden block J = 5, K = 2 (n_j = n_theta - 2, basis Pbar_j^2)
+    base = _cs_base()
+    run = S.cs_case(base, 5, 2, 0, 2)
+    a, b = S.copy_case(run), S.copy_case(run)
+    norms, _ = O.oracle_time_evolution(a, norms=True)
+    with Propagator(b) as p:
+        p.propagate(30)
+        gn = p.norms(30)
+        e_gpu = p.energies()
+        p.download()
+    assert rel(b.psi, a.psi) < FP64_PSI_REL
+    assert np.abs(gn - norms).max() < FP64_PSI_REL * norms.max()
+    assert np.abs(b.CRP.CRP - a.CRP.CRP).max() < FP64_CRP_ABS
+    e_ref = O.oracle_energies(a)
+    assert np.abs(e_gpu - e_ref).max() < 1e-10 * np.abs(e_ref).max()
+
+
+@pytest.mark.parametrize("slice_kind", ["auto", "8"])
+def test_cs_mixed_batch(slice_kind, monkeypatch):
+    # one batch of blocks with different K (different angular bases and n_j):
+    # FP64 against the oracle run by run; complex64 (tensor-core column pass,
+    # per-run operand images) against FP64
+    if slice_kind != "auto":
+        monkeypatch.setenv("QD_SLICE_CLUSTER", slice_kind)
+    base = _cs_base(64, 64, 32, steps=40)
+    combos = [(0, 0, 0, 0), (5, 1, 0, 1), (5, 2, 0, 2), (10, 0, 1, 0), (10, 3, 0, 2)]
+    runs = [S.cs_case(base, *c) for c in combos]
+    got = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        rs = [S.copy_case(r) for r in runs]
+        for r in rs:
+            r.options.precision = prec
+        with Propagator(rs) as p:
+            p.propagate(40)
+            got[prec] = [(p.psi(i), p.crp(i)) for i in range(len(rs))]
+    for r, (psi64, crp64), (psi32, crp32) in zip(runs, got[QD_PREC_FP64], got[QD_PREC_FP32]):
+        a = S.copy_case(r)
+        O.oracle_time_evolution(a)
+        assert rel(psi64, a.psi) < FP64_PSI_REL
+        assert np.abs(crp64 - a.CRP.CRP).max() < FP64_CRP_ABS
+        if np.abs(a.psi).max() > 0:
+            assert rel(psi32, psi64) < 1e-4
+        assert np.abs(crp32 - crp64).max() < FP32_CRP_ABS
