@@ -140,6 +140,7 @@ struct TcDev {
   const float4 *mats;    // image sets (B1 hi|lo, B2 hi|lo), set_bytes apart
   uint32_t set_bytes;
   const int *run_set;    // image set of each run (null: set 0)
+  const int *run_order;  // tile order: virtual run v is run_order[v], runs of a set adjacent
   const int *run_nl;     // orders stored per run (null: n_l)
   int *status;           // device status word (0 = ok)
   int renorm;            // per-column isometry rescaling on
@@ -219,7 +220,8 @@ constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share
 // leaves the kernel (flux rows, psi_z, the last step of a call: the "slow"
 // tiles), elsewhere GEMM2 runs on V * D1 unscaled and one factor
 // dd sqrt(n_l / n_out) at the store does both.
-template <int S, int MODE, bool EX>
+// MS: runs of the batch have different angular bases (image sets, orders stored)
+template <int S, int MODE, bool EX, bool MS>
 __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev t)
 {
   constexpr int mode = MODE;
@@ -252,12 +254,15 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
                  :: "r"(smem_u32(tmem_slot)), "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // this CTA's tiles: a contiguous range, so that it meets few run boundaries
+  // tiles are strided over the CTAs (neighbouring CTAs read neighbouring
+  // columns); tile t belongs to virtual run t / tpr, and runs that share an
+  // angular set are adjacent in that order, so a CTA reloads its operand
+  // images at most (sets - 1) times
   const int n12 = (int)p.n12, n1 = p.n1;
   const int tpr = (n12 + TPTS - 1) / TPTS;      // tiles per run
   const int ntiles = tpr * p.nruns;
-  const int tbeg = (int)(((long)blockIdx.x * ntiles) / gridDim.x);
-  const int tend = (int)(((long)(blockIdx.x + 1) * ntiles) / gridDim.x);
+  const int tbeg = blockIdx.x, tend = ntiles;
+#define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[(tl) / tpr] : (tl) / tpr)
   const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
   // the B images of set `st` (4 * B_BYTES, a multiple of 16) by bulk
   // asynchronous copies from this GPU's global memory into this CTA's shared
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
     }                                                                                  \
   } while (0)
-  int loaded = tbeg < tend && t.run_set ? t.run_set[tbeg / tpr] : 0;   // image set in smem
+  int loaded = MS && tbeg < tend && t.run_set ? t.run_set[QD_RUN_OF(tbeg)] : 0;   // image set in smem
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
@@ -313,7 +318,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   float a[H];
 #define QD_PREFETCH_A(tl)                                                            \
   do {                                                                               \
-    const int rr = (tl) / tpr, qq = ((tl) - rr * tpr) * TPTS + pt;                   \
+    const int rr = (tl) < tend ? QD_RUN_OF(tl) : 0;                                  \
+    const int qq = ((tl) - ((tl) / tpr) * tpr) * TPTS + pt;                          \
     const bool ok = EX || ((tl) < tend && qq < n12);                                 \
     const float *src = lsrc + (size_t)rr * nl * stride + (size_t)c0 * stride + 2 * qq + comp; \
     _Pragma("unroll") for (int u = 0; u < H; u++) {                                  \
@@ -326,7 +332,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #define QD_STAGE_EV(tl)                                                              \
   do {                                                                               \
     if ((tl) < tend) {                                                               \
-      const int rr = (tl) / tpr, qb = ((tl) - rr * tpr) * TPTS;                      \
+      const int rr = QD_RUN_OF(tl), qb = ((tl) - ((tl) / tpr) * tpr) * TPTS;       \
       const float2 *eb = expv + (size_t)rr * p.vrun + qb;                            \
       for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
         const int k = x / (TPTS / 2), c2 = 2 * (x % (TPTS / 2));                     \
@@ -339,17 +345,20 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   if (mode != COL_HEAD) QD_PREFETCH_A(tbeg);
   if (mode == COL_MID) QD_STAGE_EV(tbeg);
 
-  for (int tile = tbeg; tile < tend && !failed; tile++) {
-    const int run = tile / tpr;
-    const int set = t.run_set ? t.run_set[run] : 0;
-    if (set != loaded) {                        // a run with another angular basis
-      if (tid == 0) QD_LOAD_IMAGES(set);        // earlier MMAs have all completed
-      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
-      ph3 ^= 1;
-      loaded = set;
+  for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
+    const int run = QD_RUN_OF(tile);
+    int nlr = nl;                               // orders stored for this run
+    if constexpr (MS) {
+      const int set = t.run_set ? t.run_set[run] : 0;
+      if (set != loaded) {                      // a run with another angular basis
+        if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
+        if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+        ph3 ^= 1;
+        loaded = set;
+      }
+      if (t.run_nl) nlr = t.run_nl[run];
     }
-    const int nlr = t.run_nl ? t.run_nl[run] : nl;   // orders stored for this run
-    const int q0 = (tile - run * tpr) * TPTS;
+    const int q0 = (tile - (tile / tpr) * tpr) * TPTS;
     const int q = q0 + pt;
     const bool qok = EX || q < n12;
     int j, i;
@@ -483,10 +492,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
     }
     if (mode == COL_TAIL) {
-      QD_PREFETCH_A(tile + 1);
+      QD_PREFETCH_A(tile + (int)gridDim.x);
       continue;
     }
-    if (mode == COL_MID) QD_STAGE_EV(tile + 1);   // evs is free again
+    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
@@ -494,7 +503,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
       mma_commit(mb2);
     }
-    if (mode != COL_HEAD) QD_PREFETCH_A(tile + 1);   // next tile's loads fly during GEMM2
+    if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
@@ -526,13 +535,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
 #pragma unroll
       for (int x = 0; x < 4; x++)
-        if ((EX || qok) && c0 + u + x < nlr) dst[(u + x) * stride] = v[x] * so;
+        if ((EX || qok) && (EX && !MS ? true : c0 + u + x < nlr)) dst[(u + x) * stride] = v[x] * so;
     }
     tc_fence_before();
   }
 #undef QD_PREFETCH_A
 #undef QD_STAGE_EV
 #undef QD_LOAD_IMAGES
+#undef QD_RUN_OF
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
@@ -545,34 +555,36 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   }
 }
 
-template <int S, bool EX> cudaError_t set_smem_attr_ex(int bytes)
+template <int S, bool EX, bool MS> cudaError_t set_smem_attr_ex(int bytes)
 {
-  cudaError_t e = cudaFuncSetAttribute(k_column_tc<S, COL_HEAD, EX>,
+  cudaError_t e = cudaFuncSetAttribute(k_column_tc<S, COL_HEAD, EX, MS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_column_tc<S, COL_MID, EX>,
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_MID, EX, MS>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_column_tc<S, COL_TAIL, EX>,
+    e = cudaFuncSetAttribute(k_column_tc<S, COL_TAIL, EX, MS>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 }
 template <int S> cudaError_t set_smem_attr(int bytes)
 {
-  cudaError_t e = set_smem_attr_ex<S, false>(bytes);
+  cudaError_t e = set_smem_attr_ex<S, false, false>(bytes);
+  if (e == cudaSuccess) e = set_smem_attr_ex<S, false, true>(bytes);
   if constexpr (S == 64) {
-    if (e == cudaSuccess) e = set_smem_attr_ex<S, true>(bytes);
+    if (e == cudaSuccess) e = set_smem_attr_ex<S, true, false>(bytes);
+    if (e == cudaSuccess) e = set_smem_attr_ex<S, true, true>(bytes);
   }
   return e;
 }
 
-template <int S, bool EX>
+template <int S, bool EX, bool MS>
 void launch_mode_ex(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
                     int mode)
 {
-  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD, EX><<<grid, NTHREADS, smem, s>>>(p, t);
-  else if (mode == COL_MID) k_column_tc<S, COL_MID, EX><<<grid, NTHREADS, smem, s>>>(p, t);
-  else k_column_tc<S, COL_TAIL, EX><<<grid, NTHREADS, smem, s>>>(p, t);
+  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
+  else if (mode == COL_MID) k_column_tc<S, COL_MID, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
+  else k_column_tc<S, COL_TAIL, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
 }
 
 template <int S>
@@ -580,10 +592,13 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
                  int mode)
 {
   const bool ex = S == 64 && p.nl == S && p.nth == S && p.n12 % TPTS == 0 && p.n1 % TPTS == 0;
+  const bool ms = t.run_set || t.run_nl;
   if constexpr (S == 64) {
-    if (ex) { launch_mode_ex<S, true>(grid, smem, s, p, t, mode); return; }
+    if (ex && ms) { launch_mode_ex<S, true, true>(grid, smem, s, p, t, mode); return; }
+    if (ex) { launch_mode_ex<S, true, false>(grid, smem, s, p, t, mode); return; }
   }
-  launch_mode_ex<S, false>(grid, smem, s, p, t, mode);
+  if (ms) launch_mode_ex<S, false, true>(grid, smem, s, p, t, mode);
+  else launch_mode_ex<S, false, false>(grid, smem, s, p, t, mode);
 }
 
 template <int S> constexpr int smem_bytes_for()
@@ -719,6 +734,7 @@ cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode
   t.mats = reinterpret_cast<const float4 *>(plan.mats);
   t.set_bytes = (uint32_t)plan.set_bytes;
   t.run_set = p.run_set;
+  t.run_order = p.run_order;
   t.run_nl = p.run_nl;
   t.status = tc_status_ptr(plan);
   t.renorm = plan.renorm;

@@ -125,7 +125,7 @@ struct qd_handle {
   // centrifugal-sudden run has j = K + l
   int nsets = 1, jrows = 0;
   std::vector<int> run_set, run_k, run_nl;
-  int *d_run_set = nullptr, *d_run_k = nullptr, *d_run_nl = nullptr;
+  int *d_run_set = nullptr, *d_run_k = nullptr, *d_run_nl = nullptr, *d_run_order = nullptr;
   int npts = 0, h = 0, surf_j0 = 0, ne = 0;
   bool do_crp = false, have_dump = false;
   double dt = 0;
@@ -329,6 +329,7 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   p.surf = h->d_surf; p.surf_j0 = h->surf_j0; p.surf_nrows = 2 * h->h + 1;
   p.w = h->d_w; p.norm_out = norm_out; p.out_z = out_z ? 1 : 0;
   p.run_set = h->d_run_set; p.set_stride = (long)h->nth * h->nl; p.run_nl = h->d_run_nl;
+  p.run_order = h->d_run_order;
   cudaError_t e;
   TRY(prof_mark(h, -1));
   if (sizeof(R) == 4 && h->use_tc) e = launch_column_tc(h->tc, p, mode, h->st);
@@ -714,9 +715,18 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   TRY(h->alloc(h->d_WP32, sstride * h->nsets));
   TRY(h->alloc(h->d_P32lo, sstride * h->nsets));
   TRY(h->alloc(h->d_WP32lo, sstride * h->nsets));
-  if (h->nsets > 1) TRY(upload(h, h->d_run_set, h->run_set.data(), nruns));
+  if (h->nsets > 1) {
+    TRY(upload(h, h->d_run_set, h->run_set.data(), nruns));
+    std::vector<int> order(nruns);                 // runs grouped by angular set
+    for (int r = 0; r < nruns; r++) order[r] = r;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return h->run_set[a] < h->run_set[b]; });
+    TRY(upload(h, h->d_run_order, order.data(), nruns));
+  }
   if (any_k) TRY(upload(h, h->d_run_k, h->run_k.data(), nruns));
-  TRY(upload(h, h->d_run_nl, h->run_nl.data(), nruns));
+  bool ragged = false;                      // some run stores fewer orders than the layout
+  for (int r = 0; r < nruns; r++) ragged = ragged || h->run_nl[r] < h->nl;
+  if (ragged) TRY(upload(h, h->d_run_nl, h->run_nl.data(), nruns));
   std::vector<double> T1, I1, T2, I2;
   radial_tables(d->r1, T1, I1);
   radial_tables(d->r2, T2, I2);

@@ -52,6 +52,7 @@ struct ColumnParams {
   const int *run_set;
   long set_stride;
   const int *run_nl;
+  const int *run_order;    // tensor-core pass: tile order over runs (null: 0, 1, ...)
 };
 
 struct FluxParams {
