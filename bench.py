@@ -1,7 +1,7 @@
 """Benchmark: grid-point * steps / s of the split-operator propagator.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0|c2|c2j0]
+                    [--workload c1|c0|c2|c2j0|c3]
 
 Workload (default c1): F + H2, J = 0, extended-LEPS surface on a
 128 x 128 x 64 Jacobi grid (n_l = 64), complex64 wavefunction with the
@@ -41,6 +41,56 @@ METRIC = "grid-pt*steps/s"
 FLUSH_BYTES = 256 << 20
 
 
+EXTRA = {}
+
+
+def surrogate_c1(precision, n_train=200000, steps=20000, seed=12345):
+    """C1 with the potential replaced by the MLP surrogate: training on the GPU,
+    the judge's |dV| on the grid, and |dP(E)| of two full 10000-step complex64
+    propagations (plain LEPS vs surrogate)."""
+    from qd_b200 import systems as S
+    from qd_b200.surrogate import Surrogate, training_set, judge
+    from qd_b200.timeevolution import Propagator, potential_jacobi
+    data = S.case_c1(precision=precision)
+    m_amu = np.array([18.9984, 1.00783, 1.00783]) * S.AMU_ME
+    pes = S.leps_f_h2()
+    R, r, x = data.r1.r, data.r2.r, data.theta.x
+    r12, r23, r13, V = training_set(pes, m_amu, n=n_train, seed=seed)
+    sur = Surrogate(seed=seed)
+    t0 = time.perf_counter()
+    loss = sur.fit(r12, r23, r13, V, steps=steps)
+    t_train = time.perf_counter() - t0
+    sur.potential(R, r, x, m_amu)
+    t0 = time.perf_counter()
+    pot = sur.potential(R, r, x, m_amu)
+    t_grid = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    potential_jacobi(R, r, x, m_amu, pes)
+    t_plain = time.perf_counter() - t0
+    rms, mx, _, plain = judge(sur, pes, R, r, x, m_amu)
+    crp = []
+    for p_ in (plain, pot):
+        d = S.copy_case(data)
+        d.pot = np.ascontiguousarray(p_)
+        d.options.precision = 1
+        with Propagator(d) as pr:
+            pr.propagate(10000)
+            crp.append(pr.crp())
+    eta = data.CRP.eta_sq
+    sel = eta > 1e-3 * eta.max()
+    sur.close()
+    out = S.copy_case(data)
+    out.pot = np.ascontiguousarray(pot)
+    info = {"n_train": int(r12.size), "adam_steps": steps, "batch": 4096,
+            "train_seconds": t_train, "final_loss_std_units": loss,
+            "dV_rms_meV": rms * S.HARTREE_EV * 1e3, "dV_max_meV": mx * S.HARTREE_EV * 1e3,
+            "dV_region": "grid points where the plain LEPS is below 3 eV",
+            "max_abs_dP_10000_steps": float(np.abs(crp[0] - crp[1])[sel].max()),
+            "grid_eval_seconds_gpu_mlp": t_grid,
+            "grid_eval_seconds_plain_pes_host_callback": t_plain}
+    return out, info
+
+
 def as_runs(data):
     """A workload is one run (a data struct) or a batch (a list of them)."""
     return list(data) if isinstance(data, (list, tuple)) else [data]
@@ -75,6 +125,12 @@ def build_workload(name, precision, runs=64):
     elif name == "c0":
         data = S.case_c0(precision=precision)
         desc = "H+H2 J=0 extended-LEPS, 64x64x40 Jacobi grid, n_l=39, dt=10 au, 241 energies"
+    elif name == "c3":
+        data, info = surrogate_c1(precision)
+        EXTRA["surrogate"] = info
+        desc = ("F+H2 J=0 on the MLP surrogate of the extended-LEPS surface (trained on the GPU "
+                f"on {info['n_train']} LEPS-labelled geometries), 128x128x64 Jacobi grid, n_l=64, "
+                "dt=10 au, 241 energies")
     elif name == "c2":
         data = S.case_c2(runs, precision=precision)
         desc = (f"batch of {runs} F+H2 centrifugal-sudden blocks (J in 0,5,10,15,20; "
@@ -330,7 +386,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "value_l2_resident": pts * K / (ms_warm * 1e-3),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clk.summary(), "gpu_launches": launches,
+            "clocks": clk.summary(), "gpu_launches": launches, **EXTRA,
             "pe_curves_per_hour_e2e": curves_per_hour}
     print(json.dumps(line))
     if dist:
@@ -343,7 +399,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c2j0"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c2j0", "c3"])
     ap.add_argument("--runs", type=int, default=64, help="runs of the c2j0 batch")
     ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -265,6 +265,43 @@ int qd_read_grids(const char *dir, int32_t n, double *x, double *w);
  * recurrence of common/LegendreP2.m:9-21, computed in FP64 on the GPU. */
 int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre);
 
+/* ---- learned PES surrogate ---------------------------------------------- */
+
+/* A small permutation-symmetric MLP in place of a PES routine.  No counterpart
+ * in the reference, which evaluates its PES (Fortran/MEX) at every grid point.
+ * Features p_ij = exp(-r_ij / 1.5 bohr): (p23, p12 + p13, p12 p13), invariant
+ * under exchanging the two diatom atoms, standardised; four dense SiLU layers
+ * of width 64; linear scalar output (standardised V).  BF16-rounded weights in
+ * every product, FP32 accumulation, FP32 Adam masters.  Trained and evaluated
+ * on the GPU by this library's kernels; the plain PES judges it. */
+typedef struct qd_mlp qd_mlp;
+int     qd_mlp_create(qd_mlp **out, uint64_t seed);      /* He-uniform initial weights */
+int     qd_mlp_destroy(qd_mlp *m);
+int32_t qd_mlp_n_params(void);
+/* FP32 master weights (qd_mlp_n_params floats) and the standardisation
+ * (feature means[3], feature stds[3], V mean, V std). */
+int qd_mlp_get_params(qd_mlp *m, float *w_out, float norm_out[8]);
+int qd_mlp_set_params(qd_mlp *m, const float *w, const float norm[8]);
+/* Feature and target standardisation from a training set. */
+int qd_mlp_fit_normalisation(qd_mlp *m, int64_t n, const double *r12, const double *r23,
+                             const double *r13, const double *V);
+/* train_steps > 0: that many Adam steps over the n samples in minibatches of
+ * `batch` (in order, wrapping), learning rate decaying geometrically from lr
+ * to lr_end; loss_out = mean squared error (standardised V) of the last epoch.
+ * train_steps <= 0: no update; loss_out = the loss over all n samples and, if
+ * grad_out, its gradient with respect to the FP32 parameters. */
+int qd_mlp_train(qd_mlp *m, int64_t n, const double *r12, const double *r23, const double *r13,
+                 const double *V, int32_t train_steps, int32_t batch, double lr, double lr_end,
+                 float *grad_out, double *loss_out);
+/* V (hartree) at n geometries, r_ij in bohr. */
+int qd_mlp_eval(qd_mlp *m, int64_t n, const double *r12, const double *r23, const double *r13,
+                double *V_out);
+/* The surrogate on the Jacobi grid with the mapping, mask and cap of
+ * qd_potential_jacobi (H3/H3PESJacobi.m:5-27). */
+int qd_mlp_potential(qd_mlp *m, const qd_radial *R, const qd_radial *r, const qd_angle *theta,
+                     const double masses[3], double vmax, double rmin, int32_t cap,
+                     double *pot_out);
+
 /* theta.legendre of centrifugal-sudden block K: L[l][k] =
  * Pbar_{K+l}^K(x_k) / sqrt(l + 1/2), l = 0..m, with Pbar_j^K the associated
  * Legendre function normalised to one on [-1, 1] (no Condon-Shortley phase),

@@ -7,6 +7,7 @@ import ctypes as C
 import os
 
 c_double_p = C.POINTER(C.c_double)
+c_float_p = C.POINTER(C.c_float)
 
 QD_OK = 0
 QD_ERR_INVALID = -1
@@ -203,6 +204,20 @@ def lib():
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
         "qd_cs_legendre": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, c_double_p, c_double_p]),
+        "qd_mlp_create": (C.c_int, [P(H), C.c_uint64]),
+        "qd_mlp_destroy": (C.c_int, [H]),
+        "qd_mlp_n_params": (C.c_int32, []),
+        "qd_mlp_get_params": (C.c_int, [H, c_float_p, c_float_p]),
+        "qd_mlp_set_params": (C.c_int, [H, c_float_p, c_float_p]),
+        "qd_mlp_fit_normalisation": (C.c_int, [H, C.c_int64, c_double_p, c_double_p,
+                                               c_double_p, c_double_p]),
+        "qd_mlp_train": (C.c_int, [H, C.c_int64, c_double_p, c_double_p, c_double_p,
+                                   c_double_p, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                   c_float_p, c_double_p]),
+        "qd_mlp_eval": (C.c_int, [H, C.c_int64, c_double_p, c_double_p, c_double_p,
+                                  c_double_p]),
+        "qd_mlp_potential": (C.c_int, [H, P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
+                                       C.c_double, C.c_double, C.c_int32, c_double_p]),
         "qd_potential_jacobi": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
                                           PES_FN, C.c_void_p, C.c_double, C.c_double,
                                           C.c_int32, c_double_p]),

@@ -1,0 +1,98 @@
+"""The PES surrogate's GPU kernels (qd_mlp_*): forward pass and gradient
+against the FP64 restatement (oracle/mlp_oracle.py), permutation symmetry,
+training judged by the plain PES, and what it gains over the plain PES routine.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from qd_b200 import systems as S
+from qd_b200.surrogate import Surrogate, training_set, judge
+
+pytestmark = pytest.mark.gpu
+
+MASSES = np.array([18.9984, 1.00783, 1.00783]) * S.AMU_ME
+
+
+def _data(n, seed):
+    return training_set(S.leps_f_h2(), MASSES, n=n, seed=seed)
+
+
+def test_forward_and_gradient_match_fp64_restatement():
+    r12, r23, r13, V = _data(3000, 11)
+    with Surrogate(seed=7) as sur:
+        sur.fit_normalisation(r12, r23, r13, V)
+        w, norm = sur.params()
+        # forward: the GPU output against the FP64 network with the same BF16 weights
+        got = sur(r12, r23, r13)
+        ref = M.predict(w, norm, r12, r23, r13)
+        assert np.abs(got - ref).max() < 1e-5 * np.abs(ref).max() + 1e-7
+        loss, g = sur.loss_and_grad(r12, r23, r13, V)
+    l_ref, g_ref = M.loss_and_grad(w, norm, r12, r23, r13, V)
+    assert abs(loss - l_ref) < 1e-4 * l_ref
+    assert np.linalg.norm(g - g_ref) < 2e-3 * np.linalg.norm(g_ref)
+    for l in range(M.NL):                       # each layer's block, not just the total
+        K = M.NF if l == 0 else M.W
+        o = M.layer_off(l)
+        blk = slice(o, o + M.W * K + M.W)
+        assert np.linalg.norm(g[blk] - g_ref[blk]) < 5e-3 * np.linalg.norm(g_ref[blk]) + 1e-9
+
+
+def test_exchange_symmetry_is_exact():
+    r12, r23, r13, V = _data(1000, 12)
+    with Surrogate(seed=8) as sur:
+        sur.fit_normalisation(r12, r23, r13, V)
+        assert np.array_equal(sur(r12, r23, r13), sur(r13, r23, r12))
+
+
+def test_training_judged_by_the_plain_pes():
+    pes = S.leps_f_h2()
+    r12, r23, r13, V = _data(50000, 13)
+    with Surrogate(seed=9) as sur:
+        first = sur.fit(r12, r23, r13, V, steps=1, batch=4096)
+        last = sur.fit(r12, r23, r13, V, steps=4000, batch=4096, normalise=False)
+        assert last < 0.05 * first
+        # held-out geometries of the same distribution
+        h12, h23, h13, hV = _data(20000, 14)
+        d = np.abs(sur(h12, h23, h13) - hV)
+        assert np.sqrt(np.mean(d * d)) * S.HARTREE_EV < 0.02         # 20 meV rms
+        # the grid: the surrogate's own grid kernel against its point evaluation,
+        # and the plain PES as judge where it is below the training cut
+        x, _ = S.gauss_legendre(24)
+        R = np.linspace(0.5, 12.0, 40)
+        r = np.linspace(0.4, 8.0, 32)
+        rms, mx, grid, plain = judge(sur, pes, R, r, x, MASSES)
+        assert rms * S.HARTREE_EV < 0.03
+        masked = plain == 2.5
+        r12g, r13g, r23g = S.jacobi_to_internuclear(R[None, None, :], r[None, :, None],
+                                                     x[:, None, None], MASSES)
+        inside = (np.minimum(np.minimum(r12g, r13g), r23g) > 0.4)
+        assert np.all(grid[~inside] == 2.5)
+        pts = sur(r12g[inside], r23g[inside], r13g[inside])
+        assert np.abs(np.minimum(pts, 2.5) - grid[inside]).max() < 1e-5 * np.abs(grid).max()
+        assert masked.sum() >= (~inside).sum()
+
+
+def test_surrogate_gains_over_the_plain_pes_routine():
+    # what the network buys: the grid on the GPU in one launch against the plain
+    # PES routine called through the host callback, as the reference calls its
+    # PES MEX on every grid point
+    from qd_b200.timeevolution import potential_jacobi
+    pes = S.leps_f_h2()
+    r12, r23, r13, V = _data(20000, 15)
+    x, _ = S.gauss_legendre(64)
+    R = np.linspace(0.5, 12.0, 128)
+    r = np.linspace(0.4, 8.0, 128)
+    with Surrogate(seed=10) as sur:
+        sur.fit(r12, r23, r13, V, steps=300)
+        sur.potential(R, r, x, MASSES)                   # warm-up
+        t0 = time.perf_counter()
+        g = sur.potential(R, r, x, MASSES)
+        t_mlp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    p = potential_jacobi(R, r, x, MASSES, pes)
+    t_plain = time.perf_counter() - t0
+    assert g.shape == p.shape
+    assert t_mlp * 3 < t_plain, (t_mlp, t_plain)
