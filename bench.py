@@ -44,7 +44,7 @@ FLUSH_BYTES = 256 << 20
 EXTRA = {}
 
 
-def surrogate_c1(precision, n_train=200000, steps=20000, seed=12345):
+def surrogate_c1(precision, n_train=200000, steps=60000, seed=12345):
     """C1 with the potential replaced by the MLP surrogate: training on the GPU,
     the judge's |dV| on the grid, and |dP(E)| of two full 10000-step complex64
     propagations (plain LEPS vs surrogate)."""
@@ -58,7 +58,7 @@ def surrogate_c1(precision, n_train=200000, steps=20000, seed=12345):
     r12, r23, r13, V = training_set(pes, m_amu, n=n_train, seed=seed)
     sur = Surrogate(seed=seed)
     t0 = time.perf_counter()
-    loss = sur.fit(r12, r23, r13, V, steps=steps)
+    loss = sur.fit(r12, r23, r13, V, steps=steps, lr=2e-3, lr_end=1e-6)
     t_train = time.perf_counter() - t0
     sur.potential(R, r, x, m_amu)
     t0 = time.perf_counter()

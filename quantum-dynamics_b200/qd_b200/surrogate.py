@@ -7,7 +7,7 @@ at every grid point (H3/H3PESJacobi.m:5-27).
 
     sur = Surrogate(seed=12345)
     r12, r23, r13, V = training_set(pes, masses, n=200000)
-    sur.fit(r12, r23, r13, V, steps=20000)
+    sur.fit(r12, r23, r13, V)                   # 60000 Adam steps
     pot = sur.potential(R, r, x, masses)          # the Jacobi grid, on the GPU
 """
 import ctypes as C
@@ -82,7 +82,7 @@ class Surrogate:
         a, b, c, v = (_as64(x) for x in (r12, r23, r13, V))
         check(lib().qd_mlp_fit_normalisation(self._h, a.size, _dp(a), _dp(b), _dp(c), _dp(v)))
 
-    def fit(self, r12, r23, r13, V, steps=20000, batch=4096, lr=3e-3, lr_end=2e-5,
+    def fit(self, r12, r23, r13, V, steps=60000, batch=4096, lr=2e-3, lr_end=1e-6,
             normalise=True):
         """Adam on the mean squared error of the standardised V; returns the
         mean loss of the last epoch."""
