@@ -96,3 +96,18 @@ def test_surrogate_gains_over_the_plain_pes_routine():
     t_plain = time.perf_counter() - t0
     assert g.shape == p.shape
     assert t_mlp * 3 < t_plain, (t_mlp, t_plain)
+
+
+def test_plain_pes_is_the_fallback():
+    # an untrained network fails the judge, and the plain PES grid comes back
+    from qd_b200.surrogate import potential_with_fallback
+    pes = S.leps_f_h2()
+    r12, r23, r13, V = _data(2000, 16)
+    x, _ = S.gauss_legendre(12)
+    R = np.linspace(0.5, 12.0, 20)
+    r = np.linspace(0.4, 8.0, 16)
+    with Surrogate(seed=17) as sur:
+        sur.fit_normalisation(r12, r23, r13, V)
+        pot, used, rms, mx = potential_with_fallback(sur, pes, R, r, x, MASSES)
+    assert not used and rms * S.HARTREE_EV > 5e-3
+    assert np.array_equal(pot, S.potential_on_grid(R, r, x, MASSES, pes))
