@@ -309,6 +309,21 @@ int qd_mlp_potential(qd_mlp *m, const qd_radial *R, const qd_radial *r, const qd
  * P_l(x_k), the reference's matrix. */
 int qd_cs_legendre(int32_t n, int32_t K, int32_t m, const double *x, double *legendre);
 
+/* Initial wavepacket on the GPU in FP64 (H3/InitWavePacket.m:13-31,
+ * H3/H2VibRotWaveFunction.m:20-46): the v0-th sinc-DVR eigenstate
+ * phi_{v0 j0}(r) of the diatom (v_diatom[r2.n] its potential in hartree, plus
+ * j0(j0+1)/(2 mu r^2)), largest component positive, times
+ * g(R) = (pi delta^2)^(-1/4) exp(-(R-R0)^2/(2 delta^2) - i k0 R) (R0, k0, delta
+ * from r1) and the angular function Pbar_{j0}^K(x_k) (sqrt(j0+1/2) P_{j0} for
+ * K = 0; zero if K > j0).  psi_out: complex128 in the layout of qd_data.psi;
+ * e_vj_out: the diatom level (hartree); phi_out (optional, r2.n): phi_vj. */
+int qd_init_state(const qd_radial *R, const qd_radial *r, const qd_angle *theta, int32_t j0,
+                  int32_t v0, int32_t K, const double *v_diatom, double *psi_out,
+                  double *e_vj_out, double *phi_out);
+/* eta^2(E) of the initial packet (common/EtaSq.m:12-15) at collision
+ * energies e_coll (hartree), on the GPU in FP64. */
+int qd_eta_sq(const qd_radial *R, int32_t ne, const double *e_coll, double *eta_sq_out);
+
 /* ---- potential on the Jacobi grid (H3/H3PESJacobi.m:5-27) --------------- */
 
 /* A PES in the convention of the reference's PES MEX functions

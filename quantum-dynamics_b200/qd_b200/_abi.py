@@ -204,6 +204,10 @@ def lib():
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
         "qd_cs_legendre": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, c_double_p, c_double_p]),
+        "qd_init_state": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), C.c_int32,
+                                    C.c_int32, C.c_int32, c_double_p, c_double_p, c_double_p,
+                                    c_double_p]),
+        "qd_eta_sq": (C.c_int, [P(QdRadial), C.c_int32, c_double_p, c_double_p]),
         "qd_mlp_create": (C.c_int, [P(H), C.c_uint64]),
         "qd_mlp_destroy": (C.c_int, [H]),
         "qd_mlp_n_params": (C.c_int32, []),

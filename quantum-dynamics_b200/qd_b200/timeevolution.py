@@ -227,3 +227,41 @@ def potential_leps_gpu(R, r, x, masses, pes, vmax=2.5, rmin=0.4, cap=True):
                                   m.ctypes.data_as(_abi.c_double_p), C.byref(p), vmax, rmin,
                                   1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
     return out
+
+
+def _radial(c):
+    s = _abi.QdRadial()
+    arr = np.ascontiguousarray(c.r, dtype=np.float64)
+    s.n, s.r, s.dr, s.mass = int(c.n), _abi._ptr(arr), float(c.dr), float(c.mass)
+    s.r0, s.k0, s.delta = float(getattr(c, "r0", 0.0)), float(getattr(c, "k0", 0.0)), \
+        float(getattr(c, "delta", 0.0))
+    s._keep = arr                                 # the pointer's array lives with the struct
+    return s
+
+
+def init_state_gpu(r1, r2, theta, j0, v0, v_diatom, K=0):
+    """(psi, e_vj, phi): the initial wavepacket built on the GPU (qd_init_state);
+    v_diatom is the diatom potential on r2.r (hartree)."""
+    a, b = _radial(r1), _radial(r2)
+    x = np.ascontiguousarray(theta.x, dtype=np.float64)
+    t = _abi.QdAngle()
+    t.n, t.x = x.size, x.ctypes.data_as(_abi.c_double_p)
+    vd = np.ascontiguousarray(v_diatom, dtype=np.float64)
+    psi = np.empty((x.size, int(r2.n), int(r1.n)), dtype=np.complex128)
+    phi = np.empty(int(r2.n))
+    e = C.c_double()
+    check(lib().qd_init_state(C.byref(a), C.byref(b), C.byref(t), int(j0), int(v0), int(K),
+                              vd.ctypes.data_as(_abi.c_double_p),
+                              psi.ctypes.data_as(_abi.c_double_p), C.byref(e),
+                              phi.ctypes.data_as(_abi.c_double_p)))
+    return psi, e.value, phi
+
+
+def eta_sq_gpu(r1, e_coll):
+    """eta^2 at the collision energies, on the GPU (qd_eta_sq)."""
+    a = _radial(r1)
+    e = np.ascontiguousarray(e_coll, dtype=np.float64)
+    out = np.empty(e.size)
+    check(lib().qd_eta_sq(C.byref(a), e.size, e.ctypes.data_as(_abi.c_double_p),
+                          out.ctypes.data_as(_abi.c_double_p)))
+    return out

@@ -379,3 +379,25 @@ def test_cs_mixed_batch(slice_kind, monkeypatch):
         if np.abs(a.psi).max() > 0:
             assert rel(psi32, psi64) < 1e-4
         assert np.abs(crp32 - crp64).max() < FP32_CRP_ABS
+
+
+@pytest.mark.parametrize("j0,v0,K", [(0, 0, 0), (2, 0, 0), (0, 1, 0), (2, 0, 1), (1, 0, 2)])
+def test_initial_state_on_gpu(j0, v0, K):
+    # the GPU builder (sinc-DVR by parallel Jacobi, packet, eta^2) against the
+    # host restatement of InitWavePacket.m / H2VibRotWaveFunction.m / EtaSq.m
+    from qd_b200.timeevolution import init_state_gpu, eta_sq_gpu
+    base = S.build_case("f+h2", 64, 96, 24, m=23, total_steps=1, n_energies=31)
+    pes = S.leps_f_h2()
+    vd = pes.diatom(base.r2.r)
+    psi, e_vj, phi = init_state_gpu(base.r1, base.r2, base.theta, j0, v0, vd, K=K)
+    e_ref, phi_ref = S.diatom_vibrot(base.r2, pes.diatom, j0, v0)
+    assert abs(e_vj - e_ref) < 1e-11 * max(1.0, abs(e_ref))
+    assert np.abs(phi - phi_ref).max() < 1e-8 * np.abs(phi_ref).max()
+    if K == 0:
+        ref, _, _ = S.init_wavepacket(base.r1, base.r2, base.theta, j0, v0, pes.diatom)
+    else:
+        ref = S.cs_case(base, max(K, 1), K, v0, j0).psi
+    assert np.abs(psi - ref).max() < 1e-8 * max(np.abs(ref).max(), 1e-300)
+    e_coll = base.CRP.energies - base.CRP.eDiatomic
+    assert np.abs(eta_sq_gpu(base.r1, e_coll) - S.eta_sq(base.r1, e_coll)).max() < \
+        1e-12 * S.eta_sq(base.r1, e_coll).max()
