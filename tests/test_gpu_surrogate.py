@@ -51,8 +51,9 @@ def test_training_judged_by_the_plain_pes():
     pes = S.leps_f_h2()
     r12, r23, r13, V = _data(50000, 13)
     with Surrogate(seed=9) as sur:
-        first = sur.fit(r12, r23, r13, V, steps=1, batch=4096)
-        last = sur.fit(r12, r23, r13, V, steps=4000, batch=4096, normalise=False)
+        first = sur.fit(r12, r23, r13, V, steps=1, batch=4096, lr=3e-3, lr_end=3e-3)
+        last = sur.fit(r12, r23, r13, V, steps=4000, batch=4096, lr=3e-3, lr_end=2e-5,
+                       normalise=False)
         assert last < 0.05 * first
         # held-out geometries of the same distribution
         h12, h23, h13, hV = _data(20000, 14)
@@ -86,7 +87,7 @@ def test_surrogate_gains_over_the_plain_pes_routine():
     R = np.linspace(0.5, 12.0, 128)
     r = np.linspace(0.4, 8.0, 128)
     with Surrogate(seed=10) as sur:
-        sur.fit(r12, r23, r13, V, steps=300)
+        sur.fit(r12, r23, r13, V, steps=300, lr=3e-3, lr_end=1e-3)
         sur.potential(R, r, x, MASSES)                   # warm-up
         t0 = time.perf_counter()
         g = sur.potential(R, r, x, MASSES)
