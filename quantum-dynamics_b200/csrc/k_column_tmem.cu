@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   float *rsw = sw + S;                                    // [S] 1/sqrt(w_k)
   float2 *evs = reinterpret_cast<float2 *>(rsw + S);      // [S][TPTS] exp(-i V dt) of a tile
 
+  pdl_trigger();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int row = (warp & 3) * 32 + lane;        // TMEM lane == GEMM row
   const int grp = warp >> 2;                     // column group
@@ -342,8 +343,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     }                                                                                \
     asm volatile("cp.async.commit_group;" ::: "memory");                             \
   } while (0)
+  if (mode == COL_MID) QD_STAGE_EV(tbeg);      // exp(-iVdt): set up before this launch
+  pdl_wait();                                   // psi_l, psi_z, flux rows: the previous grid's
   if (mode != COL_HEAD) QD_PREFETCH_A(tbeg);
-  if (mode == COL_MID) QD_STAGE_EV(tbeg);
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
@@ -582,9 +584,19 @@ template <int S, bool EX, bool MS>
 void launch_mode_ex(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
                     int mode)
 {
-  if (mode == COL_HEAD) k_column_tc<S, COL_HEAD, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
-  else if (mode == COL_MID) k_column_tc<S, COL_MID, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
-  else k_column_tc<S, COL_TAIL, EX, MS><<<grid, NTHREADS, smem, s>>>(p, t);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(NTHREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  if (mode == COL_HEAD) cudaLaunchKernelEx(&cfg, k_column_tc<S, COL_HEAD, EX, MS>, p, t);
+  else if (mode == COL_MID) cudaLaunchKernelEx(&cfg, k_column_tc<S, COL_MID, EX, MS>, p, t);
+  else cudaLaunchKernelEx(&cfg, k_column_tc<S, COL_TAIL, EX, MS>, p, t);
 }
 
 template <int S>

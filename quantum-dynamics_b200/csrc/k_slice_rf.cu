@@ -30,6 +30,7 @@
 // Radix-16 and radix-12 DFTs are 4x4 and 4x3 compositions whose internal
 // twiddles are compensated constants (value + residual), like the radix-8
 // and radix-3 butterflies, so no fixed-point rounding bias enters the norm.
+#include <cstdlib>
 #include "qd_kernels.h"
 
 namespace {
@@ -167,7 +168,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   float2 *r1 = S + N2 * RS;                          // rc1[l][0..N1)
   float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
   const int tid = threadIdx.x;
+  pdl_trigger();
   if ((int)blockIdx.x >= p.nruns * p.nl) {           // extra CTAs: flux preparation
+    pdl_wait();
     const int q = ((int)blockIdx.x - p.nruns * p.nl) * NT + tid;
     if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
@@ -179,6 +182,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   const float2 *rc2 = p.rc2 + l * N2;
   for (int e = tid; e < N1; e += NT) r1[e] = __ldg(p.rc1 + l * N1 + e);
   for (int e = tid; e < N2; e += NT) t2[e] = __ldg(tw2 + e);
+  pdl_wait();                                        // psi_l: the column pass's output
   __syncthreads();
 
   // P1: items (j, a); elements i = a + A1 b from global
@@ -296,8 +300,17 @@ template <int N1, int N2, int NT> cudaError_t launch_rf(const LineParams &p, cud
   cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const unsigned grid = (unsigned)(p.nruns * p.nl + p.flux_ctas);
-  k_slice_rf<N1, N2, NT><<<grid, NT, sm, s>>>(p);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(p.nruns * p.nl + p.flux_ctas));
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_slice_rf<N1, N2, NT>, p);
   return cudaGetLastError();
 }
 
@@ -317,4 +330,13 @@ cudaError_t launch_slice_rf(const LineParams &p, cudaStream_t s)
   if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256>(p, s);
   if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512>(p, s);
   return cudaErrorInvalidValue;
+}
+
+bool pdl_enabled()
+{
+  static const bool on = [] {
+    const char *e = getenv("QD_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }

@@ -127,6 +127,15 @@ struct LineParams {
   int jrows;
 };
 
+// Programmatic dependent launch: a hot kernel lets the next one start its
+// prologue (trigger at entry) and waits for the previous grid (and its
+// memory) before its first read of data that grid produces.  Both are no-ops
+// for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// host: whether launches carry the attribute (QD_PDL=0 turns it off)
+bool pdl_enabled();
+
 // rotational-table row of slice sl = run * nl + l, clamped to the table (the
 // padded l-slices of runs with fewer angular functions hold zeros)
 __device__ __forceinline__ int rot_row(const LineParams &p, int sl)
