@@ -2,7 +2,8 @@
 //     psi_l <- Rot(dt/2) IFFT2 [exp(-i(T1+T2)dt)/(n1 n2)] FFT2 Rot(dt/2) psi_l
 // (evolution_dt, timeEvol.C:625-635; the FFTW 2-D DFT pair of
 // fftwinterface.C:70-76; phase tables timeEvol.C:465-517), one l-slice per
-// CTA, with every 1-D transform done as two register passes.
+// CTA (or per 2-CTA cluster), with every 1-D transform done as two register
+// passes.
 //
 // A length N = A*B transform (n = a + A b, k = c + B d) is
 //   pass 1, one item per a:  B-point DFT over b in registers, times W_N^{a c}
@@ -27,11 +28,24 @@
 // k = c + B1 d at slot d of block c; the inverse row transform reads that
 // order directly (its decomposition is the transposed one, A = B1, B = A1).
 //
+// The kinetic phase tables (kc1 permuted to the column-counter order, kc2),
+// rc1[l] and the N2-point roots are staged in shared memory by the prologue,
+// which runs before the previous kernel's results are waited on.
+//
+// A slice may also run on a 2-CTA cluster (for small batches, where one CTA
+// per slice leaves most SMs idle): each CTA then keeps half the rows for the
+// row passes and half the columns, over all rows, for the column passes, and
+// P2 and P5 store their results straight into the shared memory of the CTA
+// that reads them next, so the two transposes cost no extra pass.
+//
 // Radix-16 and radix-12 DFTs are 4x4 and 4x3 compositions whose internal
 // twiddles are compensated constants (value + residual), like the radix-8
 // and radix-3 butterflies, so no fixed-point rounding bias enters the norm.
 #include <cstdlib>
+#include <cooperative_groups.h>
 #include "qd_kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -144,132 +158,195 @@ template <int SGN> struct Dft<16, SGN> {
   static __device__ __forceinline__ void run(float2 *v) { Dft4xQ<16, 4, SGN>::run(v); }
 };
 
-template <int N1, int N2, int NT> struct RfShape {
+template <int N1, int N2, int NT, int CL> struct RfShape {
   static constexpr int A1 = N1 == 64 ? 8 : 16;        // row pass 2 radix (B1 = 8)
   static constexpr int B1 = N1 / A1;
   static constexpr int A2 = N2 / 8;                   // column pass 2 radix (B2 = 8)
   static constexpr int B2 = 8;
   static constexpr int RS = N1 + B1;                  // padded row stride (complex)
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)N2 * RS + N1 + N2);
+  static constexpr int HR = N2 / CL;                  // rows of the row passes per CTA
+  static constexpr int QC = N1 / CL;                  // columns of the column passes per CTA
+  static constexpr int CS = RS / CL;                  // row stride of the column-pass array
+  // row array [HR][RS]; column array [N2][CS] (the row array itself if
+  // CL = 1); rc1[l], W_N2, kc1 in column-counter order, kc2
+  static constexpr size_t SMEM =
+      sizeof(float2) * ((size_t)HR * RS + (CL > 1 ? (size_t)N2 * CS : 0) + 2 * (N1 + N2));
   static_assert(B1 == 8 && RS % 16 == 8, "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
+  static_assert(CL == 1 || (CL == 2 && A1 == 16 && HR == 4 * A2 && CS % 16 == 4),
+                "2-CTA split: four whole row blocks per CTA, column rows A2 b' split at b' = 4");
 };
 
 __device__ __forceinline__ float2 rot_at(const float2 *r1, float2 rj, int i)
 { return cmul(r1[i], rj); }
 
-template <int N1, int N2, int NT>
+__device__ __forceinline__ void cluster_arrive_relaxed()
+{ asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait()
+{ asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_sync()
+{
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// CL = 2: a 2-CTA thread-block cluster per slice.  CTA `rank` runs the row
+// passes on rows [rank HR, (rank+1) HR) and the column passes on columns
+// [rank QC, (rank+1) QC) over all N2 rows.  The two transposes between them
+// ride in the stores of P2 and P5, which write straight into the shared
+// memory of the CTA that reads the element next (distributed shared
+// memory); a cluster barrier follows each.  Every shared-memory load is
+// local.  CL = 1 keeps the slice in one array and works in place.
+template <int N1, int N2, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
-  using Sh = RfShape<N1, N2, NT>;
+  using Sh = RfShape<N1, N2, NT, CL>;
   constexpr int A1 = Sh::A1, B1 = Sh::B1, A2 = Sh::A2, B2 = Sh::B2, RS = Sh::RS;
+  constexpr int HR = Sh::HR, QC = Sh::QC, CS = Sh::CS;
   extern __shared__ float4 smem4[];
-  float2 *S = reinterpret_cast<float2 *>(smem4);    // [N2][RS]
-  float2 *r1 = S + N2 * RS;                          // rc1[l][0..N1)
+  float2 *R = reinterpret_cast<float2 *>(smem4);    // [HR][RS]
+  float2 *C = CL > 1 ? R + HR * RS : R;              // [N2][CS]
+  float2 *r1 = C + (CL > 1 ? N2 * CS : HR * RS);    // rc1[l][0..N1)
   float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
+  float2 *k1 = t2 + N2;                              // kc1[k(q)], q < N1
+  float2 *k2 = k1 + N1;                              // kc2
   const int tid = threadIdx.x;
   pdl_trigger();
-  if ((int)blockIdx.x >= p.nruns * p.nl) {           // extra CTAs: flux preparation
+  if ((int)blockIdx.x >= p.nruns * p.nl * CL) {      // extra CTAs: flux preparation
     pdl_wait();
-    const int q = ((int)blockIdx.x - p.nruns * p.nl) * NT + tid;
+    const int q = ((int)blockIdx.x - p.nruns * p.nl * CL) * NT + tid;
     if (q < p.flux.nruns * p.flux.nth * p.flux.n1) flux_point<float2>(p.flux, q);
     return;
   }
-  const int sl = blockIdx.x, l = rot_row(p, sl);     // slice = run * nl + l; l = table row
+  int rank = 0;
+  float2 *C0 = C, *C1 = C, *R0 = R, *R1 = R;          // each CTA's arrays
+  if constexpr (CL == 2) {
+    cluster_arrive_relaxed();                        // waited on before the first remote store
+    cg::cluster_group cluster = cg::this_cluster();
+    rank = (int)cluster.block_rank();
+    float2 *pc = cluster.map_shared_rank(C, rank ^ 1), *pr = cluster.map_shared_rank(R, rank ^ 1);
+    C0 = rank ? pc : C;
+    C1 = rank ? C : pc;
+    R0 = rank ? pr : R;
+    R1 = rank ? R : pr;
+  }
+  const int sl = blockIdx.x / CL, l = rot_row(p, sl);   // slice = run * nl + l; l = table row
+  const int j0 = rank * HR, q0 = rank * QC;
   float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
   const float2 *tw1 = reinterpret_cast<const float2 *>(p.tw1);
   const float2 *tw2 = reinterpret_cast<const float2 *>(p.tw2);
   const float2 *rc2 = p.rc2 + l * N2;
-  for (int e = tid; e < N1; e += NT) r1[e] = __ldg(p.rc1 + l * N1 + e);
-  for (int e = tid; e < N2; e += NT) t2[e] = __ldg(tw2 + e);
+  for (int e = tid; e < N1; e += NT) {
+    r1[e] = __ldg(p.rc1 + l * N1 + e);
+    k1[e] = __ldg(p.kc1 + (e / A1) + B1 * (e % A1));
+  }
+  for (int e = tid; e < N2; e += NT) {
+    t2[e] = __ldg(tw2 + e);
+    k2[e] = __ldg(p.kc2 + e);
+  }
   pdl_wait();                                        // psi_l: the column pass's output
   __syncthreads();
 
-  // P1: items (j, a); elements i = a + A1 b from global
+  // P1: items (j, a) of this CTA's rows; elements i = a + A1 b from global
   {
     const int a = tid % A1;
     float2 w[B1];
 #pragma unroll
     for (int c = 0; c < B1; c++) w[c] = __ldg(tw1 + a * c);
 #pragma unroll 2
-    for (int e = tid; e < N2 * A1; e += NT) {
-      const int j = e / A1;
-      const float2 rj = __ldg(rc2 + j);
+    for (int e = tid; e < HR * A1; e += NT) {
+      const int j = e / A1, jg = j0 + j;
+      const float2 rj = __ldg(rc2 + jg);
       float2 v[B1];
 #pragma unroll
-      for (int b = 0; b < B1; b++) v[b] = g[j * N1 + a + A1 * b];
+      for (int b = 0; b < B1; b++) v[b] = g[jg * N1 + a + A1 * b];
 #pragma unroll
       for (int b = 0; b < B1; b++) v[b] = cmul(v[b], rot_at(r1, rj, a + A1 * b));
       Dft<B1, -1>::run(v);
 #pragma unroll
-      for (int c = 0; c < B1; c++) S[j * RS + a + (A1 + 1) * c] = c ? cmul(v[c], w[c]) : v[c];
+      for (int c = 0; c < B1; c++) R[j * RS + a + (A1 + 1) * c] = c ? cmul(v[c], w[c]) : v[c];
     }
   }
   __syncthreads();
-  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
-  for (int e = tid; e < N2 * B1; e += NT) {
+  if constexpr (CL == 2) cluster_wait();            // the peer runs: its arrays may be written
+  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d; the
+  // block goes to the column array of the CTA owning its columns
+  for (int e = tid; e < HR * B1; e += NT) {
     const int j = e / B1, c = e % B1;
-    float2 *blk = S + j * RS + (A1 + 1) * c;
+    const float2 *blk = R + j * RS + (A1 + 1) * c;
     float2 v[A1];
 #pragma unroll
     for (int a = 0; a < A1; a++) v[a] = blk[a];
     Dft<A1, -1>::run(v);
+    float2 *dst;
+    if constexpr (CL == 1) dst = R + j * RS + (A1 + 1) * c;
+    else dst = (c < B1 / 2 ? C0 : C1) + (j0 + j) * CS + (A1 + 1) * (c % (B1 / 2));
 #pragma unroll
-    for (int d = 0; d < A1; d++) blk[d] = v[d];
+    for (int d = 0; d < A1; d++) dst[d] = v[d];
   }
-  __syncthreads();
-  // column passes on physical column pc of counter q (frequency k(q))
+  if constexpr (CL == 2) cluster_sync();
+  else __syncthreads();
+  // column passes on column-array column pcol(qq) of counter q = q0 + qq
+  // (frequency k(q) = q / A1 + B1 (q % A1))
+  auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
   // P3: items (q, a'): rows a' + A2 b'
-  for (int e = tid; e < N1 * A2; e += NT) {
-    const int q = e % N1, ap = e / N1;
-    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + ap * RS;
+  for (int e = tid; e < QC * A2; e += NT) {
+    const int qq = e % QC, ap = e / QC;
+    float2 *col = C + pcol(qq) + ap * CS;
     float2 v[B2];
 #pragma unroll
-    for (int b = 0; b < B2; b++) v[b] = col[A2 * b * RS];
+    for (int b = 0; b < B2; b++) v[b] = col[A2 * b * CS];
     Dft<B2, -1>::run(v);
 #pragma unroll
-    for (int c = 0; c < B2; c++) col[A2 * c * RS] = c ? cmul(v[c], t2[ap * c]) : v[c];
+    for (int c = 0; c < B2; c++) col[A2 * c * CS] = c ? cmul(v[c], t2[ap * c]) : v[c];
   }
   __syncthreads();
   // P4: items (q, c'): rows a' + A2 c'; forward pass 2, kinetic phase, inverse pass 1
-  for (int e = tid; e < N1 * B2; e += NT) {
-    const int q = e % N1, cp = e / N1;
-    const int k = (q / A1) + B1 * (q % A1);
-    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + A2 * cp * RS;
-    const float2 k1 = __ldg(p.kc1 + k);
+  for (int e = tid; e < QC * B2; e += NT) {
+    const int qq = e % QC, cp = e / QC;
+    float2 *col = C + pcol(qq) + A2 * cp * CS;
+    const float2 kq = k1[q0 + qq];
     float2 v[A2];
 #pragma unroll
-    for (int a = 0; a < A2; a++) v[a] = col[a * RS];
+    for (int a = 0; a < A2; a++) v[a] = col[a * CS];
     Dft<A2, -1>::run(v);
 #pragma unroll
     for (int d = 0; d < A2; d++)
-      v[d] = cmul(v[d], cscale2(cmul(k1, __ldg(p.kc2 + cp + B2 * d)), p.kscale, p.kscale_lo));
+      v[d] = cmul(v[d], cscale2(cmul(kq, k2[cp + B2 * d]), p.kscale, p.kscale_lo));
     Dft<A2, +1>::run(v);
 #pragma unroll
-    for (int cc = 0; cc < A2; cc++) col[cc * RS] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
+    for (int cc = 0; cc < A2; cc++) col[cc * CS] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
   }
   __syncthreads();
-  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d''
-  for (int e = tid; e < N1 * A2; e += NT) {
-    const int q = e % N1, cc = e / N1;
-    float2 *col = S + (q % A1) + (A1 + 1) * (q / A1) + cc * RS;
+  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d'', to
+  // the row array of the CTA owning the row
+  for (int e = tid; e < QC * A2; e += NT) {
+    const int qq = e % QC, cc = e / QC;
+    const float2 *col = C + pcol(qq) + cc * CS;
     float2 v[B2];
 #pragma unroll
-    for (int a = 0; a < B2; a++) v[a] = col[A2 * a * RS];
+    for (int a = 0; a < B2; a++) v[a] = col[A2 * a * CS];
     Dft<B2, +1>::run(v);
+    if constexpr (CL == 1) {
 #pragma unroll
-    for (int d = 0; d < B2; d++) col[A2 * d * RS] = v[d];
+      for (int d = 0; d < B2; d++) R[(cc + A2 * d) * RS + pcol(qq)] = v[d];
+    } else {
+      const int pr = pcol(q0 + qq);
+#pragma unroll
+      for (int d = 0; d < B2; d++) (d < B2 / 2 ? R0 : R1)[(cc + A2 * (d % (B2 / 2))) * RS + pr] = v[d];
+    }
   }
-  __syncthreads();
+  if constexpr (CL == 2) cluster_sync();            // the last remote access
+  else __syncthreads();
   // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
   {
     const int bk = tid % B1;
     float2 w[A1];
 #pragma unroll
     for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
-    for (int e = tid; e < N2 * B1; e += NT) {
+    for (int e = tid; e < HR * B1; e += NT) {
       const int j = e / B1;
-      float2 *blk = S + j * RS + (A1 + 1) * bk;
+      float2 *blk = R + j * RS + (A1 + 1) * bk;
       float2 v[A1];
 #pragma unroll
       for (int s = 0; s < A1; s++) v[s] = blk[s];
@@ -281,54 +358,76 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   __syncthreads();
   // P7: items (j, c'): slot c' of every block -> i = c' + A1 d', Rot/2, store
 #pragma unroll 2
-  for (int e = tid; e < N2 * A1; e += NT) {
-    const int j = e / A1, c = e % A1;
-    const float2 rj = __ldg(rc2 + j);
+  for (int e = tid; e < HR * A1; e += NT) {
+    const int j = e / A1, c = e % A1, jg = j0 + j;
+    const float2 rj = __ldg(rc2 + jg);
     float2 v[B1];
 #pragma unroll
-    for (int b = 0; b < B1; b++) v[b] = S[j * RS + c + (A1 + 1) * b];
+    for (int b = 0; b < B1; b++) v[b] = R[j * RS + c + (A1 + 1) * b];
     Dft<B1, +1>::run(v);
 #pragma unroll
     for (int d = 0; d < B1; d++)
-      g[j * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
+      g[jg * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
   }
 }
 
-template <int N1, int N2, int NT> cudaError_t launch_rf(const LineParams &p, cudaStream_t s)
+template <int N1, int N2, int NT, int CL>
+cudaError_t launch_rf(const LineParams &p, cudaStream_t s)
 {
-  constexpr size_t sm = RfShape<N1, N2, NT>::SMEM;
-  cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT>,
+  constexpr size_t sm = RfShape<N1, N2, NT, CL>::SMEM;
+  cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT, CL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(p.nruns * p.nl + p.flux_ctas));
+  cfg.gridDim = dim3((unsigned)(p.nruns * p.nl * CL + p.flux_ctas));
   cfg.blockDim = dim3(NT);
   cfg.dynamicSmemBytes = sm;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute attr[2];
+  int na = 0;
+  if (CL > 1) {
+    attr[na].id = cudaLaunchAttributeClusterDimension;
+    attr[na].val.clusterDim.x = CL;
+    attr[na].val.clusterDim.y = 1;
+    attr[na].val.clusterDim.z = 1;
+    na++;
+  }
+  if (pdl_enabled()) {
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    na++;
+  }
   cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
-  cudaLaunchKernelEx(&cfg, k_slice_rf<N1, N2, NT>, p);
+  cfg.numAttrs = na;
+  cudaLaunchKernelEx(&cfg, k_slice_rf<N1, N2, NT, CL>, p);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-int slice_rf_threads(int n1, int n2)
+int slice_rf_threads(int n1, int n2, int cl)
 {
-  if (n1 == 64 && n2 == 64) return 256;
-  if (n1 == 128 && n2 == 96) return 256;
-  if (n1 == 128 && n2 == 128) return 512;
+  if (cl == 1) {
+    if (n1 == 64 && n2 == 64) return 256;
+    if (n1 == 128 && n2 == 96) return 256;
+    if (n1 == 128 && n2 == 128) return 512;
+  } else if (cl == 2) {
+    if (n1 == 128 && n2 == 96) return 256;
+    if (n1 == 128 && n2 == 128) return 512;
+  }
   return 0;
 }
 
-cudaError_t launch_slice_rf(const LineParams &p, cudaStream_t s)
+cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s)
 {
-  if (p.n1 == 64 && p.n2 == 64) return launch_rf<64, 64, 256>(p, s);
-  if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256>(p, s);
-  if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512>(p, s);
+  if (cl == 1) {
+    if (p.n1 == 64 && p.n2 == 64) return launch_rf<64, 64, 256, 1>(p, s);
+    if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256, 1>(p, s);
+    if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512, 1>(p, s);
+  } else if (cl == 2) {
+    if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256, 2>(p, s);
+    if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512, 2>(p, s);
+  }
   return cudaErrorInvalidValue;
 }
 

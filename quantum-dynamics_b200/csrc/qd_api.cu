@@ -397,10 +397,10 @@ LineParams line_params(qd_handle *h, bool f32)
 }
 
 // Autotuner of the complex64 l-space pass: time the fused slice kernel with
-// 1, 2 and 4 CTAs per slice, the register-FFT slice kernel and the split
-// kernels on a scratch wavepacket
-// and keep the fastest.  QD_SLICE_CLUSTER=0|1|2|4|8 forces a choice (8 = the
-// register-FFT kernel).
+// 1, 2 and 4 CTAs per slice, the register-FFT slice kernel on 1 and 2 CTAs
+// per slice and the split kernels on a scratch wavepacket and keep the
+// fastest.  QD_SLICE_CLUSTER=0|1|2|4|8|9 forces a choice (8 = the
+// register-FFT kernel, 9 = the same on a 2-CTA cluster).
 int tune_slice(qd_handle *h)
 {
   h->slice_cluster = 0;
@@ -421,7 +421,7 @@ int tune_slice(qd_handle *h)
   LineParams p = line_params(h, true);
   p.lpsi = scratch;
   float best = 1e30f;
-  for (int cl : {0, 1, 2, 4, SLICE_RF}) {
+  for (int cl : {0, 1, 2, 4, SLICE_RF, SLICE_RF2}) {
     if (cl > 0 && !slice_cluster_ok(h->n1, h->n2, cl)) continue;
     p.cluster = cl;
     bool ok = true;
@@ -455,7 +455,7 @@ template <typename R> int issue_lines(qd_handle *h)
     const int nq = h->nth * h->n1 * h->nruns;
     const int nt = slice_threads(h->n1, h->n2, p.cluster);
     const int ctas = (nq + nt - 1) / nt;
-    const int cl = p.cluster == SLICE_RF ? 1 : p.cluster;   // whole clusters
+    const int cl = slice_ctas(p.cluster);                   // whole clusters
     p.flux_ctas = (ctas + cl - 1) / cl * cl;
   }
   TRY(prof_mark(h, -1));

@@ -208,10 +208,13 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
 // fused slice kernel (FP32): CTAs per slice it can run with for these sizes
 // (0 if none), its launch, and the smem bytes it needs
 constexpr int SLICE_RF = 8;    // LineParams::cluster value of the register-FFT slice kernel
+constexpr int SLICE_RF2 = 9;   // the same on a 2-CTA cluster per slice
+inline int slice_ctas(int cluster)           // CTAs per slice
+{ return cluster == SLICE_RF ? 1 : cluster == SLICE_RF2 ? 2 : cluster; }
 int slice_cluster_ok(int n1, int n2, int cluster);
-int slice_rf_threads(int n1, int n2);        // threads per CTA, 0 if the shape is not built
+int slice_rf_threads(int n1, int n2, int cl); // threads per CTA, 0 if the shape is not built
 int slice_threads(int n1, int n2, int cluster);
-cudaError_t launch_slice_rf(const LineParams &p, cudaStream_t s);
+cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s);
 cudaError_t launch_slice(const LineParams &p, cudaStream_t s);
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const double *w,
                                      const double *legendre, double *P, double *WP,

@@ -165,13 +165,14 @@ def test_fp32_tensor_core_and_simt_agree(monkeypatch):
 @pytest.mark.parametrize("shape", [(64, 64, 32), (128, 128, 64), (128, 96, 64), (48, 40, 24)])
 def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
     # fused slice kernel with 1, 2, 4 CTAs per slice and the register-FFT slice
-    # kernel (8), where they are built, against the three-kernel split pass;
+    # kernel on 1 (8) and 2 (9) CTAs per slice, where they are built, against
+    # the three-kernel split pass;
     # the flux preparation rides in the fused launches, so P(E) is compared too
     n1, n2, nth = shape
     base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=8, n_energies=5,
                         n_gradient_points=5, r=(0.5, 9.0))
     out = {}
-    for cl in ("0", "1", "2", "4", "8"):
+    for cl in ("0", "1", "2", "4", "8", "9"):
         monkeypatch.setenv("QD_SLICE_CLUSTER", cl)
         d = S.copy_case(base)
         d.options.precision = QD_PREC_FP32
@@ -184,15 +185,17 @@ def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
         assert np.abs(crp - ref[1]).max() < 1e-6, cl
 
 
-@pytest.mark.parametrize("shape", [(64, 64, 32), (128, 96, 64)])
-def test_fp32_register_fft_slice_batch_matches_fp64(shape, monkeypatch):
-    # the register-FFT slice kernel on a 3-run batch (flux preparation in its
-    # extra CTAs) against the FP64 plain form of the same runs, 40 steps
+@pytest.mark.parametrize("shape,kind", [((64, 64, 32), "8"), ((128, 96, 64), "8"),
+                                        ((128, 96, 64), "9")])
+def test_fp32_register_fft_slice_batch_matches_fp64(shape, kind, monkeypatch):
+    # the register-FFT slice kernel (one CTA or a 2-CTA cluster per slice) on
+    # a 3-run batch (flux preparation in its extra CTAs) against the FP64
+    # plain form of the same runs, 40 steps
     n1, n2, nth = shape
     base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=40, n_energies=9,
                         n_gradient_points=5, r=(0.5, 9.0))
     runs = S.batch_cases(base, [(0, 0), (0, 1), (1, 0)])
-    monkeypatch.setenv("QD_SLICE_CLUSTER", "8")
+    monkeypatch.setenv("QD_SLICE_CLUSTER", kind)
     got = {}
     for prec in (QD_PREC_FP64, QD_PREC_FP32):
         rs = [S.copy_case(r) for r in runs]
