@@ -34,18 +34,15 @@
 //
 // A slice may also run on a 2-CTA cluster (for small batches, where one CTA
 // per slice leaves most SMs idle): each CTA then keeps half the rows for the
-// row passes and half the columns, over all rows, for the column passes, and
-// P2 and P5 store their results straight into the shared memory of the CTA
-// that reads them next, so the two transposes cost no extra pass.
+// row passes and half the columns, over all rows, for the column passes; the
+// two transposes between them are bulk shared-memory-to-shared-memory copies
+// of whole row halves, so no pass touches the other CTA's memory itself.
 //
 // Radix-16 and radix-12 DFTs are 4x4 and 4x3 compositions whose internal
 // twiddles are compensated constants (value + residual), like the radix-8
 // and radix-3 butterflies, so no fixed-point rounding bias enters the norm.
 #include <cstdlib>
-#include <cooperative_groups.h>
 #include "qd_kernels.h"
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -164,52 +161,83 @@ template <int N1, int N2, int NT, int CL> struct RfShape {
   static constexpr int A2 = N2 / 8;                   // column pass 2 radix (B2 = 8)
   static constexpr int B2 = 8;
   static constexpr int RS = N1 + B1;                  // padded row stride (complex)
-  static constexpr int HR = N2 / CL;                  // rows of the row passes per CTA
-  static constexpr int QC = N1 / CL;                  // columns of the column passes per CTA
-  static constexpr int CS = RS / CL;                  // row stride of the column-pass array
-  // row array [HR][RS]; column array [N2][CS] (the row array itself if
-  // CL = 1); rc1[l], W_N2, kc1 in column-counter order, kc2
-  static constexpr size_t SMEM =
-      sizeof(float2) * ((size_t)HR * RS + (CL > 1 ? (size_t)N2 * CS : 0) + 2 * (N1 + N2));
+  static constexpr int HR = N2 / CL;                  // rows held by one CTA
+  static constexpr int HW = RS / CL;                  // row-half width: B1 / CL whole blocks
+  // own rows [HR][RS]; CL = 2: the peer's rows, this CTA's column half
+  // [HR][HW]; rc1[l], W_N2, kc1 in column-counter order, kc2; two mbarriers
+  static constexpr size_t TABLES = 2 * (N1 + N2);
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (CL > 1 ? (size_t)HR * HW : 0) +
+                                                   TABLES) + (CL > 1 ? 16 : 0);
+  static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row half, one bulk copy
   static_assert(B1 == 8 && RS % 16 == 8, "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
-  static_assert(CL == 1 || (CL == 2 && A1 == 16 && HR == 4 * A2 && CS % 16 == 4),
-                "2-CTA split: four whole row blocks per CTA, column rows A2 b' split at b' = 4");
+  static_assert(CL == 1 || (CL == 2 && A1 == 16 && HR == 4 * A2 && HW == 4 * (A1 + 1) &&
+                            HALF_BYTES % 16 == 0 && HR <= NT),
+                "2-CTA split: four whole row blocks per half, column rows A2 b' split at b' = 4");
 };
 
 __device__ __forceinline__ float2 rot_at(const float2 *r1, float2 rj, int i)
 { return cmul(r1[i], rj); }
 
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{ return (uint32_t)__cvta_generic_to_shared(p); }
+// the same shared-memory offset in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(uint32_t a, uint32_t rank)
+{
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
 __device__ __forceinline__ void cluster_arrive_relaxed()
 { asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_arrive_release()
+{ asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait()
-{ asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
-__device__ __forceinline__ void cluster_sync()
+{ asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+// bulk copy of `bytes` from this CTA's shared memory into the peer's, whose
+// mbarrier receives the byte count
+__device__ __forceinline__ void bulk_to_peer(uint32_t dst, uint32_t src, uint32_t bytes, uint32_t mbar)
 {
-  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
-  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(dst), "r"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+// bounded wait on phase 0 of a local mbarrier; false if it ran out
+__device__ __forceinline__ bool mbar_wait0(uint32_t mbar)
+{
+  for (int it = 0; it < (1 << 22); it++) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], 0;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok) : "r"(mbar) : "memory");
+    if (ok) return true;
+  }
+  return false;
 }
 
 // CL = 2: a 2-CTA thread-block cluster per slice.  CTA `rank` runs the row
-// passes on rows [rank HR, (rank+1) HR) and the column passes on columns
-// [rank QC, (rank+1) QC) over all N2 rows.  The two transposes between them
-// ride in the stores of P2 and P5, which write straight into the shared
-// memory of the CTA that reads the element next (distributed shared
-// memory); a cluster barrier follows each.  Every shared-memory load is
-// local.  CL = 1 keeps the slice in one array and works in place.
+// passes on rows [rank HR, (rank+1) HR) and the column passes on column
+// half `rank` (row blocks 4 rank .. 4 rank + 3) over all N2 rows: its own
+// rows in place in its row array, the peer's rows in a second array.  The
+// two transposes are bulk copies of whole row halves (HW complex, 544
+// bytes) between the CTAs' shared memories: after P2 each CTA sends its
+// rows' other half to the peer, after P5 it sends the peer's rows back; an
+// mbarrier in the receiving CTA counts the bytes in.  Every load and store
+// of the passes is local.  CL = 1 keeps the slice in one array in place.
 template <int N1, int N2, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
   using Sh = RfShape<N1, N2, NT, CL>;
   constexpr int A1 = Sh::A1, B1 = Sh::B1, A2 = Sh::A2, B2 = Sh::B2, RS = Sh::RS;
-  constexpr int HR = Sh::HR, QC = Sh::QC, CS = Sh::CS;
+  constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
-  float2 *R = reinterpret_cast<float2 *>(smem4);    // [HR][RS]
-  float2 *C = CL > 1 ? R + HR * RS : R;              // [N2][CS]
-  float2 *r1 = C + (CL > 1 ? N2 * CS : HR * RS);    // rc1[l][0..N1)
+  float2 *R = reinterpret_cast<float2 *>(smem4);    // own rows [HR][RS]
+  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column half [HR][HW]
+  float2 *r1 = P + (CL > 1 ? HR * HW : 0);           // rc1[l][0..N1)
   float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
   float2 *k1 = t2 + N2;                              // kc1[k(q)], q < N1
   float2 *k2 = k1 + N1;                              // kc2
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL = 2: [0] P filled, [1] R's other half
   const int tid = threadIdx.x;
   pdl_trigger();
   if ((int)blockIdx.x >= p.nruns * p.nl * CL) {      // extra CTAs: flux preparation
@@ -219,19 +247,23 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     return;
   }
   int rank = 0;
-  float2 *C0 = C, *C1 = C, *R0 = R, *R1 = R;          // each CTA's arrays
+  if constexpr (CL > 1) asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
   if constexpr (CL == 2) {
-    cluster_arrive_relaxed();                        // waited on before the first remote store
-    cg::cluster_group cluster = cg::this_cluster();
-    rank = (int)cluster.block_rank();
-    float2 *pc = cluster.map_shared_rank(C, rank ^ 1), *pr = cluster.map_shared_rank(R, rank ^ 1);
-    C0 = rank ? pc : C;
-    C1 = rank ? C : pc;
-    R0 = rank ? pr : R;
-    R1 = rank ? R : pr;
+    if (tid == 0) {
+      const uint32_t tx = HR * Sh::HALF_BYTES;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[0])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[1])));
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                   :: "r"(smem_addr(&mbar[0])), "r"(tx) : "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                   :: "r"(smem_addr(&mbar[1])), "r"(tx) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    cluster_arrive_relaxed();                        // waited on before the first copy
   }
   const int sl = blockIdx.x / CL, l = rot_row(p, sl);   // slice = run * nl + l; l = table row
-  const int j0 = rank * HR, q0 = rank * QC;
+  const int j0 = rank * HR, q0 = rank * (N1 / CL);
   float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
   const float2 *tw1 = reinterpret_cast<const float2 *>(p.tw1);
   const float2 *tw2 = reinterpret_cast<const float2 *>(p.tw2);
@@ -268,76 +300,106 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     }
   }
   __syncthreads();
-  if constexpr (CL == 2) cluster_wait();            // the peer runs: its arrays may be written
-  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d; the
-  // block goes to the column array of the CTA owning its columns
+  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
   for (int e = tid; e < HR * B1; e += NT) {
     const int j = e / B1, c = e % B1;
-    const float2 *blk = R + j * RS + (A1 + 1) * c;
+    float2 *blk = R + j * RS + (A1 + 1) * c;
     float2 v[A1];
 #pragma unroll
     for (int a = 0; a < A1; a++) v[a] = blk[a];
     Dft<A1, -1>::run(v);
-    float2 *dst;
-    if constexpr (CL == 1) dst = R + j * RS + (A1 + 1) * c;
-    else dst = (c < B1 / 2 ? C0 : C1) + (j0 + j) * CS + (A1 + 1) * (c % (B1 / 2));
 #pragma unroll
-    for (int d = 0; d < A1; d++) dst[d] = v[d];
+    for (int d = 0; d < A1; d++) blk[d] = v[d];
   }
-  if constexpr (CL == 2) cluster_sync();
-  else __syncthreads();
-  // column passes on column-array column pcol(qq) of counter q = q0 + qq
-  // (frequency k(q) = q / A1 + B1 (q % A1))
+  bool ok = true;
+  if constexpr (CL == 2) {
+    // the other column half of every own row -> the peer's P array
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    cluster_wait();                                  // the peer's mbarriers are initialised
+    if (tid < HR) {
+      const uint32_t peer = rank ^ 1;
+      bulk_to_peer(peer_addr(smem_addr(P + tid * HW), peer),
+                   smem_addr(R + tid * RS + HW * peer), Sh::HALF_BYTES,
+                   peer_addr(smem_addr(&mbar[0]), peer));
+    }
+    ok = mbar_wait0(smem_addr(&mbar[0]));            // the peer's rows of this half are in
+  } else {
+    __syncthreads();
+  }
+  // column passes: column counter q = q0 + qq (frequency k(q) = q / A1 + B1 (q % A1))
+  // at offset pcol(qq) of this CTA's half; rows A2 b + r, b < 4 in CTA 0's rows
   auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
+  float2 *blo, *bhi;                                 // row 0 of b < 4 and of b >= 4
+  int slo, shi;                                      // their row strides
+  if constexpr (CL == 1) {
+    blo = R; bhi = R + 4 * A2 * RS; slo = shi = RS;
+  } else {
+    blo = rank == 0 ? R : P;
+    bhi = rank == 0 ? P : R + HW;
+    slo = rank == 0 ? RS : HW;
+    shi = rank == 0 ? HW : RS;
+  }
+  auto at = [&](int b, int inner, int qq) -> float2 & {
+    return b < 4 ? blo[(inner + A2 * b) * slo + pcol(qq)]
+                 : bhi[(inner + A2 * (b - 4)) * shi + pcol(qq)];
+  };
+  constexpr int QC = N1 / CL;
   // P3: items (q, a'): rows a' + A2 b'
   for (int e = tid; e < QC * A2; e += NT) {
     const int qq = e % QC, ap = e / QC;
-    float2 *col = C + pcol(qq) + ap * CS;
     float2 v[B2];
 #pragma unroll
-    for (int b = 0; b < B2; b++) v[b] = col[A2 * b * CS];
+    for (int b = 0; b < B2; b++) v[b] = at(b, ap, qq);
     Dft<B2, -1>::run(v);
 #pragma unroll
-    for (int c = 0; c < B2; c++) col[A2 * c * CS] = c ? cmul(v[c], t2[ap * c]) : v[c];
+    for (int c = 0; c < B2; c++) at(c, ap, qq) = c ? cmul(v[c], t2[ap * c]) : v[c];
   }
   __syncthreads();
   // P4: items (q, c'): rows a' + A2 c'; forward pass 2, kinetic phase, inverse pass 1
   for (int e = tid; e < QC * B2; e += NT) {
     const int qq = e % QC, cp = e / QC;
-    float2 *col = C + pcol(qq) + A2 * cp * CS;
+    float2 *col = (cp < 4 ? blo + A2 * cp * slo : bhi + A2 * (cp - 4) * shi) + pcol(qq);
+    const int cs = cp < 4 ? slo : shi;
     const float2 kq = k1[q0 + qq];
     float2 v[A2];
 #pragma unroll
-    for (int a = 0; a < A2; a++) v[a] = col[a * CS];
+    for (int a = 0; a < A2; a++) v[a] = col[a * cs];
     Dft<A2, -1>::run(v);
 #pragma unroll
     for (int d = 0; d < A2; d++)
       v[d] = cmul(v[d], cscale2(cmul(kq, k2[cp + B2 * d]), p.kscale, p.kscale_lo));
     Dft<A2, +1>::run(v);
 #pragma unroll
-    for (int cc = 0; cc < A2; cc++) col[cc * CS] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
+    for (int cc = 0; cc < A2; cc++) col[cc * cs] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
   }
   __syncthreads();
-  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d'', to
-  // the row array of the CTA owning the row
+  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d'', in place
   for (int e = tid; e < QC * A2; e += NT) {
     const int qq = e % QC, cc = e / QC;
-    const float2 *col = C + pcol(qq) + cc * CS;
     float2 v[B2];
 #pragma unroll
-    for (int a = 0; a < B2; a++) v[a] = col[A2 * a * CS];
+    for (int a = 0; a < B2; a++) v[a] = at(a, cc, qq);
     Dft<B2, +1>::run(v);
-    if constexpr (CL == 1) {
 #pragma unroll
-      for (int d = 0; d < B2; d++) R[(cc + A2 * d) * RS + pcol(qq)] = v[d];
-    } else {
-      const int pr = pcol(q0 + qq);
-#pragma unroll
-      for (int d = 0; d < B2; d++) (d < B2 / 2 ? R0 : R1)[(cc + A2 * (d % (B2 / 2))) * RS + pr] = v[d];
-    }
+    for (int d = 0; d < B2; d++) at(d, cc, qq) = v[d];
   }
-  if constexpr (CL == 2) cluster_sync();            // the last remote access
-  else __syncthreads();
+  if constexpr (CL == 2) {
+    // the peer's rows of this half -> back into the peer's row array
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid < HR) {
+      const uint32_t peer = rank ^ 1;
+      bulk_to_peer(peer_addr(smem_addr(R + tid * RS + HW * rank), peer),
+                   smem_addr(P + tid * HW), Sh::HALF_BYTES,
+                   peer_addr(smem_addr(&mbar[1]), peer));
+    }
+    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other half of the own rows is back
+    cluster_arrive_release();                        // this CTA's incoming copies are complete
+    if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
+  } else {
+    __syncthreads();
+  }
   // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
   {
     const int bk = tid % B1;
@@ -369,6 +431,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int d = 0; d < B1; d++)
       g[jg * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
   }
+  // no CTA leaves while its shared memory may still be the source of a copy
+  // (the peer arrives only once all of its incoming copies are complete)
+  if constexpr (CL == 2) cluster_wait();
 }
 
 template <int N1, int N2, int NT, int CL>

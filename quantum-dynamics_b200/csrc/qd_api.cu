@@ -139,6 +139,7 @@ struct qd_handle {
   double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
   float2 *d_expV32 = nullptr;
   float2 *d_rc1 = nullptr, *d_rc2 = nullptr, *d_kc1 = nullptr, *d_kc2 = nullptr;
+  int *d_lstatus = nullptr;       // status word of the l-space kernels (0 = ok)
   int slice_cluster = 0;          // l-space kernel (LineParams::cluster code)
   double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
@@ -301,14 +302,21 @@ FluxParams flux_params(qd_handle *h)
 int after_flux_prep(qd_handle *h);
 template <typename R> int issue_flux_prep(qd_handle *h);
 
-// Device-side status word of the tensor-core pass (bounded waits that ran out).
+// Device-side status words of the tensor-core pass and of the l-space
+// kernels (bounded waits that ran out).
 int check_status(qd_handle *h)
 {
-  if (!h->use_tc) return QD_OK;
   int st = 0;
-  CU(cudaMemcpy(&st, tc_status_ptr(h->tc), sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) return set_err(QD_ERR_DEVICE, "tensor-core column pass: an MMA completion wait "
-                         "timed out (status %d)", st);
+  if (h->use_tc) {
+    CU(cudaMemcpy(&st, tc_status_ptr(h->tc), sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) return set_err(QD_ERR_DEVICE, "tensor-core column pass: an MMA completion wait "
+                           "timed out (status %d)", st);
+  }
+  if (h->d_lstatus) {
+    CU(cudaMemcpy(&st, h->d_lstatus, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) return set_err(QD_ERR_DEVICE, "l-space pass: a shared-memory exchange wait "
+                           "timed out (status %d)", st);
+  }
   return QD_OK;
 }
 
@@ -393,6 +401,7 @@ LineParams line_params(qd_handle *h, bool f32)
   else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
   p.pl1 = h->pl1; p.pl2 = h->pl2;
   p.run_k = h->d_run_k; p.jrows = h->jrows;
+  p.status = h->d_lstatus;
   return p;
 }
 
@@ -771,6 +780,8 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     TRY(h->alloc(h->d_rc2, (size_t)h->jrows * h->n2));
     TRY(h->alloc(h->d_kc1, h->n1));
     TRY(h->alloc(h->d_kc2, h->n2));
+    TRY(h->alloc(h->d_lstatus, 1));
+    CU(cudaMemsetAsync(h->d_lstatus, 0, sizeof(int), h->st));
     CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth * npot, h->jrows, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV32, h->d_rc1, h->d_rc2,
                                 h->d_kc1, h->d_kc2, h->st));

@@ -125,6 +125,7 @@ struct LineParams {
   // the rotational tables have jrows rows
   const int *run_k;
   int jrows;
+  int *status;             // device status word: bounded waits that ran out (0 = ok)
 };
 
 // Programmatic dependent launch: a hot kernel lets the next one start its
