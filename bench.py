@@ -10,8 +10,10 @@ on 241 energies, 11-point flux stencil.  A step is one split-operator step
 of the whole grid (1,048,576 grid points) including the flux capture.
 
 value   device time (CUDA events on the library's stream) of K steps after
-        W warm-up steps, L2 flushed (256 MiB write) before every step outside
-        the timed spans; whole-job = sum over ranks' points / max rank time.
+        W warm-up steps, L2 flushed before every step outside the timed spans
+        (256 MiB written, then read back, so the step meets neither its own
+        data nor dirty lines in L2); whole-job = sum over ranks' points / max
+        rank time.
 e2e     the drop-in entry point qd_time_evolution on host arrays for the
         same K steps: upload of pot and psi, table set-up, the K steps, P(E)
         and the download of psi and P(E), wall clock.
@@ -316,10 +318,10 @@ def run_ours(args):
     value = pts * K * world / (t_max * 1e-3)
 
     # --- end to end through the drop-in entry point -------------------------------
-    # three repetitions, median reported (each a full call: upload, set-up, K steps,
+    # five repetitions, median reported (each a full call: upload, set-up, K steps,
     # P(E), download)
     reps = []
-    for _ in range(3):
+    for _ in range(5):
         e = copy_workload(data)
         for r in as_runs(e):
             r.time.total_steps = K
@@ -340,7 +342,7 @@ def run_ours(args):
     e2e = {"value": pts * K * world / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
            "seconds": e2e_s, "seconds_each": reps,
-           "entry_point": "qd_time_evolution (TimeEvolutionMexCUDA), median of 3 calls"}
+           "entry_point": "qd_time_evolution (TimeEvolutionMexCUDA), median of 5 calls"}
 
     if rank != 0:
         if dist:
@@ -382,7 +384,7 @@ def run_ours(args):
             "config": {"workload": desc, "grid_points": pts,
                        "precision": "FP64 plain" if args.fp64 else
                        "complex64 + 3xTF32 Legendre + FP64 flux accumulation",
-                       "l2": "flushed before every step (256 MiB write, outside timed spans)",
+                       "l2": "flushed before every step (256 MiB write, then read back so no dirty lines remain; outside the timed spans)",
                        "parallelism": f"replicas x{world}"},
             "value_l2_resident": pts * K / (ms_warm * 1e-3),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,

@@ -182,8 +182,9 @@ int qd_destroy(qd_handle *h);
 int qd_propagate(qd_handle *h, int32_t n_steps);
 /* qd_propagate that also reports the device time of the n_steps steps
  * (CUDA events on the handle's stream, summed over steps).  If
- * flush_bytes > 0 a buffer of that size is overwritten between steps, outside
- * the timed spans, so that every step starts with a cold L2. */
+ * flush_bytes > 0 a buffer of that size is overwritten and then read back
+ * between steps, outside the timed spans, so that every step starts with a
+ * cold L2 (holding none of the propagation's data and no dirty lines). */
 int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes,
                        double *device_ms);
 /* Current theta-space psi (layout of qd_data.psi) into psi_out (host). */

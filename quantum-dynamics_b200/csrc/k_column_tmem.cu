@@ -165,6 +165,27 @@ __device__ __forceinline__ void tmem_st4(uint32_t taddr, float a, float b, float
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+// tcgen05.ld of this thread's H consecutive columns: all loads issued, then
+// one wait; the wait names the destination registers, so no use of them can
+// be scheduled before it
+template <int H>
+__device__ __forceinline__ void tmem_ld_all(uint32_t taddr, float (&v)[H])
+{
+  static_assert(H % 4 == 0, "whole x4 loads");
+  uint32_t r[H];
+#pragma unroll
+  for (int u = 0; u < H; u += 4)
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[u]), "=r"(r[u + 1]), "=r"(r[u + 2]), "=r"(r[u + 3]) : "r"(taddr + u));
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
+#pragma unroll
+  for (int u = 4; u < H; u += 4)
+    asm volatile("" : "+r"(r[u]), "+r"(r[u + 1]), "+r"(r[u + 2]), "+r"(r[u + 3]));
+#pragma unroll
+  for (int u = 0; u < H; u++) v[u] = __uint_as_float(r[u]);
+}
+
 // the split of 4 values into the Ahi and Alo TMEM columns (col0 % 4 == 0)
 __device__ __forceinline__ void put4_tmem(uint32_t ahi, uint32_t alo, float x0, float x1,
                                           float x2, float x3)
@@ -400,13 +421,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       ph1 ^= 1;
       tc_fence_after();
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
-        float nt_part = 0.f;
+        float nt_part = 0.f, dv[H];
+        tmem_ld_all<H>(my_d, dv);
 #pragma unroll
-        for (int u = 0; u < H; u += 4) {
-          float v0, v1, v2, v3;
-          tmem_ld4(my_d + u, v0, v1, v2, v3);
-          nt_part = fmaf(v0, v0, fmaf(v1, v1, fmaf(v2, v2, fmaf(v3, v3, nt_part))));
-        }
+        for (int u = 0; u < H; u++) nt_part = fmaf(dv[u], dv[u], nt_part);
         nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
         if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
         __syncthreads();
@@ -424,11 +442,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
                                                  : nullptr;
     float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
                        : nullptr;
+    float dv[H];
+    if (mode != COL_HEAD) tmem_ld_all<H>(my_d, dv);
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
       float v[4];
       if (mode != COL_HEAD) {
-        tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
+#pragma unroll
+        for (int x = 0; x < 4; x++) v[x] = dv[u + x];
 #pragma unroll
         for (int x = 0; x < 4; x++) {
           const int k = c0 + u + x;
@@ -509,17 +530,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
-    float no_part = 0.f;
+    float no_part = 0.f, ov[H];
+    tmem_ld_all<H>(my_d, ov);
 #pragma unroll
-    for (int u = 0; u < H; u += 4) {
-      float v0, v1, v2, v3;
-      tmem_ld4(my_d + u, v0, v1, v2, v3);
-      if (EX) {
-        no_part = fmaf(v0, v0, fmaf(v1, v1, fmaf(v2, v2, fmaf(v3, v3, no_part))));
-      } else {
-        no_part += (c0 + u < t.nnorm ? v0 * v0 : 0.f) + (c0 + u + 1 < t.nnorm ? v1 * v1 : 0.f) +
-                   (c0 + u + 2 < t.nnorm ? v2 * v2 : 0.f) + (c0 + u + 3 < t.nnorm ? v3 * v3 : 0.f);
-      }
+    for (int u = 0; u < H; u++) {
+      if (EX) no_part = fmaf(ov[u], ov[u], no_part);
+      else no_part += c0 + u < t.nnorm ? ov[u] * ov[u] : 0.f;
     }
     no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
     if (!is_im) xch[3 * NG * TPTS + grp * TPTS + pt] = no_part;
@@ -532,13 +548,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     else so = (slow || mode == COL_HEAD) ? 1.f : ddv;
     float *dst = ldst + (size_t)run * nl * stride + (size_t)c0 * stride + 2 * q + comp;
 #pragma unroll
-    for (int u = 0; u < H; u += 4) {
-      float v[4];
-      tmem_ld4(my_d + u, v[0], v[1], v[2], v[3]);
-#pragma unroll
-      for (int x = 0; x < 4; x++)
-        if ((EX || qok) && (EX && !MS ? true : c0 + u + x < nlr)) dst[(u + x) * stride] = v[x] * so;
-    }
+    for (int u = 0; u < H; u++)
+      if ((EX || qok) && (EX && !MS ? true : c0 + u < nlr)) dst[u * stride] = ov[u] * so;
     tc_fence_before();
   }
 #undef QD_PREFETCH_A

@@ -542,7 +542,10 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
   }
   CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n * R, h->st));
   for (int s = 0; s < n; s++) {
-    if (timed && flush_bytes) CU(cudaMemsetAsync(h->d_flush, s & 0xff, flush_bytes, h->st));
+    if (timed && flush_bytes) {       // L2 flush outside the timed spans: write, then read back
+      CU(cudaMemsetAsync(h->d_flush, s & 0xff, flush_bytes, h->st));
+      CU(launch_l2_read(h->d_flush, flush_bytes, h->st));
+    }
     if (timed) CU(cudaEventRecord(h->events[2 * s], h->st));
     if (!h->started) {
       TRY(issue_column<Real>(h, COL_HEAD, false, nullptr, false));
