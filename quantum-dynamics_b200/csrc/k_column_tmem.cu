@@ -82,11 +82,14 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p)
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// round a finite FP32 value to TF32 (10 stored mantissa bits), to nearest
+// with ties away from zero, on its bit pattern: add half of the dropped
+// 13-bit field to the magnitude and clear the field (a carry moves into the
+// exponent, which is the correct round-up); the same result as
+// cvt.rna.tf32.f32 for finite inputs, in two integer operations
 __device__ __forceinline__ float tf32_rna(float x)
 {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr)
@@ -310,23 +313,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     QD_LOAD_IMAGES(loaded);
   }
-  for (int i = tid; i < S; i += NTHREADS) {
-    const double w = i < p.nth ? p.w[i] : 0.0;
-    sw[i] = (float)sqrt(w);
-    rsw[i] = w > 0.0 ? (float)(1.0 / sqrt(w)) : 0.f;
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  const uint32_t lane_base = ((uint32_t)((warp & 3) * 32)) << 16;
-  const uint32_t Ahi = tmem, Alo = tmem + S, D = tmem + 2 * S;       // column bases
-  const uint32_t my_hi = Ahi + lane_base + c0, my_lo = Alo + lane_base + c0;
-  const uint32_t my_d = D + lane_base + c0;
-  const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
-  uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
-  bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
-
+  static_assert(S <= NTHREADS, "one quadrature weight per thread");
+  const double wq = tid < S && tid < p.nth ? p.w[tid] : 0.0;   // in flight during what follows
   // 32-bit tile arithmetic: the host checks n12 * n_l * 2 * n_runs < 2^31
   const int nl = p.nl, nth = p.nth;
   const int stride = 2 * n12;                   // floats between orders l (or k) of a point
@@ -358,7 +346,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       const float2 *eb = expv + (size_t)rr * p.vrun + qb;                            \
       for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
         const int k = x / (TPTS / 2), c2 = 2 * (x % (TPTS / 2));                     \
-        const bool okv = k < nth && qb + c2 < n12;                                   \
+        const bool okv = EX || (k < nth && qb + c2 < n12);                           \
         cp16_zfill(&evs[k * TPTS + c2], okv ? eb + (size_t)k * n12 + c2 : expv, okv); \
       }                                                                              \
     }                                                                                \
@@ -367,6 +355,24 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   if (mode == COL_MID) QD_STAGE_EV(tbeg);      // exp(-iVdt): set up before this launch
   pdl_wait();                                   // psi_l, psi_z, flux rows: the previous grid's
   if (mode != COL_HEAD) QD_PREFETCH_A(tbeg);
+  // the prologue's loads (images, exp(-iVdt), psi_l, weights) are all in
+  // flight before anything waits on one of them
+  if (tid < S) {
+    sw[tid] = (float)sqrt(wq);
+    rsw[tid] = wq > 0.0 ? (float)(1.0 / sqrt(wq)) : 0.f;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = ((uint32_t)((warp & 3) * 32)) << 16;
+  const uint32_t Ahi = tmem, Alo = tmem + S, D = tmem + 2 * S;       // column bases
+  const uint32_t my_hi = Ahi + lane_base + c0, my_lo = Alo + lane_base + c0;
+  const uint32_t my_d = D + lane_base + c0;
+  const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
+  uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
+  // one warp polls each mbarrier; the rest of the CTA sleeps in the barrier
+  bool failed = __syncthreads_or(warp == 0 && !mbar_wait(mb3, 0));
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
@@ -375,7 +381,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       const int set = t.run_set ? t.run_set[run] : 0;
       if (set != loaded) {                      // a run with another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
-        if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+        if (__syncthreads_or(warp == 0 && !mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
         loaded = set;
       }
@@ -417,7 +423,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       }
 #pragma unroll
       for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
-      if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
+      if (__syncthreads_or(warp == 0 && !mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
@@ -443,29 +449,32 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
                        : nullptr;
     float dv[H];
-    if (mode != COL_HEAD) tmem_ld_all<H>(my_d, dv);
+    if (mode != COL_HEAD) {
+      tmem_ld_all<H>(my_d, dv);
+      if (slow) {                               // whole-tile branch: the fast tiles skip it
+#pragma unroll
+        for (int u = 0; u < H; u++) {
+          const int k = c0 + u;
+          dv[u] *= sin_;
+          tsum = fmaf(dv[u], dv[u], tsum);
+          if (EX || (qok && k < nth)) {
+            if (srow) srow[(size_t)2 * k * n1] = dv[u] * rsw[k];
+            if (zrow) zrow[(size_t)2 * k * n12] = dv[u] * rsw[k];
+          }
+        }
+      }
+    }
 #pragma unroll
     for (int u = 0; u < H; u += 4) {
       float v[4];
       if (mode != COL_HEAD) {
 #pragma unroll
-        for (int x = 0; x < 4; x++) v[x] = dv[u + x];
-#pragma unroll
         for (int x = 0; x < 4; x++) {
-          const int k = c0 + u + x;
-          float mine = v[x];
-          if (slow) {
-            mine *= sin_;
-            tsum = fmaf(mine, mine, tsum);
-            if (EX || (qok && k < nth)) {
-              if (srow) srow[(size_t)2 * k * n1] = mine * rsw[k];
-              if (zrow) zrow[(size_t)2 * k * n12] = mine * rsw[k];
-            }
-          }
+          v[x] = dv[u + x];
           if (mode == COL_MID) {
-            const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-            const float2 e = evs[k * TPTS + pt];
-            v[x] = fmaf(other * ysg, e.y, mine * e.x);
+            const float other = __shfl_xor_sync(0xffffffffu, v[x], 1);
+            const float2 e = evs[(c0 + u + x) * TPTS + pt];
+            v[x] = fmaf(other * ysg, e.y, v[x] * e.x);
           }
         }
       } else {
@@ -527,7 +536,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       mma_commit(mb2);
     }
     if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
-    if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
+    if (__syncthreads_or(warp == 0 && !mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
     float no_part = 0.f, ov[H];

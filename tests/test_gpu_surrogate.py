@@ -89,12 +89,16 @@ def test_surrogate_gains_over_the_plain_pes_routine():
     with Surrogate(seed=10) as sur:
         sur.fit(r12, r23, r13, V, steps=300, lr=3e-3, lr_end=1e-3)
         sur.potential(R, r, x, MASSES)                   # warm-up
+        t_mlp = 1e30
+        for _ in range(3):                               # best of three: shared host
+            t0 = time.perf_counter()
+            g = sur.potential(R, r, x, MASSES)
+            t_mlp = min(t_mlp, time.perf_counter() - t0)
+    t_plain = 1e30
+    for _ in range(3):
         t0 = time.perf_counter()
-        g = sur.potential(R, r, x, MASSES)
-        t_mlp = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    p = potential_jacobi(R, r, x, MASSES, pes)
-    t_plain = time.perf_counter() - t0
+        p = potential_jacobi(R, r, x, MASSES, pes)
+        t_plain = min(t_plain, time.perf_counter() - t0)
     assert g.shape == p.shape
     assert t_mlp * 3 < t_plain, (t_mlp, t_plain)
 
