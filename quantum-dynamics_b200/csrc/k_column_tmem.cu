@@ -148,6 +148,9 @@ struct TcDev {
   int *status;           // device status word (0 = ok)
   int renorm;            // per-column isometry rescaling on
   int nnorm;             // orders l < nnorm enter the GEMM2 output norm
+  // x / tiles-per-run and x / n1 as (x * m) >> 40, m = floor(2^40 / d) + 1:
+  // exact while x * d < 2^40 (checked at launch)
+  uint64_t m_tpr, m_n1;
 };
 
 
@@ -287,7 +290,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   const int tpr = (n12 + TPTS - 1) / TPTS;      // tiles per run
   const int ntiles = tpr * p.nruns;
   const int tbeg = blockIdx.x, tend = ntiles;
-#define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[(tl) / tpr] : (tl) / tpr)
+#define QD_DIV(x, m) ((int)(((uint64_t)(uint32_t)(x) * (m)) >> 40))
+#define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[QD_DIV(tl, t.m_tpr)] : QD_DIV(tl, t.m_tpr))
   const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
   // the B images of set `st` (4 * B_BYTES, a multiple of 16) by bulk
   // asynchronous copies from this GPU's global memory into this CTA's shared
@@ -329,12 +333,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #define QD_PREFETCH_A(tl)                                                            \
   do {                                                                               \
     const int rr = (tl) < tend ? QD_RUN_OF(tl) : 0;                                  \
-    const int qq = ((tl) - ((tl) / tpr) * tpr) * TPTS + pt;                          \
+    const int qq = ((tl) - QD_DIV(tl, t.m_tpr) * tpr) * TPTS + pt;                   \
     const bool ok = EX || ((tl) < tend && qq < n12);                                 \
     const float *src = lsrc + (size_t)rr * nl * stride + (size_t)c0 * stride + 2 * qq + comp; \
     _Pragma("unroll") for (int u = 0; u < H; u++) {                                  \
-      if (EX) a[u] = (tl) < tend ? __ldg(src + u * stride) : 0.f;                     \
-      else a[u] = (ok && c0 + u < nl) ? __ldg(src + u * stride) : 0.f;               \
+      if (EX) a[u] = (tl) < tend ? src[u * stride] : 0.f;                             \
+      else a[u] = (ok && c0 + u < nl) ? src[u * stride] : 0.f;                       \
     }                                                                                \
   } while (0)
   // exp(-i V dt) of tile tl into evs, 16-byte asynchronous copies (zero-filled
@@ -342,7 +346,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #define QD_STAGE_EV(tl)                                                              \
   do {                                                                               \
     if ((tl) < tend) {                                                               \
-      const int rr = QD_RUN_OF(tl), qb = ((tl) - ((tl) / tpr) * tpr) * TPTS;       \
+      const int rr = QD_RUN_OF(tl), qb = ((tl) - QD_DIV(tl, t.m_tpr) * tpr) * TPTS; \
       const float2 *eb = expv + (size_t)rr * p.vrun + qb;                            \
       for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
         const int k = x / (TPTS / 2), c2 = 2 * (x % (TPTS / 2));                     \
@@ -371,8 +375,9 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   const uint32_t my_d = D + lane_base + c0;
   const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
   uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
-  // one warp polls each mbarrier; the rest of the CTA sleeps in the barrier
-  bool failed = __syncthreads_or(warp == 0 && !mbar_wait(mb3, 0));
+  // every thread observes each mbarrier completion itself before it reads
+  // what the asynchronous operation wrote
+  bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
@@ -381,18 +386,18 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       const int set = t.run_set ? t.run_set[run] : 0;
       if (set != loaded) {                      // a run with another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
-        if (__syncthreads_or(warp == 0 && !mbar_wait(mb3, ph3))) { failed = true; break; }
+        if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
         loaded = set;
       }
       if (t.run_nl) nlr = t.run_nl[run];
     }
-    const int q0 = (tile - (tile / tpr) * tpr) * TPTS;
+    const int q0 = (tile - QD_DIV(tile, t.m_tpr) * tpr) * TPTS;
     const int q = q0 + pt;
     const bool qok = EX || q < n12;
     int j, i;
-    if (EX) { j = q0 / n1; i = q0 - j * n1 + pt; }
-    else { j = qok ? q / n1 : 0; i = qok ? q - (q / n1) * n1 : 0; }
+    if (EX) { j = QD_DIV(q0, t.m_n1); i = q0 - j * n1 + pt; }
+    else { j = qok ? QD_DIV(q, t.m_n1) : 0; i = qok ? q - j * n1 : 0; }
     const size_t voff = (size_t)run * p.vrun;
     const float ddv = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) : 1.f;
     const bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
@@ -423,7 +428,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       }
 #pragma unroll
       for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
-      if (__syncthreads_or(warp == 0 && !mbar_wait(mb1, ph1))) { failed = true; break; }
+      if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
@@ -536,7 +541,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       mma_commit(mb2);
     }
     if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
-    if (__syncthreads_or(warp == 0 && !mbar_wait(mb2, ph2))) { failed = true; break; }
+    if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
     float no_part = 0.f, ov[H];
@@ -565,6 +570,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #undef QD_STAGE_EV
 #undef QD_LOAD_IMAGES
 #undef QD_RUN_OF
+#undef QD_DIV
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
@@ -771,8 +777,14 @@ cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode
   t.status = tc_status_ptr(plan);
   t.renorm = plan.renorm;
   t.nnorm = plan.nth < plan.S ? plan.nth : plan.S;
-  const long ntiles = (p.n12 + TPTS - 1) / TPTS * p.nruns;   // tiles of all runs
+  const long tpr = (p.n12 + TPTS - 1) / TPTS;
+  const long ntiles = tpr * p.nruns;                          // tiles of all runs
   const int grid = (int)(ntiles < plan.grid ? ntiles : plan.grid);
+  if ((uint64_t)(ntiles + grid) * (uint64_t)tpr >= (1ull << 40) ||
+      (uint64_t)p.n12 * (uint64_t)p.n1 >= (1ull << 40))
+    return cudaErrorInvalidValue;                              // tile arithmetic range
+  t.m_tpr = (1ull << 40) / (uint64_t)tpr + 1;
+  t.m_n1 = (1ull << 40) / (uint64_t)p.n1 + 1;
   switch (plan.S) {
     case 16: launch_mode<16>(grid, plan.smem_bytes, s, p, t, mode); break;
     case 32: launch_mode<32>(grid, plan.smem_bytes, s, p, t, mode); break;

@@ -323,8 +323,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
                    smem_addr(R + tid * RS + HW * peer), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[0]), peer));
     }
-    if (tid < 32) ok = mbar_wait0(smem_addr(&mbar[0]));   // the peer's rows of this half are in
-    ok = __syncthreads_and(ok);                      // (one warp polls, the rest sleep here)
+    ok = mbar_wait0(smem_addr(&mbar[0]));            // the peer's rows of this half are in
   } else {
     __syncthreads();
   }
@@ -395,9 +394,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
                    smem_addr(P + tid * HW), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[1]), peer));
     }
-    bool ok2 = true;
-    if (tid < 32) ok2 = mbar_wait0(smem_addr(&mbar[1]));  // the other half of the own rows is back
-    ok = __syncthreads_and(ok2) && ok;
+    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other half of the own rows is back
     cluster_arrive_release();                        // this CTA's incoming copies are complete
     if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
   } else {
