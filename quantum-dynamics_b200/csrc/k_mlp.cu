@@ -280,15 +280,26 @@ struct GridArgs {
   double f2, f3, vmax, rmin;
   int cap;
 };
+// every layer's weights stay in shared memory for the whole launch (loaded
+// once per CTA), activations of 64 points at a time in place
+constexpr int WS = W + 1;                                  // padded weight / activation row
+constexpr size_t GRID_SMEM = sizeof(float) * ((size_t)NL * W * WS + 64 * WS + 64 * NF) + 64;
 __global__ void __launch_bounds__(256) k_mlp_grid(GridArgs g, Norm nm, const float *wq,
                                                   double *pot, long npts, const double *r12p,
                                                   const double *r23p, const double *r13p)
 {
-  __shared__ float Wsm[W][W + 1];
-  __shared__ float H[64][W + 1];          // activations, updated in place per layer
-  __shared__ float feat[64][NF];
-  __shared__ unsigned char mask[64];
+  extern __shared__ float4 grid_sm4[];
+  float *sm = reinterpret_cast<float *>(grid_sm4);
+  float (*Wsm)[W][WS] = reinterpret_cast<float (*)[W][WS]>(sm);            // [NL][W][WS]
+  float (*H)[WS] = reinterpret_cast<float (*)[WS]>(sm + NL * W * WS);      // [64][WS]
+  float (*feat)[NF] = reinterpret_cast<float (*)[NF]>(sm + NL * W * WS + 64 * WS);
+  unsigned char *mask = reinterpret_cast<unsigned char *>(sm + NL * W * WS + 64 * WS + 64 * NF);
   const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+  for (int l = 0; l < NL; l++) {
+    const int K = l == 0 ? NF : W;
+    const float *Wl = wq + layer_off(l);
+    for (int x = tid; x < W * K; x += 256) Wsm[l][x / K][x % K] = Wl[x];
+  }
   for (long base = (long)blockIdx.x * 64; base < npts; base += (long)gridDim.x * 64) {
     if (tid < 64) {
       const long q = base + tid;
@@ -313,12 +324,10 @@ __global__ void __launch_bounds__(256) k_mlp_grid(GridArgs g, Norm nm, const flo
       for (int c = 0; c < NF; c++) feat[tid][c] = f[c];
       mask[tid] = ok;
     }
-    __syncthreads();
+    __syncthreads();                      // features (and, first time, the weights) in place
     for (int l = 0; l < NL; l++) {
       const int K = l == 0 ? NF : W;
-      const float *Wl = wq + layer_off(l), *bl = Wl + W * K;
-      for (int x = tid; x < W * K; x += 256) Wsm[x / K][x % K] = Wl[x];
-      __syncthreads();
+      const float *bl = wq + layer_off(l) + W * K;
       float acc[4][4];
 #pragma unroll
       for (int i = 0; i < 4; i++)
@@ -329,13 +338,13 @@ __global__ void __launch_bounds__(256) k_mlp_grid(GridArgs g, Norm nm, const flo
 #pragma unroll
         for (int i = 0; i < 4; i++) a[i] = l == 0 ? feat[tr + 16 * i][k] : H[tr + 16 * i][k];
 #pragma unroll
-        for (int j = 0; j < 4; j++) w[j] = Wsm[tc + 16 * j][k];
+        for (int j = 0; j < 4; j++) w[j] = Wsm[l][tc + 16 * j][k];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
           for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], w[j], acc[i][j]);
       }
-      __syncthreads();                    // every read of H and Wsm is done
+      __syncthreads();                    // every read of H is done
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -359,6 +368,19 @@ __global__ void __launch_bounds__(256) k_mlp_grid(GridArgs g, Norm nm, const flo
     }
     __syncthreads();
   }
+}
+
+cudaError_t launch_mlp_grid(long blocks, const GridArgs &g, const Norm &nm, const float *wq,
+                            double *pot, long npts, const double *r12p, const double *r23p,
+                            const double *r13p)
+{
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      k_mlp_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GRID_SMEM);
+  if (attr != cudaSuccess) return attr;
+  k_mlp_grid<<<(unsigned)(blocks < 148 * 2 ? blocks : 148 * 2), 256, GRID_SMEM>>>(
+      g, nm, wq, pot, npts, r12p, r23p, r13p);
+  qd_count_launches(1);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -632,10 +654,7 @@ int qd_mlp_eval(qd_mlp *m, int64_t n, const double *r12, const double *r23, cons
   if (e == cudaSuccess) {
     GridArgs g{};
     const long blocks = (n + 63) / 64;
-    k_mlp_grid<<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), 256>>>(g, m->norm, m->d_wq,
-                                                                       d + 3 * n, n, d, d + n, d + 2 * n);
-    qd_count_launches(1);
-    e = cudaGetLastError();
+    e = launch_mlp_grid(blocks, g, m->norm, m->d_wq, d + 3 * n, n, d, d + n, d + 2 * n);
   }
   if (e == cudaSuccess) e = cudaMemcpy(V_out, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
   cudaFree(d);
@@ -666,10 +685,7 @@ int qd_mlp_potential(qd_mlp *m, const qd_radial *R, const qd_radial *r, const qd
   if (e == cudaSuccess) {
     g.R = dR; g.r = dr; g.x = dx;
     const long blocks = (n + 63) / 64;
-    k_mlp_grid<<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), 256>>>(g, m->norm, m->d_wq, d, n,
-                                                                       nullptr, nullptr, nullptr);
-    qd_count_launches(1);
-    e = cudaGetLastError();
+    e = launch_mlp_grid(blocks, g, m->norm, m->d_wq, d, n, nullptr, nullptr, nullptr);
   }
   if (e == cudaSuccess) e = cudaMemcpy(pot_out, d, sizeof(double) * n, cudaMemcpyDeviceToHost);
   cudaFree(d);

@@ -17,7 +17,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 #include "qd.h"
 #include "qd_kernels.h"
@@ -171,26 +174,51 @@ struct qd_handle {
   std::vector<int> prof_cls;
   size_t prof_used = 0;
 
+  // device buffers come from the device's stream-ordered memory pool, which
+  // keeps freed memory (release threshold raised once per process), so that
+  // creating a handle after an earlier one was destroyed reuses its memory
+  // instead of paying cudaMalloc / cudaFree again
   template <typename T> int alloc(T *&p, size_t count)
   {
     void *q = nullptr;
     const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
-    cudaError_t e = cudaMalloc(&q, bytes);
+    keep_pool();
+    cudaError_t e = cudaMallocAsync(&q, bytes, st);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      return set_err(QD_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes,
+      return set_err(QD_ERR_NOMEM, "cudaMallocAsync(%zu bytes) failed: %s", bytes,
                      cudaGetErrorString(e));
     }
     allocs.push_back(q);
     p = reinterpret_cast<T *>(q);
+    // pooled memory holds whatever its last user left: every buffer starts
+    // zeroed (unused orders of ragged runs, flux rows and rings rely on it)
+    e = cudaMemsetAsync(q, 0, bytes, st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(QD_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    }
     return QD_OK;
+  }
+  static bool keep_pool()
+  {
+    static const bool ok = [] {
+      int dev = 0;
+      cudaMemPool_t pool;
+      if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess)
+        return false;
+      uint64_t keep = ~0ull;
+      return cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
+    }();
+    return ok;
   }
   ~qd_handle()
   {
     if (st) cudaStreamSynchronize(st);
-    for (void *p : allocs) cudaFree(p);
-    if (d_norms) cudaFree(d_norms);
-    if (d_flush) cudaFree(d_flush);
+    for (void *p : allocs) cudaFreeAsync(p, st);
+    if (d_norms) cudaFreeAsync(d_norms, st);
+    if (d_flush) cudaFreeAsync(d_flush, st);
+    if (st) cudaStreamSynchronize(st);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
     for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
     tc_plan_destroy(tc);
@@ -408,8 +436,9 @@ LineParams line_params(qd_handle *h, bool f32)
 // Autotuner of the complex64 l-space pass: time the fused slice kernel with
 // 1, 2 and 4 CTAs per slice, the register-FFT slice kernel on 1 and 2 CTAs
 // per slice and the split kernels on a scratch wavepacket and keep the
-// fastest.  QD_SLICE_CLUSTER=0|1|2|4|8|9 forces a choice (8 = the
-// register-FFT kernel, 9 = the same on a 2-CTA cluster).
+// fastest; the choice is kept for later handles of the same shapes.
+// QD_SLICE_CLUSTER=0|1|2|4|8|9 forces a choice (8 = the register-FFT kernel,
+// 9 = the same on a 2-CTA cluster).
 int tune_slice(qd_handle *h)
 {
   h->slice_cluster = 0;
@@ -420,9 +449,24 @@ int tune_slice(qd_handle *h)
     h->slice_cluster = slice_cluster_ok(h->n1, h->n2, cl) ? cl : 0;
     return QD_OK;
   }
+  // the choice depends on the shapes only: measured once per process and device
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, int, int, int>, int> chosen;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, h->n1, h->n2, h->nl, h->nruns, h->jrows,
+                                   h->d_run_k ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = chosen.find(key);
+    if (it != chosen.end()) {
+      h->slice_cluster = it->second;
+      return QD_OK;
+    }
+  }
   void *scratch = nullptr;
   const size_t sbytes = sizeof(float2) * h->n12 * h->nl * h->nruns;
-  CU(cudaMalloc(&scratch, sbytes));
+  CU(cudaMallocAsync(&scratch, sbytes, h->st));
   CU(cudaMemsetAsync(scratch, 0, sbytes, h->st));
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
@@ -451,7 +495,9 @@ int tune_slice(qd_handle *h)
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  CU(cudaFree(scratch));
+  CU(cudaFreeAsync(scratch, h->st));
+  std::lock_guard<std::mutex> lock(mu);
+  chosen[key] = h->slice_cluster;
   return QD_OK;
 }
 
@@ -527,17 +573,17 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
       h->events.push_back(e);
     }
     if (flush_bytes > h->flush_bytes) {
-      if (h->d_flush) cudaFree(h->d_flush);
+      if (h->d_flush) cudaFreeAsync(h->d_flush, h->st);
       h->d_flush = nullptr;
-      CU(cudaMalloc(&h->d_flush, flush_bytes));
+      CU(cudaMallocAsync(&h->d_flush, flush_bytes, h->st));
       h->flush_bytes = flush_bytes;
     }
   }
   const int R = h->nruns;                         // norms: [step][run]
   if (h->norms_cap < n * R) {
-    if (h->d_norms) cudaFree(h->d_norms);
+    if (h->d_norms) cudaFreeAsync(h->d_norms, h->st);
     h->d_norms = nullptr;
-    CU(cudaMalloc(&h->d_norms, sizeof(double) * n * R));
+    CU(cudaMallocAsync(&h->d_norms, sizeof(double) * n * R, h->st));
     h->norms_cap = n * R;
   }
   CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n * R, h->st));
