@@ -355,19 +355,32 @@ def run_ours(args):
     nl, nth = int(r0.theta.m) + 1, int(r0.theta.n)
     n12 = int(r0.r1.n) * int(r0.r2.n) * len(runs)
     cb = 16 if args.fp64 else 8        # bytes per complex
-    alg = {  # algorithmic bytes per launch group
-        "column": n12 * (2 * nl * cb + nth * (16 if args.fp64 else 4)),
+    shared_pot = all(np.array_equal(r.pot, r0.pot) for r in runs[1:])
+    npot = 1 if shared_pot else len(runs)
+    alg = {  # algorithmic bytes per launch: psi_l read + written, exp(-iV dt) read once
+        "column": n12 * 2 * nl * cb + int(r0.r1.n) * int(r0.r2.n) * nth * cb * npot,
         "lines": n12 * nl * 2 * cb,
     }
+    # DRAM bytes (read + write) per launch from one ncu capture each (cold caches:
+    # ncu flushes them before every captured launch); the batch figures were
+    # captured on 32 runs and scale with the runs.  Sources: the ncu summaries
+    # column_tc_and_slice_rf2_c1_128x128x64.md and
+    # column_tc_and_slice_rf_batch32_128x96x64.md under profiles/.
+    traffic_ncu = {("c1", "column"): 16.89e6, ("c1", "lines"): 9.30e6,
+                   ("c2j0", "column"): 373.7e6 / 32, ("c2j0", "lines"): 379.7e6 / 32}
     names = ["column", "lines", "flux_prep", "flux_accum", "crp"]
     per = {names[i]: kclass[i] for i in range(min(5, len(kclass)))}
     step_ms = t_max / K
     dom = max(("column", "lines"), key=lambda k: per.get(k, 0.0))
     dom_ms = per.get(dom, float("nan"))
     achieved = alg[dom] / (dom_ms * 1e-3) / 1e9 if dom_ms and dom_ms > 0 else None
+    tr = traffic_ncu.get((args.workload, dom)) if not args.fp64 else None
+    if tr is not None and args.workload == "c2j0":
+        tr *= len(runs)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": None,
+                "frac": achieved / peak if achieved else None,
+                "traffic": tr, "traffic_unit": "bytes per launch (ncu)",
                 "alg_bytes_per_launch": alg[dom], "avg_launch_ms": dom_ms,
                 "kernel_class_ms": per}
 
