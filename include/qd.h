@@ -365,6 +365,34 @@ int qd_potential_leps(const qd_radial *R, const qd_radial *r, const qd_angle *th
                       const double masses[3], const qd_leps *leps, double vmax, double rmin,
                       int32_t cap, double *pot_out);
 
+/* The HSW surface of F + H2 (FH2/HSW/hswpot.F:1-99 with sospline.F; replaces
+ * the PES MEX FH2/HSW/HSWMex.C:29-90 and its Fortran): the SW1 fit plus the
+ * spline-interpolated spin-orbit correction, evaluated on the GPU in FP64.
+ * qd_hsw_create reads the reference's own data files three.param, two.param,
+ * so.input and so.param from dir (the HSW_DATA_DIR of HSWMex.C:48-56) and
+ * builds the spline once on the host; qd_hsw_create_from_tables takes the
+ * same numbers as arrays: the three.param records (n3 of them; the last six
+ * are b1 b2 b3 x0 y0 z0 in a[]), the 12 two.param values, the so.input grid
+ * (nodes x[nx], y[ny], z[nz], values so[i][j][k] in file order, k fastest)
+ * and the three so.param values (kcal/mol, bohr, bohr). */
+typedef struct qd_hsw qd_hsw;
+int qd_hsw_create(const char *dir, qd_hsw **out);
+int qd_hsw_create_from_tables(int32_t n3, const int32_t *ix, const int32_t *iy,
+                              const int32_t *iz, const double *a, const double p[12],
+                              int32_t nx, int32_t ny, int32_t nz, const double *x,
+                              const double *y, const double *z, const double *so,
+                              const double so_param[3], qd_hsw **out);
+int qd_hsw_destroy(qd_hsw *h);
+/* V (hartree) at n points given as internuclear distances in bohr, in the
+ * argument order of pot() (hswpot.F:1): r(F-H1), r(H1-H2), r(F-H2). */
+int qd_hsw_eval(const qd_hsw *h, int64_t n, const double *r_fh1, const double *r_hh,
+                const double *r_fh2, double *v_out);
+/* The surface on the Jacobi grid, with the mapping, masking and cap of
+ * qd_potential_jacobi (atom 1 = F: r12 = r(F-H1), r23 = r(H1-H2), r13 = r(F-H2)). */
+int qd_potential_hsw(const qd_radial *R, const qd_radial *r, const qd_angle *theta,
+                     const double masses[3], const qd_hsw *h, double vmax, double rmin,
+                     int32_t cap, double *pot_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,6 +7,7 @@ import ctypes as C
 import os
 
 c_double_p = C.POINTER(C.c_double)
+c_int32_p = C.POINTER(C.c_int32)
 c_float_p = C.POINTER(C.c_float)
 
 QD_OK = 0
@@ -228,6 +229,16 @@ def lib():
         "qd_potential_leps": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
                                         P(QdLeps), C.c_double, C.c_double, C.c_int32,
                                         c_double_p]),
+        "qd_hsw_create": (C.c_int, [C.c_char_p, P(H)]),
+        "qd_hsw_create_from_tables": (C.c_int, [C.c_int32, c_int32_p, c_int32_p, c_int32_p,
+                                                c_double_p, c_double_p, C.c_int32, C.c_int32,
+                                                C.c_int32, c_double_p, c_double_p, c_double_p,
+                                                c_double_p, c_double_p, P(H)]),
+        "qd_hsw_destroy": (C.c_int, [H]),
+        "qd_hsw_eval": (C.c_int, [H, C.c_int64, c_double_p, c_double_p, c_double_p,
+                                  c_double_p]),
+        "qd_potential_hsw": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p, H,
+                                       C.c_double, C.c_double, C.c_int32, c_double_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

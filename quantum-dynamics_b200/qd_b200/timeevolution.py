@@ -13,6 +13,7 @@ they propagate them as one batch (same grid; see qd_create_batch).
 handle API).
 """
 import ctypes as C
+import os
 import numpy as np
 
 from . import _abi
@@ -227,6 +228,74 @@ def potential_leps_gpu(R, r, x, masses, pes, vmax=2.5, rmin=0.4, cap=True):
                                   m.ctypes.data_as(_abi.c_double_p), C.byref(p), vmax, rmin,
                                   1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
     return out
+
+
+class HswSurface:
+    """The HSW surface of F + H2 on the GPU (qd_hsw_*; the reference's
+    FH2/HSW/hswpot.F + sospline.F behind HSWMex.C).  Build it from the
+    reference's data directory (`HswSurface(dir)`, the HSW_DATA_DIR of
+    HSWMex.C) or from the file contents as arrays (`HswSurface(tables=...)`
+    with keys ix, iy, iz, a, p, x, y, z, so, so_param)."""
+
+    def __init__(self, data_dir=None, tables=None):
+        self._h = C.c_void_p()
+        if tables is None:
+            if data_dir is None:
+                raise ValueError("need a data directory or tables")
+            check(lib().qd_hsw_create(os.fsencode(data_dir), C.byref(self._h)))
+            return
+        t = {k: np.asarray(v) for k, v in tables.items()}
+        ix, iy, iz = (np.ascontiguousarray(t[k], dtype=np.int32) for k in ("ix", "iy", "iz"))
+        a = np.ascontiguousarray(t["a"], dtype=np.float64)
+        pp = np.ascontiguousarray(t["p"], dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(t[k], dtype=np.float64) for k in ("x", "y", "z"))
+        so = np.ascontiguousarray(t["so"], dtype=np.float64)
+        sp = np.ascontiguousarray(t["so_param"], dtype=np.float64)
+        if so.shape != (x.size, y.size, z.size) or pp.size < 12 or sp.size < 3:
+            raise ValueError("inconsistent HSW tables")
+        i32 = _abi.c_int32_p
+        check(lib().qd_hsw_create_from_tables(
+            a.size, ix.ctypes.data_as(i32), iy.ctypes.data_as(i32), iz.ctypes.data_as(i32),
+            _abi._ptr(a), _abi._ptr(pp), x.size, y.size, z.size, _abi._ptr(x), _abi._ptr(y),
+            _abi._ptr(z), _abi._ptr(so), _abi._ptr(sp), C.byref(self._h)))
+
+    def __call__(self, r_fh1, r_hh, r_fh2):
+        """V (hartree) at internuclear distances (bohr), the argument order of
+        the reference's pot(): r(F-H1), r(H1-H2), r(F-H2)."""
+        a, b, c = np.broadcast_arrays(*(np.asarray(v, dtype=np.float64) for v in (r_fh1, r_hh, r_fh2)))
+        a, b, c = (np.ascontiguousarray(v).ravel() for v in (a, b, c))
+        out = np.empty(a.size)
+        check(lib().qd_hsw_eval(self._h, a.size, _abi._ptr(a), _abi._ptr(b), _abi._ptr(c),
+                                _abi._ptr(out)))
+        return out.reshape(np.shape(np.broadcast_arrays(r_fh1, r_hh, r_fh2)[0]))
+
+    def potential(self, R, r, x, masses, vmax=2.5, rmin=0.4, cap=True):
+        """The surface on the Jacobi grid (shape (n_theta, n_r, n_R)), the
+        mapping and masking of potential_jacobi (atom 1 = F)."""
+        (ga, gb, gt), keep = _grid_structs(R, r, x)
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        out = np.empty((gt.n, gb.n, ga.n))
+        check(lib().qd_potential_hsw(C.byref(ga), C.byref(gb), C.byref(gt),
+                                     m.ctypes.data_as(_abi.c_double_p), self._h, vmax, rmin,
+                                     1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().qd_hsw_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _radial(c):
