@@ -1,7 +1,7 @@
 """Benchmark: grid-point * steps / s of the split-operator propagator.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0|c2|c2j0|c3]
+                    [--workload c1|c0|c2|c2j0|c3|c4]
 
 Workload (default c1): F + H2, J = 0, extended-LEPS surface on a
 128 x 128 x 64 Jacobi grid (n_l = 64), complex64 wavefunction with the
@@ -138,6 +138,12 @@ def build_workload(name, precision, runs=64):
         desc = (f"batch of {runs} F+H2 centrifugal-sudden blocks (J in 0,5,10,15,20; "
                 "K <= min(J,4); n_j = 64 - K) x initial (v0,j0) in (0,0),(0,1),(0,2),(1,0), "
                 "128x96x64 Jacobi grid, dt=10 au, 241 energies each")
+    elif name == "c4":
+        data = S.case_c4(min(runs, 32), precision=precision)
+        desc = (f"batch of {min(runs, 32)} F+H2 centrifugal-sudden blocks (J in 0,4,..,28 with "
+                "K <= min(J,3), then J=30 with K <= 2; n_j = 128 - K) from (v0,j0) = (0,3), "
+                "256x192x128 Jacobi grid, dt=10 au, 241 energies each; extended-LEPS surface "
+                "(the surface does not enter the step's arithmetic)")
     elif name == "c2j0":
         data = S.case_c2_j0(runs, precision=precision)
         desc = (f"batch of {runs} F+H2 J=0 propagations, 128x96x64 Jacobi grid, n_l=64, dt=10 au, "
@@ -414,7 +420,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c2j0", "c3"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c2j0", "c3", "c4"])
     ap.add_argument("--runs", type=int, default=64, help="runs of the c2j0 batch")
     ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")

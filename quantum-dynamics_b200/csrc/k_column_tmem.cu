@@ -18,9 +18,14 @@
 // a quarter of its columns), the constant B images in shared memory (K-major,
 // 128-byte swizzle, built once on the host), the accumulator in TMEM.  The
 // tile's exp(-i V dt) values are staged into shared memory by asynchronous
-// copies issued while the previous tile finishes.  512 threads per CTA, two
-// CTAs per SM overlap each other's load / MMA / epilogue phases.  TMEM per
-// CTA: [Ahi | Alo | D], S columns each.
+// copies issued while the previous tile finishes.  512 threads per CTA.  TMEM
+// per CTA: [Ahi | Alo | D], S columns each.  S <= 64: two CTAs per SM overlap
+// each other's load / MMA / epilogue phases.  S = 96, 128 (n_theta up to 128):
+// one CTA per SM (512 TMEM columns); at S = 128 the four operand images
+// (256 KB) do not fit in shared memory together, so the CTA keeps one GEMM's
+// pair: B2 is copied over B1 as soon as GEMM1 has completed, and the next
+// tile's B1 over B2 as soon as GEMM2 has, each copy overlapping the work
+// between the two GEMMs or after them.
 //
 // Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
 // smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
@@ -50,11 +55,15 @@ namespace {
 constexpr int TPTS = 64;          // complex grid points per tile
 constexpr int MROWS = 128;        // GEMM rows per tile
 constexpr int NTHREADS = 512;
-constexpr int MAXS = 64;          // max padded n_l / n_theta handled here
-constexpr uint32_t TMEM_COLS = 256;
+constexpr int MAXS = 128;         // max padded n_l / n_theta handled here
+// per-size resources: TMEM columns (Ahi | Alo | D, S each, rounded up to a
+// power of two), CTAs per SM, and whether both GEMMs' operand images stay in
+// shared memory (else the CTA streams B1 and B2 in turn through one buffer)
+__host__ __device__ constexpr uint32_t tmem_cols(int S) { return 3 * S <= 256 ? 256u : 512u; }
+__host__ __device__ constexpr int ctas_per_sm(int S) { return 3 * S <= 256 ? 2 : 1; }
+__host__ __device__ constexpr bool stream_images(int S) { return S > 96; }
 constexpr long WAIT_LIMIT = 1L << 22;   // mbarrier polls before giving up
 
-__host__ __device__ constexpr int pad16(int x) { return (x + 15) & ~15; }
 
 // byte offset of element (r, k) in a K-major SW128 operand of R rows
 __host__ __device__ __forceinline__ uint32_t sw128_off(int r, int k, int R)
@@ -154,15 +163,7 @@ struct TcDev {
 };
 
 
-// tcgen05.ld / tcgen05.st of 4 consecutive 32-bit columns of this thread's lane
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float &a, float &b, float &c, float &d)
-{
-  uint32_t r0, r1, r2, r3;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-  a = __uint_as_float(r0); b = __uint_as_float(r1); c = __uint_as_float(r2); d = __uint_as_float(r3);
-}
+// tcgen05.st of 4 consecutive 32-bit columns of this thread's lane
 __device__ __forceinline__ void tmem_st4(uint32_t taddr, float a, float b, float c, float d)
 {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
@@ -249,19 +250,21 @@ constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share
 // dd sqrt(n_l / n_out) at the store does both.
 // MS: runs of the batch have different angular bases (image sets, orders stored)
 template <int S, int MODE, bool EX, bool MS>
-__global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev t)
+__global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnParams p, TcDev t)
 {
   constexpr int mode = MODE;
   constexpr int H = S / NG;                    // K columns per thread (one group)
   constexpr int NKA = (S + 31) / 32;           // 128-byte swizzle atoms along K
   constexpr int B_BYTES = NKA * S * 128;
+  constexpr bool STREAM = stream_images(S);    // B1 and B2 take turns in one buffer
+  constexpr uint32_t TMEM_COLS = tmem_cols(S);
   static_assert(H % 4 == 0, "column group must be a multiple of 4");
   extern __shared__ unsigned char smem_raw[];
   const uint32_t base_u = smem_u32(smem_raw);
   unsigned char *base = smem_raw + ((1024u - (base_u & 1023u)) & 1023u);
   unsigned char *B1 = base;                     // hi | lo
-  unsigned char *B2 = B1 + 2 * B_BYTES;
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(B2 + 2 * B_BYTES);
+  unsigned char *B2 = STREAM ? base : B1 + 2 * B_BYTES;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(base + (STREAM ? 2 : 4) * B_BYTES);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *sw = xch + 4 * NG * TPTS;                        // [S] sqrt(w_k), 0 beyond n_theta
@@ -293,15 +296,17 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #define QD_DIV(x, m) ((int)(((uint64_t)(uint32_t)(x) * (m)) >> 40))
 #define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[QD_DIV(tl, t.m_tpr)] : QD_DIV(tl, t.m_tpr))
   const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
-  // the B images of set `st` (4 * B_BYTES, a multiple of 16) by bulk
-  // asynchronous copies from this GPU's global memory into this CTA's shared
-  // memory, completing on mbar[3]
-#define QD_LOAD_IMAGES(st)                                                             \
+  // images [first, first + count) of set `st` (B1 hi, B1 lo, B2 hi, B2 lo,
+  // B_BYTES each, multiples of 16) by bulk asynchronous copies from this
+  // GPU's global memory into this CTA's shared memory at B1, completing on
+  // mbar[3]
+#define QD_LOAD_B(st, first, count)                                                    \
   do {                                                                                 \
-    constexpr uint32_t total = 4 * B_BYTES, chunk = 16384;                             \
+    const uint32_t total = (count) * B_BYTES, chunk = 16384;                           \
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"              \
                  :: "r"(mb3), "r"(total) : "memory");                                  \
-    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes; \
+    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes + \
+                      (size_t)(first) * B_BYTES;                                       \
     for (uint32_t off = 0; off < total; off += chunk) {                                \
       const uint32_t n = total - off < chunk ? total - off : chunk;                    \
       asm volatile(                                                                    \
@@ -309,7 +314,16 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
           :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
     }                                                                                  \
   } while (0)
-  int loaded = MS && tbeg < tend && t.run_set ? t.run_set[QD_RUN_OF(tbeg)] : 0;   // image set in smem
+  // the images one launch of this mode needs resident: all four, or with
+  // STREAM the pair of the mode's single GEMM (B2 for HEAD) or B1 to start MID
+#define QD_LOAD_IMAGES(st)                                                             \
+  do {                                                                                 \
+    if (!STREAM) QD_LOAD_B(st, 0, 4);                                                  \
+    else QD_LOAD_B(st, mode == COL_HEAD ? 2 : 0, 2);                                   \
+  } while (0)
+#define QD_SET_OF(tl) (MS && t.run_set ? t.run_set[QD_RUN_OF(tl)] : 0)
+  int loaded = tbeg < tend ? QD_SET_OF(tbeg) : 0;   // image set in smem
+  bool img_pending = false;                     // a streamed image copy not yet waited on
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
@@ -382,9 +396,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
     int nlr = nl;                               // orders stored for this run
+    if (STREAM && mode == COL_MID && img_pending) {   // B1 of this tile, issued last tile
+      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+      ph3 ^= 1;
+      img_pending = false;
+    }
     if constexpr (MS) {
       const int set = t.run_set ? t.run_set[run] : 0;
-      if (set != loaded) {                      // a run with another angular basis
+      if (!(STREAM && mode == COL_MID) && set != loaded) {   // a run with another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
         if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
@@ -431,6 +450,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
+      if (STREAM && mode == COL_MID) {          // B1 is free: B2 of this tile's set in its place
+        if (tid == 0) QD_LOAD_B(QD_SET_OF(tile), 2, 2);
+        img_pending = true;
+      }
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
         float nt_part = 0.f, dv[H];
         tmem_ld_all<H>(my_d, dv);
@@ -535,6 +558,11 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
+    if (STREAM && mode == COL_MID) {            // B2 in place
+      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+      ph3 ^= 1;
+      img_pending = false;
+    }
     if (tid == 0) {
       tc_fence_after();
       gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
@@ -544,6 +572,10 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
+    if (STREAM && mode == COL_MID && tile + (int)gridDim.x < tend) {   // B1 of the next tile
+      if (tid == 0) QD_LOAD_B(QD_SET_OF(tile + (int)gridDim.x), 0, 2);
+      img_pending = true;
+    }
     float no_part = 0.f, ov[H];
     tmem_ld_all<H>(my_d, ov);
 #pragma unroll
@@ -569,11 +601,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_column_tc(ColumnParams p, TcDev
 #undef QD_PREFETCH_A
 #undef QD_STAGE_EV
 #undef QD_LOAD_IMAGES
+#undef QD_LOAD_B
+#undef QD_SET_OF
 #undef QD_RUN_OF
 #undef QD_DIV
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
+  if (STREAM && img_pending) mbar_wait(mb3, ph3);        // (bounded; after a failed wait)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -641,8 +676,19 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 
 template <int S> constexpr int smem_bytes_for()
 {
-  return 1024 + 4 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
+  return 1024 + (stream_images(S) ? 2 : 4) * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 +
+         4 * NG * TPTS * 4 + 2 * S * 4 +
          S * TPTS * 8;   // B images, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
+}
+static_assert(smem_bytes_for<128>() <= 227 * 1024 && smem_bytes_for<96>() <= 227 * 1024,
+              "shared memory of the largest column tiles");
+
+// the kernel sizes built: S is n_l / n_theta padded up to one of them
+int kernel_size(int n)
+{
+  for (int s : {16, 32, 48, 64, 96, 128})
+    if (n <= s) return s;
+  return 0;
 }
 
 }  // namespace
@@ -650,8 +696,8 @@ template <int S> constexpr int smem_bytes_for()
 int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const *leg,
                    const int *nl_set, const double *w, cudaStream_t s)
 {
-  const int S = pad16(nl > nth ? nl : nth);
-  if (S > MAXS) return QD_ERR_UNSUPPORTED;
+  const int S = kernel_size(nl > nth ? nl : nth);
+  if (S == 0 || S > MAXS) return QD_ERR_UNSUPPORTED;
   // Q[k][l] = sqrt(w_k) sqrt(l+1/2) L[l][k] per angular set; the transform pair
   // is an isometry per grid column when Q has orthonormal columns, and GEMM2
   // then also forms an orthonormal completion of them (modified Gram-Schmidt
@@ -733,7 +779,7 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  plan.grid = 2 * sms;             // two CTAs per SM (shared memory and TMEM allow it)
+  plan.grid = ctas_per_sm(S) * sms;   // two CTAs per SM where shared memory and TMEM allow
   cudaError_t e = cudaSuccess;
   switch (S) {
     case 16: plan.smem_bytes = smem_bytes_for<16>();
@@ -742,6 +788,10 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
       e = set_smem_attr<32>(plan.smem_bytes); break;
     case 48: plan.smem_bytes = smem_bytes_for<48>();
       e = set_smem_attr<48>(plan.smem_bytes); break;
+    case 96: plan.smem_bytes = smem_bytes_for<96>();
+      e = set_smem_attr<96>(plan.smem_bytes); break;
+    case 128: plan.smem_bytes = smem_bytes_for<128>();
+      e = set_smem_attr<128>(plan.smem_bytes); break;
     default: plan.smem_bytes = smem_bytes_for<64>();
       e = set_smem_attr<64>(plan.smem_bytes); break;
   }
@@ -789,6 +839,8 @@ cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode
     case 16: launch_mode<16>(grid, plan.smem_bytes, s, p, t, mode); break;
     case 32: launch_mode<32>(grid, plan.smem_bytes, s, p, t, mode); break;
     case 48: launch_mode<48>(grid, plan.smem_bytes, s, p, t, mode); break;
+    case 96: launch_mode<96>(grid, plan.smem_bytes, s, p, t, mode); break;
+    case 128: launch_mode<128>(grid, plan.smem_bytes, s, p, t, mode); break;
     default: launch_mode<64>(grid, plan.smem_bytes, s, p, t, mode); break;
   }
   return cudaGetLastError();

@@ -440,6 +440,19 @@ def case_c2(n_runs=64, **kw):
     return [cs_case(base, *c) for c in combos[:n_runs]]
 
 
+def case_c4(n_runs=32, **kw):
+    """The large batched F + H2 configuration on the 256 x 192 x 128 grid
+    (j_max 127): centrifugal-sudden blocks J in (0, 4, ..., 28) with
+    K = 0 .. min(J, 3), then J = 30 with K = 0 .. 2 (32 blocks, J = 0-30,
+    K <= 3, n_j = 128 - K), all from the initial state (v0, j0) = (0, 3) so
+    that every block carries a packet; the first n_runs of them."""
+    kw.setdefault("total_steps", 20000)
+    base = build_case("f+h2", 256, 192, 128, m=127, r=(0.4, 8.0), **kw)
+    combos = [(J, K) for J in range(0, 29, 4) for K in range(min(J, 3) + 1)]
+    combos += [(30, K) for K in range(3)]
+    return [cs_case(base, J, K, 0, 3) for J, K in combos[:n_runs]]
+
+
 def copy_case(data):
     """Deep copy of the arrays that a propagation mutates (psi, CRP, time)."""
     import copy

@@ -166,6 +166,47 @@ def test_fp32_c0_grid_against_oracle(path, monkeypatch):
     assert rel(b.psi, a.psi) < 1e-4
 
 
+@pytest.mark.parametrize("shape", [(32, 24, 128, 127), (24, 20, 80, 79), (32, 24, 128, 100)])
+def test_fp32_large_angular_bases_against_fp64(shape):
+    # n_theta up to 128: the tensor-core column pass with one CTA per SM (S = 96,
+    # 128), at S = 128 with B1 and B2 streamed through one shared-memory buffer;
+    # n_l < n_theta runs the orthonormal completion of GEMM2
+    n1, n2, nth, m = shape
+    base = S.build_case("f+h2", n1, n2, nth, m=m, total_steps=40, n_energies=9,
+                        n_gradient_points=5, r=(0.5, 9.0))
+    got = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        d = S.copy_case(base)
+        d.options.precision = prec
+        with Propagator(d) as p:
+            p.propagate(40)
+            got[prec] = (p.psi(), p.crp(), p.norms(40))
+    a, b = got[QD_PREC_FP64], got[QD_PREC_FP32]
+    assert rel(b[0], a[0]) < 1e-4
+    assert np.abs(b[1] - a[1]).max() < FP32_CRP_ABS
+    assert np.abs(b[2] - a[2]).max() < 1e-4 * np.abs(a[2]).max()
+
+
+def test_fp32_large_cs_batch_against_fp64():
+    # centrifugal-sudden blocks of uneven n_j on n_theta = 128 in one batch: the
+    # streamed operand images follow each tile's angular set
+    base = _cs_base(24, 20, 128, steps=30)
+    combos = [(0, 0, 0, 2), (4, 1, 0, 2), (4, 2, 0, 2), (8, 3, 0, 3)]
+    runs = [S.cs_case(base, *c) for c in combos]
+    got = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        rs = [S.copy_case(r) for r in runs]
+        for r in rs:
+            r.options.precision = prec
+        with Propagator(rs) as p:
+            p.propagate(30)
+            got[prec] = [(p.psi(i), p.crp(i)) for i in range(len(rs))]
+    for (psi64, crp64), (psi32, crp32) in zip(got[QD_PREC_FP64], got[QD_PREC_FP32]):
+        if np.abs(psi64).max() > 0:
+            assert rel(psi32, psi64) < 1e-4
+        assert np.abs(crp32 - crp64).max() < FP32_CRP_ABS
+
+
 def test_fp32_tensor_core_and_simt_agree(monkeypatch):
     base = S.build_case("f+h2", 128, 96, 64, m=63, total_steps=20, n_energies=9,
                         n_gradient_points=7, r=(0.5, 9.0))
