@@ -365,6 +365,20 @@ int qd_potential_leps(const qd_radial *R, const qd_radial *r, const qd_angle *th
                       const double masses[3], const qd_leps *leps, double vmax, double rmin,
                       int32_t cap, double *pot_out);
 
+/* The BKMP2 surface of H3 (H3/bkmp2.F, Boothroyd-Keogh-Martin-Peterson
+ * 1996, the parameter set of that file; replaces the PES MEX
+ * H3/BKMP2Mex.C:16-60), evaluated on the GPU in FP64.  qd_bkmp2_eval gives
+ * the MEX value (hartree) at n geometries of internuclear distances (bohr);
+ * NaN where the reference stops on an impossible triangle or a distance
+ * below 0.2 bohr.  qd_potential_bkmp2 fills the Jacobi grid (mapping, mask
+ * and cap of qd_potential_jacobi; rmin >= 0.2) with the value minus
+ * vH2Min = -0.174495770896975, as H3/H3PESBKMP2.m:23-27 does. */
+int qd_bkmp2_eval(int64_t n, const double *r1, const double *r2, const double *r3,
+                  double *v_out);
+int qd_potential_bkmp2(const qd_radial *R, const qd_radial *r, const qd_angle *theta,
+                       const double masses[3], double vmax, double rmin, int32_t cap,
+                       double *pot_out);
+
 /* The HSW surface of F + H2 (FH2/HSW/hswpot.F:1-99 with sospline.F; replaces
  * the PES MEX FH2/HSW/HSWMex.C:29-90 and its Fortran): the SW1 fit plus the
  * spline-interpolated spin-orbit correction, evaluated on the GPU in FP64.

@@ -229,6 +229,10 @@ def lib():
         "qd_potential_leps": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
                                         P(QdLeps), C.c_double, C.c_double, C.c_int32,
                                         c_double_p]),
+        "qd_bkmp2_eval": (C.c_int, [C.c_int64, c_double_p, c_double_p, c_double_p,
+                                    c_double_p]),
+        "qd_potential_bkmp2": (C.c_int, [P(QdRadial), P(QdRadial), P(QdAngle), c_double_p,
+                                         C.c_double, C.c_double, C.c_int32, c_double_p]),
         "qd_hsw_create": (C.c_int, [C.c_char_p, P(H)]),
         "qd_hsw_create_from_tables": (C.c_int, [C.c_int32, c_int32_p, c_int32_p, c_int32_p,
                                                 c_double_p, c_double_p, C.c_int32, C.c_int32,

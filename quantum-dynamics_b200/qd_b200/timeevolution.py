@@ -230,6 +230,29 @@ def potential_leps_gpu(R, r, x, masses, pes, vmax=2.5, rmin=0.4, cap=True):
     return out
 
 
+def bkmp2_gpu(r1, r2, r3):
+    """The BKMP2 H3 surface (qd_bkmp2_eval, the MEX value of
+    H3/BKMP2Mex.C in hartree) at internuclear distances in bohr."""
+    a, b, c = np.broadcast_arrays(*(np.asarray(v, dtype=np.float64) for v in (r1, r2, r3)))
+    shape = a.shape
+    a, b, c = (np.ascontiguousarray(v).ravel() for v in (a, b, c))
+    out = np.empty(a.size)
+    check(lib().qd_bkmp2_eval(a.size, _abi._ptr(a), _abi._ptr(b), _abi._ptr(c), _abi._ptr(out)))
+    return out.reshape(shape)
+
+
+def potential_bkmp2_gpu(R, r, x, masses, vmax=2.5, rmin=0.4, cap=True):
+    """BKMP2 on the Jacobi grid (shape (n_theta, n_r, n_R)), shifted by
+    -vH2Min as H3/H3PESBKMP2.m does (qd_potential_bkmp2)."""
+    (ga, gb, gt), keep = _grid_structs(R, r, x)
+    m = np.ascontiguousarray(masses, dtype=np.float64)
+    out = np.empty((gt.n, gb.n, ga.n))
+    check(lib().qd_potential_bkmp2(C.byref(ga), C.byref(gb), C.byref(gt),
+                                   m.ctypes.data_as(_abi.c_double_p), vmax, rmin,
+                                   1 if cap else 0, out.ctypes.data_as(_abi.c_double_p)))
+    return out
+
+
 class HswSurface:
     """The HSW surface of F + H2 on the GPU (qd_hsw_*; the reference's
     FH2/HSW/hswpot.F + sospline.F behind HSWMex.C).  Build it from the
