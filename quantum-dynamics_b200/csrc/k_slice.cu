@@ -398,7 +398,7 @@ template <int CL> cudaError_t launch_cl(const LineParams &p, cudaStream_t s)
 
 int slice_cluster_ok(int n1, int n2, int cl)
 {
-  if (cl == SLICE_RF || cl == SLICE_RF2) return slice_rf_threads(n1, n2, slice_ctas(cl)) > 0;
+  if (slice_is_rf(cl)) return slice_rf_threads(n1, n2, slice_ctas(cl)) > 0;
   if (cl != 1 && cl != 2 && cl != 4) return 0;
   if (n1 % cl || n2 % cl) return 0;
   return slice_smem_bytes(n1, n2, cl) <= 227 * 1024 ? 1 : 0;
@@ -406,7 +406,7 @@ int slice_cluster_ok(int n1, int n2, int cl)
 
 int slice_threads(int n1, int n2, int cl)
 {
-  return cl == SLICE_RF || cl == SLICE_RF2 ? slice_rf_threads(n1, n2, slice_ctas(cl)) : NT;
+  return slice_is_rf(cl) ? slice_rf_threads(n1, n2, slice_ctas(cl)) : NT;
 }
 
 cudaError_t launch_slice(const LineParams &p, cudaStream_t s)
@@ -414,6 +414,7 @@ cudaError_t launch_slice(const LineParams &p, cudaStream_t s)
   switch (p.cluster) {
     case SLICE_RF: return launch_slice_rf(p, 1, s);
     case SLICE_RF2: return launch_slice_rf(p, 2, s);
+    case SLICE_RF4: return launch_slice_rf(p, 4, s);
     case 1: return launch_cl<1>(p, s);
     case 2: return launch_cl<2>(p, s);
     case 4: return launch_cl<4>(p, s);

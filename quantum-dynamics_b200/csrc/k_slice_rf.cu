@@ -38,26 +38,30 @@
 // two transposes between them are bulk shared-memory-to-shared-memory copies
 // of whole row halves, so no pass touches the other CTA's memory itself.
 //
-// Radix-16 and radix-12 DFTs are 4x4 and 4x3 compositions whose internal
-// twiddles are compensated constants (value + residual), like the radix-8
-// and radix-3 butterflies, so no fixed-point rounding bias enters the norm.
+// The 6-, 12-, 16-, 24- and 32-point DFTs are P x Q compositions whose
+// internal twiddles are compensated constants (value + residual), like the
+// radix-8 and radix-3 butterflies, so no fixed-point rounding bias enters
+// the norm.
 #include <cstdlib>
 #include "qd_kernels.h"
 
 namespace {
 
 // ---- compile-time twiddles exp(SGN 2 pi i E / N) --------------------------
-// cos(2 pi a / 48) as (magnitude code, sign); a in [0, 48), a multiple of 3 or 4.
-// codes: 0 -> 0, 1 -> 1, 2 -> 1/2, 3 -> 1/sqrt2, 4 -> sqrt3/2, 5 -> cos(pi/8), 6 -> sin(pi/8)
+// cos(2 pi a / 96) as (magnitude code, sign); a in [0, 96), a multiple of 3 or 4.
+// codes: 0 -> 0, 1 -> 1, 2 -> 1/2, 3 -> 1/sqrt2, 4 -> sqrt3/2, 5 -> cos(pi/8),
+// 6 -> sin(pi/8), 7 -> cos(pi/16), 8 -> cos(3pi/16), 9 -> sin(3pi/16),
+// 10 -> sin(pi/16), 11 -> cos(pi/12), 12 -> sin(pi/12)
 __host__ __device__ constexpr int kcode(int a)
 {
-  const int r = a % 24 <= 12 ? a % 24 : 24 - a % 24;    // |cos| is even in a and 24-periodic
-  return r == 0 ? 1 : r == 3 ? 5 : r == 4 ? 4 : r == 6 ? 3 : r == 8 ? 2 : r == 9 ? 6 : r == 12 ? 0
-                                                                                               : -1;
+  const int r = a % 48 <= 24 ? a % 48 : 48 - a % 48;    // |cos| is even in a and 48-periodic
+  return r == 0 ? 1 : r == 3 ? 7 : r == 4 ? 11 : r == 6 ? 5 : r == 8 ? 4 : r == 9 ? 8
+       : r == 12 ? 3 : r == 15 ? 9 : r == 16 ? 2 : r == 18 ? 6 : r == 20 ? 12 : r == 21 ? 10
+       : r == 24 ? 0 : -1;
 }
 __host__ __device__ constexpr int ksign(int a)
 {
-  return (a % 48 > 12 && a % 48 < 36) ? -1 : 1;
+  return (a % 96 > 24 && a % 96 < 72) ? -1 : 1;
 }
 
 template <int CODE> __device__ __forceinline__ float kmag(float x)
@@ -68,10 +72,16 @@ template <int CODE> __device__ __forceinline__ float kmag(float x)
   else if constexpr (CODE == 4) return fmaf(x, 8.66025388e-01f, x * 1.55436251e-08f);
   else if constexpr (CODE == 5) return fmaf(x, 9.23879504e-01f, x * 2.83074897e-08f);
   else if constexpr (CODE == 6) return fmaf(x, 3.82683426e-01f, x * 6.22335072e-09f);
+  else if constexpr (CODE == 7) return fmaf(x, 9.80785251e-01f, x * 2.97394731e-08f);
+  else if constexpr (CODE == 8) return fmaf(x, 8.31469595e-01f, x * 1.68702634e-08f);
+  else if constexpr (CODE == 9) return fmaf(x, 5.55570245e-01f, x * -1.17695214e-08f);
+  else if constexpr (CODE == 10) return fmaf(x, 1.95090324e-01f, x * -1.67047143e-09f);
+  else if constexpr (CODE == 11) return fmaf(x, 9.65925813e-01f, x * 1.35678162e-08f);
+  else if constexpr (CODE == 12) return fmaf(x, 2.58819044e-01f, x * 1.46619872e-09f);
   else return 0.f;
 }
 
-// x * cos(2 pi A / 48)
+// x * cos(2 pi A / 96)
 template <int A> __device__ __forceinline__ float kcos(float x)
 {
   static_assert(kcode(A) >= 0, "angle not in the table");
@@ -81,9 +91,9 @@ template <int A> __device__ __forceinline__ float kcos(float x)
 
 template <int N, int E, int SGN> __device__ __forceinline__ float2 twk(float2 z)
 {
-  static_assert(48 % N == 0, "N must divide 48");
-  constexpr int a = (E % N) * (48 / N);
-  constexpr int as = (a + 36) % 48;                     // sin(t) = cos(t - pi/2)
+  static_assert(96 % N == 0, "N must divide 96");
+  constexpr int a = (E % N) * (96 / N);
+  constexpr int as = (a + 72) % 96;                     // sin(t) = cos(t - pi/2)
   if constexpr (a == 0) {
     return z;
   } else {
@@ -117,63 +127,82 @@ template <int SGN> struct Dft<8, SGN> {
   static __device__ __forceinline__ void run(float2 *v) { SmallDFT<8, float2>::run(v, SGN, nullptr, 0); }
 };
 
-// N = 4 Q: n = p + 4 q, Q-point DFTs over q, twiddles W_N^{p c}, 4-point
+// N = P Q: n = p + P q, Q-point DFTs over q, twiddles W_N^{p c}, P-point
 // DFTs over p, X[c + Q d]
-template <int N, int Q, int SGN> struct Dft4xQ {
-  template <int P, int C> static __device__ __forceinline__ void tw(float2 (&u)[4][Q])
+template <int N, int P, int Q, int SGN> struct DftPxQ {
+  template <int PP, int C> static __device__ __forceinline__ void tw(float2 (&u)[P][Q])
   {
     if constexpr (C < Q) {
-      u[P][C] = twk<N, P * C, SGN>(u[P][C]);
-      tw<P, C + 1>(u);
-    } else if constexpr (P + 1 < 4) {
-      tw<P + 1, 0>(u);
+      u[PP][C] = twk<N, PP * C, SGN>(u[PP][C]);
+      tw<PP, C + 1>(u);
+    } else if constexpr (PP + 1 < P) {
+      tw<PP + 1, 0>(u);
     }
   }
   static __device__ __forceinline__ void run(float2 *v)
   {
-    float2 u[4][Q];
+    float2 u[P][Q];
 #pragma unroll
-    for (int p = 0; p < 4; p++) {
+    for (int p = 0; p < P; p++) {
 #pragma unroll
-      for (int q = 0; q < Q; q++) u[p][q] = v[p + 4 * q];
+      for (int q = 0; q < Q; q++) u[p][q] = v[p + P * q];
       Dft<Q, SGN>::run(u[p]);
     }
     tw<1, 1>(u);
 #pragma unroll
     for (int c = 0; c < Q; c++) {
-      float2 s[4] = {u[0][c], u[1][c], u[2][c], u[3][c]};
-      Dft<4, SGN>::run(s);
+      float2 s[P];
 #pragma unroll
-      for (int d = 0; d < 4; d++) v[c + Q * d] = s[d];
+      for (int p = 0; p < P; p++) s[p] = u[p][c];
+      Dft<P, SGN>::run(s);
+#pragma unroll
+      for (int d = 0; d < P; d++) v[c + Q * d] = s[d];
     }
   }
 };
+template <int SGN> struct Dft<6, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { DftPxQ<6, 2, 3, SGN>::run(v); }
+};
 template <int SGN> struct Dft<12, SGN> {
-  static __device__ __forceinline__ void run(float2 *v) { Dft4xQ<12, 3, SGN>::run(v); }
+  static __device__ __forceinline__ void run(float2 *v) { DftPxQ<12, 4, 3, SGN>::run(v); }
 };
 template <int SGN> struct Dft<16, SGN> {
-  static __device__ __forceinline__ void run(float2 *v) { Dft4xQ<16, 4, SGN>::run(v); }
+  static __device__ __forceinline__ void run(float2 *v) { DftPxQ<16, 4, 4, SGN>::run(v); }
+};
+template <int SGN> struct Dft<24, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { DftPxQ<24, 4, 6, SGN>::run(v); }
+};
+template <int SGN> struct Dft<32, SGN> {
+  static __device__ __forceinline__ void run(float2 *v) { DftPxQ<32, 4, 8, SGN>::run(v); }
 };
 
 template <int N1, int N2, int NT, int CL> struct RfShape {
-  static constexpr int A1 = N1 == 64 ? 8 : 16;        // row pass 2 radix (B1 = 8)
+  static constexpr int A1 = N1 == 64 ? 8 : N1 == 256 ? 32 : 16;   // row pass 2 radix (B1 = 8)
   static constexpr int B1 = N1 / A1;
   static constexpr int A2 = N2 / 8;                   // column pass 2 radix (B2 = 8)
   static constexpr int B2 = 8;
   static constexpr int RS = N1 + B1;                  // padded row stride (complex)
   static constexpr int HR = N2 / CL;                  // rows held by one CTA
-  static constexpr int HW = RS / CL;                  // row-half width: B1 / CL whole blocks
-  // own rows [HR][RS]; CL = 2: the peer's rows, this CTA's column half
-  // [HR][HW]; rc1[l], W_N2, kc1 in column-counter order, kc2; two mbarriers
+  static constexpr int HW = RS / CL;                  // column part width: B1 / CL whole blocks
+  static constexpr int BPO = B2 / CL;                 // column-pass row groups per CTA's rows
+  // CL = 4: the column passes read all N2 rows of this CTA's column part
+  // from one [N2][HW] array (its own rows copied in too); CL = 2 reads its own
+  // rows in place and keeps only the peer's in the second array, which
+  // leaves room for two CTAs per SM
+  static constexpr bool FULLP = CL == 4;
+  static constexpr int PSLOTS = CL == 1 ? 0 : FULLP ? CL : CL - 1;
+  static constexpr int P1_UNROLL = FULLP ? 3 : 2;    // row items per thread loaded together
+  // own rows [HR][RS]; CL > 1: rows of this CTA's column part [PSLOTS][HR][HW];
+  // rc1[l], W_N2, kc1 in column-counter order, kc2; two mbarriers
   static constexpr size_t TABLES = 2 * (N1 + N2);
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (CL > 1 ? (size_t)HR * HW : 0) +
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (size_t)PSLOTS * HR * HW +
                                                    TABLES) + (CL > 1 ? 16 : 0);
-  static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row half, one bulk copy
+  static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row part, one bulk copy
   static_assert(B1 == 8 && RS % 16 == 8, "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
-  static_assert(CL == 1 || (CL == 2 && A1 == 16 && HR == 4 * A2 && HW == 4 * (A1 + 1) &&
-                            HALF_BYTES % 16 == 0 && HR <= NT),
-                "2-CTA split: four whole row blocks per half, column rows A2 b' split at b' = 4");
+  static_assert(CL == 1 || ((CL == 2 || CL == 4) && B1 % CL == 0 && HR == BPO * A2 &&
+                            HW == (B1 / CL) * (A1 + 1) && HALF_BYTES % 16 == 0),
+                "cluster split: whole row blocks per column part, whole column row groups per CTA");
 };
 
 __device__ __forceinline__ float2 rot_at(const float2 *r1, float2 rj, int i)
@@ -215,15 +244,18 @@ __device__ __forceinline__ bool mbar_wait0(uint32_t mbar)
   return false;
 }
 
-// CL = 2: a 2-CTA thread-block cluster per slice.  CTA `rank` runs the row
-// passes on rows [rank HR, (rank+1) HR) and the column passes on column
-// half `rank` (row blocks 4 rank .. 4 rank + 3) over all N2 rows: its own
-// rows in place in its row array, the peer's rows in a second array.  The
-// two transposes are bulk copies of whole row halves (HW complex, 544
-// bytes) between the CTAs' shared memories: after P2 each CTA sends its
-// rows' other half to the peer, after P5 it sends the peer's rows back; an
-// mbarrier in the receiving CTA counts the bytes in.  Every load and store
-// of the passes is local.  CL = 1 keeps the slice in one array in place.
+// CL = 2 or 4: a CL-CTA thread-block cluster per slice.  CTA `rank` runs
+// the row passes on rows [rank HR, (rank+1) HR) and the column passes on
+// column part `rank` (row blocks rank B1/CL .. (rank+1) B1/CL - 1) over all
+// N2 rows: its own rows in place in its row array, each peer's rows in a
+// slot of a second array (slot o for peer o < rank, o - 1 for o > rank).
+// The two transposes are bulk copies of whole row parts (HW complex: 544
+// bytes at 128 columns and CL = 2, 528 bytes at 256 columns and CL = 4)
+// between the CTAs' shared memories: after P2 each CTA sends every peer the
+// peer's part of its own rows, after P5 it sends every peer's rows back; an
+// mbarrier in the receiving CTA counts the bytes in from all peers.  Every
+// load and store of the passes is local.  CL = 1 keeps the slice in one
+// array in place.
 template <int N1, int N2, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
@@ -232,12 +264,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
   float2 *R = reinterpret_cast<float2 *>(smem4);    // own rows [HR][RS]
-  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column half [HR][HW]
-  float2 *r1 = P + (CL > 1 ? HR * HW : 0);           // rc1[l][0..N1)
+  float2 *P = R + HR * RS;                           // CL > 1: rows of own column part [PSLOTS][HR][HW]
+  float2 *r1 = P + Sh::PSLOTS * HR * HW;             // rc1[l][0..N1)
   float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
   float2 *k1 = t2 + N2;                              // kc1[k(q)], q < N1
   float2 *k2 = k1 + N1;                              // kc2
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL = 2: [0] P filled, [1] R's other half
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL > 1: [0] P filled, [1] R's other parts
   const int tid = threadIdx.x;
   pdl_trigger();
   if ((int)blockIdx.x >= p.nruns * p.nl * CL) {      // extra CTAs: flux preparation
@@ -248,9 +280,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   int rank = 0;
   if constexpr (CL > 1) asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  if constexpr (CL == 2) {
+  if constexpr (CL > 1) {
     if (tid == 0) {
-      const uint32_t tx = HR * Sh::HALF_BYTES;
+      const uint32_t tx = (CL - 1) * HR * Sh::HALF_BYTES;   // from every peer, every row
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[0])));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[1])));
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
@@ -285,7 +317,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     float2 w[B1];
 #pragma unroll
     for (int c = 0; c < B1; c++) w[c] = __ldg(tw1 + a * c);
-#pragma unroll 2
+#pragma unroll (Sh::P1_UNROLL)
     for (int e = tid; e < HR * A1; e += NT) {
       const int j = e / A1, jg = j0 + j;
       const float2 rj = __ldg(rc2 + jg);
@@ -312,37 +344,49 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int d = 0; d < A1; d++) blk[d] = v[d];
   }
   bool ok = true;
-  if constexpr (CL == 2) {
-    // the other column half of every own row -> the peer's P array
+  if constexpr (CL > 1) {
+    // peer o's column part of every own row -> this CTA's slot of o's P array
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    cluster_wait();                                  // the peer's mbarriers are initialised
-    if (tid < HR) {
-      const uint32_t peer = rank ^ 1;
-      bulk_to_peer(peer_addr(smem_addr(P + tid * HW), peer),
-                   smem_addr(R + tid * RS + HW * peer), Sh::HALF_BYTES,
+    cluster_wait();                                  // the peers' mbarriers are initialised
+    for (int e = tid; e < (CL - 1) * HR; e += NT) {
+      const int pi = e / HR, j = e % HR;
+      const uint32_t peer = pi < rank ? pi : pi + 1;
+      const int slot = Sh::FULLP ? rank : rank < (int)peer ? rank : rank - 1;
+      bulk_to_peer(peer_addr(smem_addr(P + (slot * HR + j) * HW), peer),
+                   smem_addr(R + j * RS + HW * peer), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[0]), peer));
     }
-    ok = mbar_wait0(smem_addr(&mbar[0]));            // the peer's rows of this half are in
+    if constexpr (Sh::FULLP) {                       // own rows' part -> slot rank
+      constexpr int V4 = Sh::HALF_BYTES / 16;        // float4 per row part
+      for (int e = tid; e < HR * V4; e += NT) {
+        const int j = e / V4, x = e % V4;
+        reinterpret_cast<float4 *>(P + (rank * HR + j) * HW)[x] =
+            reinterpret_cast<const float4 *>(R + j * RS + HW * rank)[x];
+      }
+      __syncthreads();
+    }
+    ok = mbar_wait0(smem_addr(&mbar[0]));            // the peers' rows of this part are in
   } else {
     __syncthreads();
   }
   // column passes: column counter q = q0 + qq (frequency k(q) = q / A1 + B1 (q % A1))
-  // at offset pcol(qq) of this CTA's half; rows A2 b + r, b < 4 in CTA 0's rows
+  // at offset pcol(qq) of this CTA's part; row A2 b + r (b < B2) is held by
+  // CTA b / BPO, as its row A2 (b % BPO) + r
+  constexpr int BPO = Sh::BPO;
   auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
-  float2 *blo, *bhi;                                 // row 0 of b < 4 and of b >= 4
-  int slo, shi;                                      // their row strides
-  if constexpr (CL == 1) {
-    blo = R; bhi = R + 4 * A2 * RS; slo = shi = RS;
-  } else {
-    blo = rank == 0 ? R : P;
-    bhi = rank == 0 ? P : R + HW;
-    slo = rank == 0 ? RS : HW;
-    shi = rank == 0 ? HW : RS;
+  float2 *cb[Sh::FULLP ? 1 : CL];                    // row 0 of CTA o's rows, this part
+  int cs[Sh::FULLP ? 1 : CL];                        // and their row stride
+  if constexpr (!Sh::FULLP) {
+#pragma unroll
+    for (int o = 0; o < CL; o++) {
+      cb[o] = o == rank ? R + HW * rank : P + (o - (o > rank ? 1 : 0)) * HR * HW;
+      cs[o] = o == rank ? RS : HW;
+    }
   }
   auto at = [&](int b, int inner, int qq) -> float2 & {
-    return b < 4 ? blo[(inner + A2 * b) * slo + pcol(qq)]
-                 : bhi[(inner + A2 * (b - 4)) * shi + pcol(qq)];
+    if constexpr (Sh::FULLP) return P[(inner + A2 * b) * HW + pcol(qq)];
+    else return cb[b / BPO][(inner + A2 * (b % BPO)) * cs[b / BPO] + pcol(qq)];
   };
   constexpr int QC = N1 / CL;
   // P3: items (q, a'): rows a' + A2 b'
@@ -359,19 +403,30 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   // P4: items (q, c'): rows a' + A2 c'; forward pass 2, kinetic phase, inverse pass 1
   for (int e = tid; e < QC * B2; e += NT) {
     const int qq = e % QC, cp = e / QC;
-    float2 *col = (cp < 4 ? blo + A2 * cp * slo : bhi + A2 * (cp - 4) * shi) + pcol(qq);
-    const int cs = cp < 4 ? slo : shi;
+    float2 *col;
+    int cst;
+    if constexpr (Sh::FULLP) {
+      col = P + A2 * cp * HW + pcol(qq);
+      cst = HW;
+    } else {
+      float2 *cbase = cb[0];
+      cst = cs[0];
+#pragma unroll
+      for (int o = 1; o < CL; o++)
+        if (cp / BPO == o) { cbase = cb[o]; cst = cs[o]; }
+      col = cbase + A2 * (cp % BPO) * cst + pcol(qq);
+    }
     const float2 kq = k1[q0 + qq];
     float2 v[A2];
 #pragma unroll
-    for (int a = 0; a < A2; a++) v[a] = col[a * cs];
+    for (int a = 0; a < A2; a++) v[a] = col[a * cst];
     Dft<A2, -1>::run(v);
 #pragma unroll
     for (int d = 0; d < A2; d++)
       v[d] = cmul(v[d], cscale2(cmul(kq, k2[cp + B2 * d]), p.kscale, p.kscale_lo));
     Dft<A2, +1>::run(v);
 #pragma unroll
-    for (int cc = 0; cc < A2; cc++) col[cc * cs] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
+    for (int cc = 0; cc < A2; cc++) col[cc * cst] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
   }
   __syncthreads();
   // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d'', in place
@@ -384,28 +439,44 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll
     for (int d = 0; d < B2; d++) at(d, cc, qq) = v[d];
   }
-  if constexpr (CL == 2) {
-    // the peer's rows of this half -> back into the peer's row array
+  if constexpr (CL > 1) {
+    // every peer's rows of this part -> back into that peer's row array
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid < HR) {
-      const uint32_t peer = rank ^ 1;
-      bulk_to_peer(peer_addr(smem_addr(R + tid * RS + HW * rank), peer),
-                   smem_addr(P + tid * HW), Sh::HALF_BYTES,
+    for (int e = tid; e < (CL - 1) * HR; e += NT) {
+      const int pi = e / HR, j = e % HR;               // slot pi holds peer pi (< rank) or pi + 1
+      const uint32_t peer = pi < rank ? pi : pi + 1;
+      const int slot = Sh::FULLP ? (int)peer : pi;
+      bulk_to_peer(peer_addr(smem_addr(R + j * RS + HW * rank), peer),
+                   smem_addr(P + (slot * HR + j) * HW), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[1]), peer));
     }
-    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other half of the own rows is back
+    if constexpr (Sh::FULLP) {                       // slot rank -> own rows' part
+      constexpr int V4 = Sh::HALF_BYTES / 16;
+      for (int e = tid; e < HR * V4; e += NT) {
+        const int j = e / V4, x = e % V4;
+        reinterpret_cast<float4 *>(R + j * RS + HW * rank)[x] =
+            reinterpret_cast<const float4 *>(P + (rank * HR + j) * HW)[x];
+      }
+    }
+    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other parts of the own rows are back
     cluster_arrive_release();                        // this CTA's incoming copies are complete
     if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
+    if constexpr (Sh::FULLP) __syncthreads();        // the own part copied back
   } else {
     __syncthreads();
   }
   // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
   {
+    // the twiddles stay in registers across items, except at A1 = 32, where
+    // they would double the live registers of the 32-point DFT
+    constexpr bool HOIST = A1 <= 16;
     const int bk = tid % B1;
-    float2 w[A1];
+    float2 w[HOIST ? A1 : 1];
+    if constexpr (HOIST) {
 #pragma unroll
-    for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
+      for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
+    }
     for (int e = tid; e < HR * B1; e += NT) {
       const int j = e / B1;
       float2 *blk = R + j * RS + (A1 + 1) * bk;
@@ -414,7 +485,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
       for (int s = 0; s < A1; s++) v[s] = blk[s];
       Dft<A1, +1>::run(v);
 #pragma unroll
-      for (int c = 0; c < A1; c++) blk[c] = c ? cmul(v[c], w[c]) : v[c];
+      for (int c = 0; c < A1; c++) {
+        if constexpr (HOIST) blk[c] = c ? cmul(v[c], w[c]) : v[c];
+        else blk[c] = c ? cmul(v[c], cconj(__ldg(tw1 + bk * c))) : v[c];
+      }
     }
   }
   __syncthreads();
@@ -432,8 +506,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
       g[jg * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
   }
   // no CTA leaves while its shared memory may still be the source of a copy
-  // (the peer arrives only once all of its incoming copies are complete)
-  if constexpr (CL == 2) cluster_wait();
+  // (a peer arrives only once all of its incoming copies are complete)
+  if constexpr (CL > 1) cluster_wait();
 }
 
 template <int N1, int N2, int NT, int CL>
@@ -479,6 +553,8 @@ int slice_rf_threads(int n1, int n2, int cl)
   } else if (cl == 2) {
     if (n1 == 128 && n2 == 96) return 256;
     if (n1 == 128 && n2 == 128) return 512;
+  } else if (cl == 4) {
+    if (n1 == 256 && n2 == 192) return 512;
   }
   return 0;
 }
@@ -492,6 +568,8 @@ cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s)
   } else if (cl == 2) {
     if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256, 2>(p, s);
     if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512, 2>(p, s);
+  } else if (cl == 4) {
+    if (p.n1 == 256 && p.n2 == 192) return launch_rf<256, 192, 512, 4>(p, s);
   }
   return cudaErrorInvalidValue;
 }

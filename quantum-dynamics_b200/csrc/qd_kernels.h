@@ -210,8 +210,13 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
 // (0 if none), its launch, and the smem bytes it needs
 constexpr int SLICE_RF = 8;    // LineParams::cluster value of the register-FFT slice kernel
 constexpr int SLICE_RF2 = 9;   // the same on a 2-CTA cluster per slice
+constexpr int SLICE_RF4 = 10;  // the same on a 4-CTA cluster per slice
+inline bool slice_is_rf(int cluster)
+{ return cluster == SLICE_RF || cluster == SLICE_RF2 || cluster == SLICE_RF4; }
 inline int slice_ctas(int cluster)           // CTAs per slice
-{ return cluster == SLICE_RF ? 1 : cluster == SLICE_RF2 ? 2 : cluster; }
+{
+  return cluster == SLICE_RF ? 1 : cluster == SLICE_RF2 ? 2 : cluster == SLICE_RF4 ? 4 : cluster;
+}
 int slice_cluster_ok(int n1, int n2, int cluster);
 int slice_rf_threads(int n1, int n2, int cl); // threads per CTA, 0 if the shape is not built
 int slice_threads(int n1, int n2, int cluster);

@@ -221,17 +221,18 @@ def test_fp32_tensor_core_and_simt_agree(monkeypatch):
     assert rel(out["tc"], out["simt"]) < 2e-5
 
 
-@pytest.mark.parametrize("shape", [(64, 64, 32), (128, 128, 64), (128, 96, 64), (48, 40, 24)])
+@pytest.mark.parametrize("shape", [(64, 64, 32), (128, 128, 64), (128, 96, 64), (48, 40, 24),
+                                   (256, 192, 16)])
 def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
     # fused slice kernel with 1, 2, 4 CTAs per slice and the register-FFT slice
-    # kernel on 1 (8) and 2 (9) CTAs per slice, where they are built, against
+    # kernel on 1 (8), 2 (9) and 4 (10) CTAs per slice, where they are built, against
     # the three-kernel split pass;
     # the flux preparation rides in the fused launches, so P(E) is compared too
     n1, n2, nth = shape
     base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=8, n_energies=5,
                         n_gradient_points=5, r=(0.5, 9.0))
     out = {}
-    for cl in ("0", "1", "2", "4", "8", "9"):
+    for cl in ("0", "1", "2", "4", "8", "9", "10"):
         monkeypatch.setenv("QD_SLICE_CLUSTER", cl)
         d = S.copy_case(base)
         d.options.precision = QD_PREC_FP32
@@ -245,9 +246,9 @@ def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
 
 
 @pytest.mark.parametrize("shape,kind", [((64, 64, 32), "8"), ((128, 96, 64), "8"),
-                                        ((128, 96, 64), "9")])
+                                        ((128, 96, 64), "9"), ((256, 192, 16), "10")])
 def test_fp32_register_fft_slice_batch_matches_fp64(shape, kind, monkeypatch):
-    # the register-FFT slice kernel (one CTA or a 2-CTA cluster per slice) on
+    # the register-FFT slice kernel (one CTA, or a 2- or 4-CTA cluster per slice) on
     # a 3-run batch (flux preparation in its extra CTAs) against the FP64
     # plain form of the same runs, 40 steps
     n1, n2, nth = shape
