@@ -554,7 +554,7 @@ int slice_rf_threads(int n1, int n2, int cl)
     if (n1 == 128 && n2 == 96) return 256;
     if (n1 == 128 && n2 == 128) return 512;
   } else if (cl == 4) {
-    if (n1 == 256 && n2 == 192) return 512;
+    if (n1 == 256 && n2 == 192) return 512;   // 128 x 96 and 128 x 128 run faster on CL <= 2
   }
   return 0;
 }
