@@ -369,11 +369,13 @@ def run_ours(args):
     }
     # DRAM bytes (read + write) per launch from one ncu capture each (cold caches:
     # ncu flushes them before every captured launch); the batch figures were
-    # captured on 32 runs and scale with the runs.  Sources: the ncu summaries
-    # column_tc_and_slice_rf2_c1_128x128x64.md and
-    # column_tc_and_slice_rf_batch32_128x96x64.md under profiles/.
+    # captured on 32 (c2j0) or 4 (c4) runs and scale with the runs.  Sources: the
+    # ncu summaries column_tc_and_slice_rf2_c1_128x128x64.md,
+    # column_tc_and_slice_rf_batch32_128x96x64.md and
+    # column_tc_and_slice_rf4_c4_4runs_256x192x128.md under profiles/.
     traffic_ncu = {("c1", "column"): 16.89e6, ("c1", "lines"): 9.30e6,
-                   ("c2j0", "column"): 373.7e6 / 32, ("c2j0", "lines"): 379.7e6 / 32}
+                   ("c2j0", "column"): 373.7e6 / 32, ("c2j0", "lines"): 379.7e6 / 32,
+                   ("c4", "column"): 568.4e6 / 4, ("c4", "lines"): 360.7e6 / 4}
     names = ["column", "lines", "flux_prep", "flux_accum", "crp"]
     per = {names[i]: kclass[i] for i in range(min(5, len(kclass)))}
     step_ms = t_max / K
@@ -381,7 +383,7 @@ def run_ours(args):
     dom_ms = per.get(dom, float("nan"))
     achieved = alg[dom] / (dom_ms * 1e-3) / 1e9 if dom_ms and dom_ms > 0 else None
     tr = traffic_ncu.get((args.workload, dom)) if not args.fp64 else None
-    if tr is not None and args.workload == "c2j0":
+    if tr is not None and args.workload in ("c2j0", "c4"):
         tr *= len(runs)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s",
