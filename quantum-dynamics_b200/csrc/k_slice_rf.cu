@@ -185,18 +185,20 @@ template <int N1, int N2, int NT, int CL> struct RfShape {
   static constexpr int HR = N2 / CL;                  // rows held by one CTA
   static constexpr int HW = RS / CL;                  // column part width: B1 / CL whole blocks
   static constexpr int BPO = B2 / CL;                 // column-pass row groups per CTA's rows
-  // CL = 4: the column passes read all N2 rows of this CTA's column part
-  // from one [N2][HW] array (its own rows copied in too); CL = 2 reads its own
-  // rows in place and keeps only the peer's in the second array, which
-  // leaves room for two CTAs per SM
-  static constexpr bool FULLP = CL == 4;
-  static constexpr int PSLOTS = CL == 1 ? 0 : FULLP ? CL : CL - 1;
-  static constexpr int P1_UNROLL = FULLP ? 3 : 2;    // row items per thread loaded together
-  // own rows [HR][RS]; CL > 1: rows of this CTA's column part [PSLOTS][HR][HW];
-  // rc1[l], W_N2, kc1 in column-counter order, kc2; two mbarriers
+  // CL = 4: the transposes swap row parts between the CTAs in place (SWAP),
+  // so a CTA holds only its row array and two CTAs fit on an SM; CL = 2
+  // keeps the peer's rows of its column part in a second array, filled and
+  // emptied by bulk copies
+  static constexpr bool SWAP = CL == 4;
+  static constexpr int PSLOTS = CL == 1 || SWAP ? 0 : CL - 1;
+  static constexpr int P1_UNROLL = 2;                // row items per thread loaded together
+  static constexpr int SWAP_ROUNDS = 4;              // row rounds of the in-place transpose
+  // own rows [HR][RS]; CL = 2: the peer's rows of this CTA's column part
+  // [HR][HW]; rc1[l], W_N2, kc1 in column-counter order, kc2; CL = 2: two
+  // mbarriers
   static constexpr size_t TABLES = 2 * (N1 + N2);
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (size_t)PSLOTS * HR * HW +
-                                                   TABLES) + (CL > 1 ? 16 : 0);
+                                                   TABLES) + (PSLOTS > 0 ? 16 : 0);
   static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row part, one bulk copy
   static_assert(B1 == 8 && RS % 16 == 8, "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
@@ -244,18 +246,74 @@ __device__ __forceinline__ bool mbar_wait0(uint32_t mbar)
   return false;
 }
 
+// st.shared::cluster of 16 bytes (a mapa address)
+__device__ __forceinline__ void st_peer4(uint32_t a, float4 v)
+{
+  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};"
+               :: "r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+
+// The in-place transpose of a CL-CTA slice: for every peer o, row part o of
+// this CTA's rows and row part `rank` of o's rows trade places (the same
+// rows j, the same HW-complex columns in both row arrays), so afterwards row
+// part o of the array holds the rows of CTA o in this CTA's column part;
+// called again it undoes itself.  NR rounds of HR / NR rows each: every
+// thread reads its share of the round's row parts into registers, the
+// cluster barrier guarantees that every CTA has read them, and the values
+// are stored into the peers' arrays; the rows of one round are disjoint
+// from the others', so only the final barrier orders the last round's
+// stores before the following passes.
+template <int NT, int CL, int HR, int HW, int RS, int NR>
+__device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
+{
+  constexpr int XW = HW / 2;                          // float4 per row part
+  constexpr int HALF = HR / NR;                       // rows per round
+  constexpr int PER = (CL - 1) * HALF * XW;           // float4 of one round
+  constexpr int F = (PER + NT - 1) / NT;              // per thread
+  static_assert(HW % 2 == 0 && RS % 2 == 0 && HR % NR == 0, "16-byte row parts, whole rows");
+  float4 *R4 = reinterpret_cast<float4 *>(R);
+#pragma unroll 1
+  for (int r = 0; r < NR; r++) {
+    float4 v[F];
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      const int e = k * NT + tid;
+      if (e < PER) {
+        const int pi = e / (HALF * XW), rem = e % (HALF * XW);
+        const int j = r * HALF + rem / XW, x = rem % XW;
+        const int peer = pi < rank ? pi : pi + 1;
+        v[k] = R4[(j * RS + HW * peer) / 2 + x];
+      }
+    }
+    cluster_arrive_release();                        // every CTA has read this round's rows
+    cluster_wait();
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+      const int e = k * NT + tid;
+      if (e < PER) {
+        const int pi = e / (HALF * XW), rem = e % (HALF * XW);
+        const int j = r * HALF + rem / XW, x = rem % XW;
+        const int peer = pi < rank ? pi : pi + 1;
+        st_peer4(peer_addr(smem_addr(R4 + (j * RS + HW * rank) / 2 + x), (uint32_t)peer), v[k]);
+      }
+    }
+  }
+  cluster_arrive_release();                          // every CTA's incoming rows are in
+  cluster_wait();
+}
+
 // CL = 2 or 4: a CL-CTA thread-block cluster per slice.  CTA `rank` runs
 // the row passes on rows [rank HR, (rank+1) HR) and the column passes on
 // column part `rank` (row blocks rank B1/CL .. (rank+1) B1/CL - 1) over all
-// N2 rows: its own rows in place in its row array, each peer's rows in a
-// slot of a second array (slot o for peer o < rank, o - 1 for o > rank).
-// The two transposes are bulk copies of whole row parts (HW complex: 544
-// bytes at 128 columns and CL = 2, 528 bytes at 256 columns and CL = 4)
-// between the CTAs' shared memories: after P2 each CTA sends every peer the
-// peer's part of its own rows, after P5 it sends every peer's rows back; an
-// mbarrier in the receiving CTA counts the bytes in from all peers.  Every
-// load and store of the passes is local.  CL = 1 keeps the slice in one
-// array in place.
+// N2 rows.  CL = 2: its own rows in place in its row array, the peer's
+// rows in a second array; the two transposes are bulk copies of whole row
+// halves (544 bytes) between the CTAs' shared memories (after P2 each CTA
+// sends the peer's half of its own rows, after P5 it sends the peer's rows
+// back; an mbarrier in the receiving CTA counts the bytes in).  CL = 4:
+// both transposes are the in-place swap of swap_parts, after which row
+// part o of the row array holds CTA o's rows in this CTA's column part.
+// Every load and store of the passes is local.  CL = 1 keeps the slice in
+// one array in place.
 template <int N1, int N2, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
@@ -264,12 +322,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
   float2 *R = reinterpret_cast<float2 *>(smem4);    // own rows [HR][RS]
-  float2 *P = R + HR * RS;                           // CL > 1: rows of own column part [PSLOTS][HR][HW]
+  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column half [HR][HW]
   float2 *r1 = P + Sh::PSLOTS * HR * HW;             // rc1[l][0..N1)
   float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
   float2 *k1 = t2 + N2;                              // kc1[k(q)], q < N1
   float2 *k2 = k1 + N1;                              // kc2
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL > 1: [0] P filled, [1] R's other parts
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL = 2: [0] P filled, [1] R's other half
   const int tid = threadIdx.x;
   pdl_trigger();
   if ((int)blockIdx.x >= p.nruns * p.nl * CL) {      // extra CTAs: flux preparation
@@ -280,7 +338,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   int rank = 0;
   if constexpr (CL > 1) asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  if constexpr (CL > 1) {
+  if constexpr (Sh::PSLOTS > 0) {
     if (tid == 0) {
       const uint32_t tx = (CL - 1) * HR * Sh::HALF_BYTES;   // from every peer, every row
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[0])));
@@ -333,6 +391,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   __syncthreads();
   // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
+#pragma unroll 1
   for (int e = tid; e < HR * B1; e += NT) {
     const int j = e / B1, c = e % B1;
     float2 *blk = R + j * RS + (A1 + 1) * c;
@@ -344,7 +403,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int d = 0; d < A1; d++) blk[d] = v[d];
   }
   bool ok = true;
-  if constexpr (CL > 1) {
+  if constexpr (Sh::SWAP) {
+    __syncthreads();
+    swap_parts<NT, CL, HR, HW, RS, Sh::SWAP_ROUNDS>(R, rank, tid);
+  } else if constexpr (CL > 1) {
     // peer o's column part of every own row -> this CTA's slot of o's P array
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -352,19 +414,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int e = tid; e < (CL - 1) * HR; e += NT) {
       const int pi = e / HR, j = e % HR;
       const uint32_t peer = pi < rank ? pi : pi + 1;
-      const int slot = Sh::FULLP ? rank : rank < (int)peer ? rank : rank - 1;
+      const int slot = rank < (int)peer ? rank : rank - 1;
       bulk_to_peer(peer_addr(smem_addr(P + (slot * HR + j) * HW), peer),
                    smem_addr(R + j * RS + HW * peer), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[0]), peer));
-    }
-    if constexpr (Sh::FULLP) {                       // own rows' part -> slot rank
-      constexpr int V4 = Sh::HALF_BYTES / 16;        // float4 per row part
-      for (int e = tid; e < HR * V4; e += NT) {
-        const int j = e / V4, x = e % V4;
-        reinterpret_cast<float4 *>(P + (rank * HR + j) * HW)[x] =
-            reinterpret_cast<const float4 *>(R + j * RS + HW * rank)[x];
-      }
-      __syncthreads();
     }
     ok = mbar_wait0(smem_addr(&mbar[0]));            // the peers' rows of this part are in
   } else {
@@ -375,9 +428,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   // CTA b / BPO, as its row A2 (b % BPO) + r
   constexpr int BPO = Sh::BPO;
   auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
-  float2 *cb[Sh::FULLP ? 1 : CL];                    // row 0 of CTA o's rows, this part
-  int cs[Sh::FULLP ? 1 : CL];                        // and their row stride
-  if constexpr (!Sh::FULLP) {
+  float2 *cb[Sh::SWAP ? 1 : CL];                     // row 0 of CTA o's rows, this part
+  int cs[Sh::SWAP ? 1 : CL];                         // and their row stride
+  if constexpr (!Sh::SWAP) {
 #pragma unroll
     for (int o = 0; o < CL; o++) {
       cb[o] = o == rank ? R + HW * rank : P + (o - (o > rank ? 1 : 0)) * HR * HW;
@@ -385,7 +438,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     }
   }
   auto at = [&](int b, int inner, int qq) -> float2 & {
-    if constexpr (Sh::FULLP) return P[(inner + A2 * b) * HW + pcol(qq)];
+    if constexpr (Sh::SWAP) return R[(inner + A2 * (b % BPO)) * RS + HW * (b / BPO) + pcol(qq)];
     else return cb[b / BPO][(inner + A2 * (b % BPO)) * cs[b / BPO] + pcol(qq)];
   };
   constexpr int QC = N1 / CL;
@@ -405,9 +458,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     const int qq = e % QC, cp = e / QC;
     float2 *col;
     int cst;
-    if constexpr (Sh::FULLP) {
-      col = P + A2 * cp * HW + pcol(qq);
-      cst = HW;
+    if constexpr (Sh::SWAP) {
+      col = R + A2 * (cp % BPO) * RS + HW * (cp / BPO) + pcol(qq);
+      cst = RS;
     } else {
       float2 *cbase = cb[0];
       cst = cs[0];
@@ -439,30 +492,23 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll
     for (int d = 0; d < B2; d++) at(d, cc, qq) = v[d];
   }
-  if constexpr (CL > 1) {
+  if constexpr (Sh::SWAP) {
+    __syncthreads();
+    swap_parts<NT, CL, HR, HW, RS, Sh::SWAP_ROUNDS>(R, rank, tid);    // the rows back to their owners
+  } else if constexpr (CL > 1) {
     // every peer's rows of this part -> back into that peer's row array
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     for (int e = tid; e < (CL - 1) * HR; e += NT) {
       const int pi = e / HR, j = e % HR;               // slot pi holds peer pi (< rank) or pi + 1
       const uint32_t peer = pi < rank ? pi : pi + 1;
-      const int slot = Sh::FULLP ? (int)peer : pi;
       bulk_to_peer(peer_addr(smem_addr(R + j * RS + HW * rank), peer),
-                   smem_addr(P + (slot * HR + j) * HW), Sh::HALF_BYTES,
+                   smem_addr(P + (pi * HR + j) * HW), Sh::HALF_BYTES,
                    peer_addr(smem_addr(&mbar[1]), peer));
     }
-    if constexpr (Sh::FULLP) {                       // slot rank -> own rows' part
-      constexpr int V4 = Sh::HALF_BYTES / 16;
-      for (int e = tid; e < HR * V4; e += NT) {
-        const int j = e / V4, x = e % V4;
-        reinterpret_cast<float4 *>(R + j * RS + HW * rank)[x] =
-            reinterpret_cast<const float4 *>(P + (rank * HR + j) * HW)[x];
-      }
-    }
-    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other parts of the own rows are back
+    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other half of the own rows is back
     cluster_arrive_release();                        // this CTA's incoming copies are complete
     if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
-    if constexpr (Sh::FULLP) __syncthreads();        // the own part copied back
   } else {
     __syncthreads();
   }
@@ -477,6 +523,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll
       for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
     }
+#pragma unroll 1
     for (int e = tid; e < HR * B1; e += NT) {
       const int j = e / B1;
       float2 *blk = R + j * RS + (A1 + 1) * bk;
@@ -505,9 +552,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int d = 0; d < B1; d++)
       g[jg * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
   }
-  // no CTA leaves while its shared memory may still be the source of a copy
-  // (a peer arrives only once all of its incoming copies are complete)
-  if constexpr (CL > 1) cluster_wait();
+  // CL = 2: no CTA leaves while its shared memory may still be the source of
+  // a copy (a peer arrives only once all of its incoming copies are
+  // complete); CL = 4 touches no peer's memory after the second swap's
+  // final barrier
+  if constexpr (Sh::PSLOTS > 0) cluster_wait();
 }
 
 template <int N1, int N2, int NT, int CL>
@@ -554,7 +603,7 @@ int slice_rf_threads(int n1, int n2, int cl)
     if (n1 == 128 && n2 == 96) return 256;
     if (n1 == 128 && n2 == 128) return 512;
   } else if (cl == 4) {
-    if (n1 == 256 && n2 == 192) return 512;   // 128 x 96 and 128 x 128 run faster on CL <= 2
+    if (n1 == 256 && n2 == 192) return 256;   // 128 x 96 and 128 x 128 run faster on CL <= 2
   }
   return 0;
 }
@@ -569,7 +618,7 @@ cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s)
     if (p.n1 == 128 && p.n2 == 96) return launch_rf<128, 96, 256, 2>(p, s);
     if (p.n1 == 128 && p.n2 == 128) return launch_rf<128, 128, 512, 2>(p, s);
   } else if (cl == 4) {
-    if (p.n1 == 256 && p.n2 == 192) return launch_rf<256, 192, 512, 4>(p, s);
+    if (p.n1 == 256 && p.n2 == 192) return launch_rf<256, 192, 256, 4>(p, s);
   }
   return cudaErrorInvalidValue;
 }
