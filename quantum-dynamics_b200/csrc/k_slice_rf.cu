@@ -391,7 +391,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   __syncthreads();
   // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
-#pragma unroll 1
   for (int e = tid; e < HR * B1; e += NT) {
     const int j = e / B1, c = e % B1;
     float2 *blk = R + j * RS + (A1 + 1) * c;
@@ -513,17 +512,19 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     __syncthreads();
   }
   // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
+  // The twiddle W^{-bk c} of slot c of block bk is applied in P6 while
+  // A1 <= 16 (A1 twiddles per thread, kept in registers); at A1 = 32 that
+  // would double the live registers of the 32-point DFT, so P7, whose thread
+  // holds one slot c of every block, applies it instead (B1 twiddles per
+  // thread).  The products are the same either way.
+  constexpr bool TW6 = A1 <= 16;
   {
-    // the twiddles stay in registers across items, except at A1 = 32, where
-    // they would double the live registers of the 32-point DFT
-    constexpr bool HOIST = A1 <= 16;
     const int bk = tid % B1;
-    float2 w[HOIST ? A1 : 1];
-    if constexpr (HOIST) {
+    float2 w[TW6 ? A1 : 1];
+    if constexpr (TW6) {
 #pragma unroll
       for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
     }
-#pragma unroll 1
     for (int e = tid; e < HR * B1; e += NT) {
       const int j = e / B1;
       float2 *blk = R + j * RS + (A1 + 1) * bk;
@@ -533,13 +534,18 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
       Dft<A1, +1>::run(v);
 #pragma unroll
       for (int c = 0; c < A1; c++) {
-        if constexpr (HOIST) blk[c] = c ? cmul(v[c], w[c]) : v[c];
-        else blk[c] = c ? cmul(v[c], cconj(__ldg(tw1 + bk * c))) : v[c];
+        if constexpr (TW6) blk[c] = c ? cmul(v[c], w[c]) : v[c];
+        else blk[c] = v[c];
       }
     }
   }
   __syncthreads();
   // P7: items (j, c'): slot c' of every block -> i = c' + A1 d', Rot/2, store
+  float2 w7[TW6 ? 1 : B1];                           // A1 = 32: W^{-b c'} of this thread's slot
+  if constexpr (!TW6) {
+#pragma unroll
+    for (int b = 0; b < B1; b++) w7[b] = cconj(__ldg(tw1 + b * (tid % A1)));
+  }
 #pragma unroll 2
   for (int e = tid; e < HR * A1; e += NT) {
     const int j = e / A1, c = e % A1, jg = j0 + j;
@@ -547,6 +553,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     float2 v[B1];
 #pragma unroll
     for (int b = 0; b < B1; b++) v[b] = R[j * RS + c + (A1 + 1) * b];
+    if constexpr (!TW6) {
+      if (c) {
+#pragma unroll
+        for (int b = 0; b < B1; b++) v[b] = cmul(v[b], w7[b]);
+      }
+    }
     Dft<B1, +1>::run(v);
 #pragma unroll
     for (int d = 0; d < B1; d++)
