@@ -434,8 +434,8 @@ LineParams line_params(qd_handle *h, bool f32)
 }
 
 // Autotuner of the complex64 l-space pass: time the fused slice kernel with
-// 1, 2 and 4 CTAs per slice, the register-FFT slice kernel on 1 and 2 CTAs
-// per slice and the split kernels on a scratch wavepacket and keep the
+// 1, 2 and 4 CTAs per slice, the register-FFT slice kernel on 1, 2 or 4
+// CTAs per slice (where built) and the split kernels on a scratch wavepacket and keep the
 // fastest; the choice is kept for later handles of the same shapes.
 // QD_SLICE_CLUSTER=0|1|2|4|8|9|10 forces a choice (8 = the register-FFT
 // kernel, 9 and 10 = the same on a 2- and a 4-CTA cluster).
