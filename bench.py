@@ -375,7 +375,7 @@ def run_ours(args):
     # column_tc_and_slice_rf4_c4_4runs_256x192x128.md under profiles/.
     traffic_ncu = {("c1", "column"): 16.89e6, ("c1", "lines"): 9.30e6,
                    ("c2j0", "column"): 373.7e6 / 32, ("c2j0", "lines"): 379.7e6 / 32,
-                   ("c4", "column"): 568.4e6 / 4, ("c4", "lines"): 365.3e6 / 4}
+                   ("c4", "column"): 568.4e6 / 4, ("c4", "lines"): 360.6e6 / 4}
     names = ["column", "lines", "flux_prep", "flux_accum", "crp"]
     per = {names[i]: kclass[i] for i in range(min(5, len(kclass)))}
     step_ms = t_max / K
