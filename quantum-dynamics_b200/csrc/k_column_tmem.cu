@@ -760,15 +760,16 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
       for (int l = 0; l < rows2; l++) put(b2, l, k, q2[(size_t)l * nth + k]); // B2: row l, K = k
     }
   }
+  // from the device's stream-ordered pool, like the handle's other buffers;
+  // a copy from pageable memory has read `img` when it returns
   void *d = nullptr;
-  if (cudaMalloc(&d, img.size() + sizeof(int)) != cudaSuccess) {
+  if (cudaMallocAsync(&d, img.size() + sizeof(int), s) != cudaSuccess) {
     cudaGetLastError();
     return QD_ERR_NOMEM;
   }
   if (cudaMemcpyAsync(d, img.data(), img.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemsetAsync((char *)d + img.size(), 0, sizeof(int), s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    cudaFree(d);
+      cudaMemsetAsync((char *)d + img.size(), 0, sizeof(int), s) != cudaSuccess) {
+    cudaFreeAsync(d, s);
     return QD_ERR_CUDA;
   }
   plan.nth = nth; plan.nl = nl; plan.S = S; plan.renorm = renorm ? 1 : 0;
@@ -797,16 +798,16 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(d);
+    cudaFreeAsync(d, s);
     plan.mats = nullptr;
     return QD_ERR_UNSUPPORTED;
   }
   return QD_OK;
 }
 
-void tc_plan_destroy(TcPlan &plan)
+void tc_plan_destroy(TcPlan &plan, cudaStream_t s)
 {
-  if (plan.mats) cudaFree(plan.mats);
+  if (plan.mats) cudaFreeAsync(plan.mats, s);
   plan.mats = nullptr;
 }
 

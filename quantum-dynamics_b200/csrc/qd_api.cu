@@ -19,6 +19,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -99,11 +100,47 @@ void radial_tables(const qd_radial &c, std::vector<double> &T, std::vector<doubl
   for (int i = 0; i < n; i++) I[i] = 1.0 / (m2 * c.r[i] * c.r[i]);
 }
 
+// Inf and NaN are the doubles whose exponent field is all ones.  The scan
+// ORs that test over the words without an early exit (so it stays a stream
+// of independent loads), and splits arrays of a million or more words over
+// up to eight host threads: the check reads the whole input once per call
+// and is bound by host memory bandwidth.
+bool finite_words(const double *a, size_t n)
+{
+  constexpr uint64_t E = 0x7ff0000000000000ull;
+  uint64_t b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+  size_t i = 0;
+  for (; i + 4 <= n; i += 4) {
+    uint64_t u[4];
+    std::memcpy(u, a + i, sizeof u);
+    b0 |= (u[0] & E) == E;
+    b1 |= (u[1] & E) == E;
+    b2 |= (u[2] & E) == E;
+    b3 |= (u[3] & E) == E;
+  }
+  for (; i < n; i++) {
+    uint64_t u;
+    std::memcpy(&u, a + i, sizeof u);
+    b0 |= (u & E) == E;
+  }
+  return (b0 | b1 | b2 | b3) == 0;
+}
+
 bool all_finite(const double *a, size_t n)
 {
-  for (size_t i = 0; i < n; i++)
-    if (!std::isfinite(a[i])) return false;
-  return true;
+  if (n < (size_t(1) << 20)) return finite_words(a, n);
+  const unsigned hw = std::thread::hardware_concurrency();
+  const unsigned nt = std::max(1u, std::min(8u, hw));
+  const size_t chunk = (n + nt - 1) / nt;
+  std::vector<char> ok(nt, 1);
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; t++) {
+    const size_t b = t * chunk, e = std::min(n, b + chunk);
+    if (b < e) th.emplace_back([&ok, a, b, e, t] { ok[t] = finite_words(a + b, e - b); });
+  }
+  ok[0] = finite_words(a, std::min(n, chunk));
+  for (std::thread &x : th) x.join();
+  return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
 }
 
 }  // namespace
@@ -218,10 +255,10 @@ struct qd_handle {
     for (void *p : allocs) cudaFreeAsync(p, st);
     if (d_norms) cudaFreeAsync(d_norms, st);
     if (d_flush) cudaFreeAsync(d_flush, st);
+    tc_plan_destroy(tc, st);
     if (st) cudaStreamSynchronize(st);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
     for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
-    tc_plan_destroy(tc);
     if (st) cudaStreamDestroy(st);
   }
 };

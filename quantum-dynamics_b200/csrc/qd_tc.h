@@ -21,7 +21,7 @@ struct TcPlan {
 // QD_ERR_UNSUPPORTED when the sizes are outside what the kernel handles.
 int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const *leg,
                    const int *nl_set, const double *w, cudaStream_t s);
-void tc_plan_destroy(TcPlan &plan);
+void tc_plan_destroy(TcPlan &plan, cudaStream_t s);   // stream-ordered free
 // Device status word: 0 = ok, non-zero = a bounded wait in the kernel expired.
 int *tc_status_ptr(const TcPlan &plan);
 cudaError_t launch_column_tc(const TcPlan &plan, const ColumnParams &p, int mode,

@@ -66,6 +66,23 @@ def test_invalid_input_rejected_before_device_work(qdlib, mutate, code, msg):
     assert not h.value
 
 
+@pytest.mark.parametrize("where", ["pot", "psi"])
+def test_nonfinite_found_in_large_inputs(qdlib, where):
+    # 128 x 128 x 64 points: the finiteness scan splits the arrays over host
+    # threads; a NaN or Inf in the last part is still found
+    d = S.build_case("h+h2", 128, 128, 64, m=63, total_steps=1, n_energies=5,
+                     n_gradient_points=5)
+    if where == "pot":
+        d.pot[-1, -1, -1] = np.nan
+    else:
+        d.psi[-1, -1, -2] = complex(0.0, -np.inf)
+    c = _abi.to_c(d)
+    h = C.c_void_p()
+    assert qdlib.qd_create(C.byref(c), C.byref(h)) == _abi.QD_ERR_NONFINITE
+    assert where.encode() in qdlib.qd_last_error()
+    assert not h.value
+
+
 def test_unsupported_fft_size(qdlib):
     d = S.build_case("h+h2", 14, 12, 8, m=6, total_steps=1, n_energies=5, n_gradient_points=5)
     c = _abi.to_c(d)
