@@ -444,6 +444,25 @@ def test_cs_mixed_batch(slice_kind, monkeypatch):
         assert np.abs(crp32 - crp64).max() < FP32_CRP_ABS
 
 
+def test_fp32_cs_batch_equals_individual_runs():
+    # centrifugal-sudden blocks of different K in one complex64 batch (one
+    # potential table and one angular basis per run) against each block
+    # propagated alone
+    base = _cs_base(64, 64, 32, steps=40)
+    runs = [S.cs_case(base, *c) for c in [(0, 0, 0, 0), (5, 1, 0, 1), (10, 2, 0, 2)]]
+    for r in runs:
+        r.options.precision = QD_PREC_FP32
+    single = [S.copy_case(r) for r in runs]
+    batch = [S.copy_case(r) for r in runs]
+    for d in single:
+        TimeEvolutionMexCUDA(d)
+    TimeEvolutionMexCUDA(batch)
+    for a, b in zip(single, batch):
+        if np.abs(a.psi).max() > 0:
+            assert rel(b.psi, a.psi) < 1e-5
+        assert np.abs(b.CRP.CRP - a.CRP.CRP).max() < 1e-5 * max(1.0, np.abs(a.CRP.CRP).max())
+
+
 @pytest.mark.parametrize("j0,v0,K", [(0, 0, 0), (2, 0, 0), (0, 1, 0), (2, 0, 1), (1, 0, 2)])
 def test_initial_state_on_gpu(j0, v0, K):
     # the GPU builder (sinc-DVR by parallel Jacobi, packet, eta^2) against the
