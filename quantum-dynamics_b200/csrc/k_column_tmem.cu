@@ -593,9 +593,14 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     if (t.renorm) so = n_o > 0.f ? sqrtf(target / n_o) : 1.f;
     else so = (slow || mode == COL_HEAD) ? 1.f : ddv;
     float *dst = ldst + (size_t)run * nl * stride + (size_t)c0 * stride + 2 * q + comp;
+    if (EX && (!MS || c0 + H <= nlr)) {         // every order of this column group is stored
 #pragma unroll
-    for (int u = 0; u < H; u++)
-      if ((EX || qok) && (EX && !MS ? true : c0 + u < nlr)) dst[u * stride] = ov[u] * so;
+      for (int u = 0; u < H; u++) dst[u * stride] = ov[u] * so;
+    } else {
+#pragma unroll
+      for (int u = 0; u < H; u++)
+        if ((EX || qok) && c0 + u < nlr) dst[u * stride] = ov[u] * so;
+    }
     tc_fence_before();
   }
 #undef QD_PREFETCH_A
