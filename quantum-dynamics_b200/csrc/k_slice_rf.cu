@@ -2,8 +2,8 @@
 //     psi_l <- Rot(dt/2) IFFT2 [exp(-i(T1+T2)dt)/(n1 n2)] FFT2 Rot(dt/2) psi_l
 // (evolution_dt, timeEvol.C:625-635; the FFTW 2-D DFT pair of
 // fftwinterface.C:70-76; phase tables timeEvol.C:465-517), one l-slice per
-// CTA (or per 2-CTA cluster), with every 1-D transform done as two register
-// passes.
+// CTA (or per 2- or 4-CTA cluster), with every 1-D transform done as two
+// register passes.
 //
 // A length N = A*B transform (n = a + A b, k = c + B d) is
 //   pass 1, one item per a:  B-point DFT over b in registers, times W_N^{a c}
@@ -37,6 +37,10 @@
 // row passes and half the columns, over all rows, for the column passes; the
 // two transposes between them are bulk shared-memory-to-shared-memory copies
 // of whole row halves, so no pass touches the other CTA's memory itself.
+// A 256 x 192 slice (384 KB) runs on a 4-CTA cluster, a quarter of the rows
+// and of the columns per CTA; its transposes swap row parts between the CTAs
+// in place (registers, cluster barrier, remote stores), so each CTA holds
+// only its own 101 KB of rows and two clusters' CTAs share an SM.
 //
 // The 6-, 12-, 16-, 24- and 32-point DFTs are P x Q compositions whose
 // internal twiddles are compensated constants (value + residual), like the
