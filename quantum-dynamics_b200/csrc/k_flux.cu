@@ -109,20 +109,35 @@ __global__ void __launch_bounds__(256) k_flux_gemm(AccumParams p)
     }
     __syncthreads();                            // buffer free for the stage after next
   }
+  // phi += acc, two energy rows at a time: their eight loads are all issued
+  // before any of their stores (a store between two loads would make each
+  // load wait for the one before, since phi and dphi may alias as far as the
+  // compiler knows)
+  auto at = [&](int i, int j) -> double2 * {
+    const int e = e0 + te + 16 * i, c = tc + 16 * j, q = q0 + (c % GQ);
+    if (e >= p.ne || q >= p.nq) return nullptr;
+    return (c < GQ ? p.fai : p.dfai) + ((size_t)run * p.ne + e) * p.nq + q;
+  };
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int e = e0 + te + 16 * i;
-    if (e >= p.ne) continue;
+  for (int h = 0; h < 4; h += 2) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = tc + 16 * j, q = q0 + (c % GQ);
-      if (q >= p.nq) continue;
-      double2 *dst = (c < GQ ? p.fai : p.dfai) + ((size_t)run * p.ne + e) * p.nq + q;
-      double2 f = *dst;
-      f.x += acc[i][j].x;
-      f.y += acc[i][j].y;
-      *dst = f;
-    }
+    for (int i = h; i < h + 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const double2 *src = at(i, j);
+        if (src) {
+          const double2 f = *src;
+          acc[i][j].x += f.x;
+          acc[i][j].y += f.y;
+        }
+      }
+#pragma unroll
+    for (int i = h; i < h + 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        double2 *dst = at(i, j);
+        if (dst) *dst = acc[i][j];
+      }
   }
 }
 

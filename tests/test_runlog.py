@@ -74,5 +74,6 @@ def test_logged_propagation_on_gpu():
     assert [r["step"] for r in recs] == [10, 20, 30]
     assert recs[-1]["norm"][0] == allnorms[-1]
     assert recs[1]["absorbed"][0] == allnorms[9] - allnorms[19]
-    assert recs[-1]["energies"]["total"] == e[3]
+    # energies are FP64 sums whose order of accumulation may differ between calls
+    assert abs(recs[-1]["energies"]["total"] - e[3]) <= 1e-12 * abs(e[3])
     assert all(r["grid_pt_steps_per_s"] > 0 for r in recs)
