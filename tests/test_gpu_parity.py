@@ -288,6 +288,28 @@ def test_fp32_c1_full_run_within_pe_budget():
     assert np.abs(out[QD_PREC_FP32][1] - out[QD_PREC_FP64][1]).max() < 1e-3
 
 
+def test_fp32_c4_block_within_pe_budget():
+    # one centrifugal-sudden block (J = 8, K = 2, n_j = 126) on the full C4 grid
+    # 256 x 192 x 128 over 3000 steps: complex64 (tensor-core column pass at
+    # n_theta = 128 with streamed operand images, 256 x 192 slices) against the
+    # FP64 plain form, max |dP(E)| <= 1e-3 where eta^2 > 1e-3 max eta^2
+    base = S.build_case("f+h2", 256, 192, 128, m=127, r=(0.4, 8.0), total_steps=3000)
+    run = S.cs_case(base, 8, 2, 0, 3)
+    out = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        d = S.copy_case(run)
+        d.options.precision = prec
+        with Propagator(d) as p:
+            p.propagate(3000)
+            out[prec] = (p.crp(), p.norms(3000), p.psi())
+    eta = run.CRP.eta_sq
+    sel = eta > 1e-3 * eta.max()
+    dP = np.abs(out[QD_PREC_FP32][0] - out[QD_PREC_FP64][0])[sel].max()
+    assert dP < FP32_CRP_ABS, dP
+    assert np.abs(out[QD_PREC_FP32][1] - out[QD_PREC_FP64][1]).max() < 1e-3
+    assert rel(out[QD_PREC_FP32][2], out[QD_PREC_FP64][2]) < 1e-3
+
+
 def _three_runs(prec, steps=25):
     # same F + H2 grid, different initial states (v0, j0) -> different psi,
     # energies and eta^2; the potential table is shared
