@@ -310,6 +310,29 @@ def test_fp32_c4_block_within_pe_budget():
     assert rel(out[QD_PREC_FP32][2], out[QD_PREC_FP64][2]) < 1e-3
 
 
+def test_fp32_c2_cs_blocks_within_pe_budget():
+    # two centrifugal-sudden blocks of the C2 batch (J = 5, K = 1 and J = 10,
+    # K = 2) on its 128 x 96 x 64 grid, in one batch, over 3000 steps (the
+    # packets are absorbed): complex64 against the FP64 plain form, max |dP(E)|
+    # <= 1e-3 where eta^2 > 1e-3 max eta^2
+    base = S.build_case("f+h2", 128, 96, 64, m=63, r=(0.4, 8.0), total_steps=3000)
+    runs = [S.cs_case(base, 5, 1, 0, 1), S.cs_case(base, 10, 2, 0, 2)]
+    out = {}
+    for prec in (QD_PREC_FP64, QD_PREC_FP32):
+        rs = [S.copy_case(r) for r in runs]
+        for r in rs:
+            r.options.precision = prec
+        with Propagator(rs) as p:
+            p.propagate(3000)
+            out[prec] = [(p.crp(i), p.norms(3000, i)) for i in range(len(rs))]
+    for r, (c64, n64), (c32, n32) in zip(runs, out[QD_PREC_FP64], out[QD_PREC_FP32]):
+        assert np.abs(c64).max() > 0.1                 # both blocks carry a packet
+        eta = r.CRP.eta_sq
+        sel = eta > 1e-3 * eta.max()
+        assert np.abs(c32 - c64)[sel].max() < FP32_CRP_ABS
+        assert np.abs(n32 - n64).max() < 1e-3
+
+
 def _three_runs(prec, steps=25):
     # same F + H2 grid, different initial states (v0, j0) -> different psi,
     # energies and eta^2; the potential table is shared
