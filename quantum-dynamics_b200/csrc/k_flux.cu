@@ -23,7 +23,7 @@ __global__ void k_flux_prep(FluxParams p)
   if (q < p.nruns * p.nth * p.n1) flux_point<C>(p, q);
 }
 
-constexpr int TMAX = 128;      // max steps per chunk
+constexpr int TMAX = FLUX_CHUNK;   // max steps per chunk
 
 // phase[run][e][t] = dt e^{i E_e (t0 + t + 1) dt} of this chunk, FP64
 __global__ void __launch_bounds__(256) k_flux_phase(AccumParams p)

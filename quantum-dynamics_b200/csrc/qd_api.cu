@@ -57,7 +57,7 @@ int set_err(int code, const char *fmt, ...)
     if (rc_ != QD_OK) return rc_; \
   } while (0)
 
-constexpr int QD_RING = 100;   // steps per E-accumulation chunk
+constexpr int QD_RING = FLUX_CHUNK;   // steps per E-accumulation chunk
 
 bool radix_plan(int n, FftPlan &pl)
 {
@@ -894,7 +894,7 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     TRY(h->alloc(h->d_ring_g, nq * QD_RING * nruns));
     TRY(h->alloc(h->d_fai, nq * h->ne * nruns));
     TRY(h->alloc(h->d_dfai, nq * h->ne * nruns));
-    TRY(h->alloc(h->d_phase, (size_t)h->ne * 128 * nruns));
+    TRY(h->alloc(h->d_phase, (size_t)h->ne * FLUX_CHUNK * nruns));
     CU(cudaMemsetAsync(h->d_fai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
     CU(cudaMemsetAsync(h->d_dfai, 0, sizeof(double2) * nq * h->ne * nruns, h->st));
     TRY(h->alloc(h->d_energies, (size_t)h->ne * nruns));

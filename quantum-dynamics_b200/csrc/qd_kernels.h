@@ -208,6 +208,9 @@ cudaError_t launch_setup_tables_fp32(int n1, int n2, int nth, int nl, double dt,
                                      cudaStream_t s);
 // fused slice kernel (FP32): CTAs per slice it can run with for these sizes
 // (0 if none), its launch, and the smem bytes it needs
+// steps of flux history accumulated into phi_E by one GEMM launch (the ring
+// of surface rows and the e^{iEt} table hold that many steps)
+constexpr int FLUX_CHUNK = 250;
 constexpr int SLICE_RF = 8;    // LineParams::cluster value of the register-FFT slice kernel
 constexpr int SLICE_RF2 = 9;   // the same on a 2-CTA cluster per slice
 constexpr int SLICE_RF4 = 10;  // the same on a 4-CTA cluster per slice
