@@ -202,6 +202,7 @@ struct qd_handle {
   bool last_finalized = true;     // flux/norm of the last step already taken
   int32_t steps = 0;
   std::vector<double> norms_host;
+  bool norm_guard = true;         // every run has n_l <= n_theta: a step cannot raise the norm
   bool profiling = false;
   std::vector<double> kernel_ms;
   void *d_flush = nullptr;        // L2 flush buffer of qd_propagate_timed
@@ -661,12 +662,25 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
     }
     *device_ms = tot;
   }
+  // unitarity guard: with n_l <= n_theta the Legendre pair is an isometry
+  // followed by a projection, so a step only loses norm (there and through
+  // the absorbers), and a norm above the run's previous one by more than
+  // rounding (FP64 1e-8, complex64 1e-4 relative) means a corrupted state or
+  // an absorber above 1.  With more angular functions than quadrature nodes
+  // the reference's transform pair itself may raise the norm: no guard.
   const double scale = h->data->r1.dr * h->data->r2.dr;
+  const double grow_tol = h->prec == QD_PREC_FP64 ? 1e-8 : 1e-4;
   for (long s = 0; s < (long)n * R; s++) {
     const double v = nb[s] * scale;
+    const int step = h->steps - n + (int)(s / R) + 1, run = (int)(s % R);
     if (!std::isfinite(v))
-      return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d (run %d)",
-                     h->steps - n + (int)(s / R) + 1, (int)(s % R));
+      return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d (run %d)", step, run);
+    if (h->norm_guard && h->norms_host.size() >= (size_t)R) {
+      const double pv = h->norms_host[h->norms_host.size() - R];   // same run, one step earlier
+      if (v > pv * (1.0 + grow_tol))
+        return set_err(QD_ERR_NONFINITE, "wavepacket norm grew from %.17g to %.17g at step %d (run %d):"
+                       " a step only loses norm, through the absorbers", pv, v, step, run);
+    }
     h->norms_host.push_back(v);
   }
   return QD_OK;
@@ -758,6 +772,7 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     h->run_k.push_back(a.cs.K);
     h->run_nl.push_back(nlr);
     h->nl = std::max(h->nl, nlr);
+    h->norm_guard = h->norm_guard && nlr <= a.theta.n;
     h->jrows = std::max(h->jrows, a.cs.K + nlr);
     any_k = any_k || a.cs.K != 0;
   }

@@ -91,6 +91,20 @@ def test_fp64_unitary_without_absorbers():
     assert np.abs(n - n[0]).max() < 1e-12 * n[0]
 
 
+@pytest.mark.parametrize("prec", [QD_PREC_FP64, QD_PREC_FP32])
+def test_norm_growth_is_reported(prec):
+    # an absorber above 1 (a host-side input error) makes the norm grow; the
+    # host-side unitarity guard stops the call with QD_ERR_NONFINITE
+    from qd_b200._abi import QdError, QD_ERR_NONFINITE
+    d = S.build_case("h+h2", 32, 24, 12, m=11, total_steps=5, n_energies=5,
+                     n_gradient_points=5, precision=prec)
+    d.dump1.dump = np.full_like(d.dump1.dump, 1.01)
+    with pytest.raises(QdError) as exc:
+        TimeEvolutionMexCUDA(d)
+    assert exc.value.code == QD_ERR_NONFINITE
+    assert "grew" in str(exc.value)
+
+
 def test_handle_split_calls_equal_one_call():
     base = S.build_case("f+h2", 32, 32, 16, m=15, total_steps=30, n_energies=9,
                         n_gradient_points=5)
