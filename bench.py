@@ -1,24 +1,31 @@
 """Benchmark: grid-point * steps / s of the split-operator propagator.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0|c2|c2j0|c3|c4]
+                    [--workload c4|c2|c2j0|c1|c0|c3]
 
-Workload (default c1): F + H2, J = 0, extended-LEPS surface on a
-128 x 128 x 64 Jacobi grid (n_l = 64), complex64 wavefunction with the
-3xTF32 Legendre GEMM and FP64 flux-to-P(E) accumulation, dt = 10 au; P(E)
-on 241 energies, 11-point flux stencil.  A step is one split-operator step
-of the whole grid (1,048,576 grid points) including the flux capture.
+Workload (default c4, the largest single-GPU configuration): a batch of 32
+F + H2 centrifugal-sudden blocks (J = 0-30, K <= 3, n_j = 128 - K) on a
+256 x 192 x 128 Jacobi grid, 201,326,592 grid points, complex64 wavefunction
+with the 3xTF32 Legendre GEMM and FP64 flux-to-P(E) accumulation, dt = 10 au,
+P(E) on 241 energies per block.  c2 is the 64-block batch on 128 x 96 x 64,
+c1 one F + H2 J = 0 run on 128 x 128 x 64.  A step is one split-operator
+step of every grid point of the workload, including the flux capture.
 
 value   device time (CUDA events on the library's stream) of K steps after
         W warm-up steps, L2 flushed before every step outside the timed spans
         (256 MiB written, then read back, so the step meets neither its own
         data nor dirty lines in L2); whole-job = sum over ranks' points / max
         rank time.
+fp64_plain  the plain FP64 form's rate on the same workload, timed the same
+        way, and value / that rate.
 e2e     the drop-in entry point qd_time_evolution on host arrays for the
         same K steps: upload of pot and psi, table set-up, the K steps, P(E)
         and the download of psi and P(E), wall clock.
+clocks  SM clock and clock-event reasons sampled through NVML every 5 ms
+        during the timed region.
 Multi-GPU: independent replicas (one propagation per rank, weak scaling,
-no data-path collective); rank times are reduced with MAX.
+no data-path collective); rank times are reduced with MAX through the host
+group of qd_b200.hostgroup.
 
 --impl reference times the reference's own CPU propagator (common/timeEvol.C,
 built in oracle/_ref against the shims) on the host cores for a bounded
@@ -26,9 +33,7 @@ sample of steps of the same workload.
 """
 import argparse
 import json
-import math
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -153,60 +158,84 @@ def build_workload(name, precision, runs=64):
     return data, desc
 
 
-class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+class GpuClock:
+    """SM clock and clock-event reasons of this process's GPU, sampled every
+    `period` seconds by a thread through NVML (read-only queries) while the
+    GPU phase of the benchmark runs; `mark` records the wall-clock bounds of
+    the timed region, whose samples the summary uses (all samples of the
+    phase when fewer than three fall inside it, which it then says)."""
+    BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+            "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, local, period=0.005):
+        self.local = local
+        self.period = period
+        self.samples = []          # (t, sm_mhz, reasons bitmask)
+        self.marks = {}
+        self.max_mhz = None
+        self.nv = None
+        self._stop = False
+
+    def _handle(self, nv):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x.strip() for x in vis.split(",") if x.strip()] if vis else []
+        if ids and self.local < len(ids):
+            tok = ids[self.local]
+            if tok.isdigit():
+                return nv.nvmlDeviceGetHandleByIndex(int(tok))
+            return nv.nvmlDeviceGetHandleByUUID(tok)
+        return nv.nvmlDeviceGetHandleByIndex(self.local)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
-        except Exception:
-            self.proc = None
+        except Exception as e:          # no NVML: the line says so
+            self.error = str(e)
+            self.nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self._stop:
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def mark(self, name):
+        self.marks[name] = time.perf_counter()
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self._stop = True
+        if self.nv:
+            self.t.join(timeout=2)
             try:
-                self.proc.wait(timeout=5)
+                self.nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"],
+                    "source": getattr(self, "error", "no samples")}
+        t0, t1 = self.marks.get("timed_begin"), self.marks.get("timed_end")
+        inside = [x for x in self.samples if t0 is not None and t1 is not None and t0 <= x[0] <= t1]
+        use, window = (inside, "timed region") if len(inside) >= 3 else \
+            (self.samples, "whole GPU phase (warm-up, timed, profiled and unflushed steps)")
+        reasons = sorted(n for n, b in self.BITS.items() if any(x[2] & b for x in use))
+        return {"sm_mhz": float(np.median([x[1] for x in use])), "sm_max_mhz": self.max_mhz,
+                "sm_min_mhz": float(min(x[1] for x in use)), "reasons": reasons,
+                "samples": len(use), "samples_timed_region": len(inside), "window": window,
+                "source": f"NVML every {self.period * 1e3:.0f} ms"}
 
 
 def cpu_reference_rate(data, max_seconds, steps_cap=None):
@@ -241,25 +270,19 @@ def cpu_reference_rate(data, max_seconds, steps_cap=None):
     return pts * n / dt, info
 
 
-def dist_setup(n_gpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+def group_setup():
+    """Rank, world, local GPU and the host group of this process (one process
+    per GPU, launched by torchrun or alone); the group gives the barrier and
+    the max over ranks, with no device library involved."""
+    from qd_b200.hostgroup import FileGroup
+    g = FileGroup.from_env()
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        return rank, world, local, dist
-    return rank, world, local, None
+    return g.rank, g.world, local, g
 
 
 def run_reference(args):
-    rank, world, local, dist = dist_setup(args.gpus)
+    rank, world, local, grp = group_setup()
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
         return
     data, desc = build_workload(args.workload, 0, args.runs)
     budget = float(os.environ.get("QD_REF_SECONDS", "60"))
@@ -276,15 +299,73 @@ def run_reference(args):
             "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+
+
+KCLASS = ["column", "lines", "flux_prep", "flux_accum", "crp"]
+
+
+def device_phase(data, prec, K, W, clk=None, profile=True):
+    """Device-resident rate of one precision: W warm-up steps, then K timed
+    steps (CUDA events on the library's stream, L2 flushed before every step
+    outside the timed spans); then, untimed for the rate, a profiled run
+    (per-kernel-class CUDA events), K plain steps (no per-step events, no
+    flush: the library's own launch chain) and K unflushed timed steps."""
+    from qd_b200 import Propagator
+    from qd_b200 import _abi
+    from qd_b200.timeevolution import kernel_launch_count
+    import ctypes as C
+    d = copy_workload(data)
+    for r in as_runs(d):
+        r.options.precision = prec
+    out = {}
+    with Propagator(d) as p:
+        p.propagate_timed(W, FLUSH_BYTES)
+        l0 = kernel_launch_count()
+        if clk:
+            clk.mark("timed_begin")
+        out["ms"] = p.propagate_timed(K, FLUSH_BYTES)
+        if clk:
+            clk.mark("timed_end")
+        out["launches"] = kernel_launch_count() - l0
+        if profile:
+            lib = _abi.lib()
+            lib.qd_set_profiling(p._h, 1)
+            p.propagate(min(K, 400))
+            buf = (C.c_double * 10)()
+            nw = C.c_int32()
+            lib.qd_kernel_times(p._h, buf, 10, C.byref(nw))
+            lib.qd_set_profiling(p._h, 0)
+            kc = list(buf)[:nw.value]
+            out["kclass_ms"] = {KCLASS[i]: kc[i] for i in range(min(5, len(kc)))}
+            t0 = time.perf_counter()
+            p.propagate(K)
+            out["plain_s"] = time.perf_counter() - t0
+            out["ms_warm"] = p.propagate_timed(K, 0)
+    return out
+
+
+def roofline_entry(name, alg_bytes, ms, peak, peak_kind, traffic):
+    ach = alg_bytes / (ms * 1e-3) / 1e9 if ms and ms > 0 else None
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak if ach else None,
+            "traffic": traffic, "traffic_unit": "DRAM bytes read + written per launch (ncu)",
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": ms}
+
+
+# DRAM bytes (read + write) per launch of the column and l-space kernels
+# from one ncu capture each (cold caches: ncu flushes them before every
+# captured launch); the batch figures were captured on fewer runs and scale
+# with the runs (traffic_runs).  The ncu summaries under profiles/ give the
+# commands that made them.
+TRAFFIC_NCU = {("c1", "column"): (16.89e6, 1), ("c1", "lines"): (9.30e6, 1),
+               ("c2j0", "column"): (373.7e6, 32), ("c2j0", "lines"): (379.7e6, 32),
+               ("c4", "column"): (568.4e6, 4), ("c4", "lines"): (360.6e6, 4)}
 
 
 def run_ours(args):
-    rank, world, local, dist = dist_setup(args.gpus)
-    from qd_b200 import QD_PREC_FP32, QD_PREC_FP64, Propagator, TimeEvolutionMexCUDA
-    from qd_b200 import systems as S
-    from qd_b200.timeevolution import kernel_launch_count, set_device
+    rank, world, local, grp = group_setup()
+    from qd_b200 import QD_PREC_FP32, QD_PREC_FP64, TimeEvolutionMexCUDA
+    from qd_b200.timeevolution import set_device
     set_device(local)
     prec = QD_PREC_FP64 if args.fp64 else QD_PREC_FP32
     data, desc = build_workload(args.workload, prec, args.runs)
@@ -292,73 +373,54 @@ def run_ours(args):
     pts = grid_points(data)
     K, W = args.steps, args.warmup
 
-    # --- device-resident throughput -------------------------------------------------
-    d = copy_workload(data)
-    with Propagator(d) as p:
-        p.propagate_timed(W, FLUSH_BYTES)
-        if dist:
-            dist.barrier()
-        l0 = kernel_launch_count()
-        with ClockSampler(local) as clk:
-            ms = p.propagate_timed(K, FLUSH_BYTES)
-        launches = kernel_launch_count() - l0
-        # per-kernel-class device time (separate, profiled run)
-        from qd_b200 import _abi
-        import ctypes as C
-        lib = _abi.lib()
-        lib.qd_set_profiling(p._h, 1)
-        p.propagate(min(K, 400))
-        buf = (C.c_double * 10)()
-        nw = C.c_int32()
-        lib.qd_kernel_times(p._h, buf, 10, C.byref(nw))
-        lib.qd_set_profiling(p._h, 0)
-        kclass = list(buf)[:nw.value]
-        # unflushed (L2-resident steady state), for context
-        ms_warm = p.propagate_timed(K, 0)
-    t_max = ms
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    # --- device-resident throughput, clocks sampled over the whole GPU phase ------------
+    grp.barrier()
+    with GpuClock(local) as clk:
+        dev = device_phase(data, prec, K, W, clk)
+    t_max = grp.max(dev["ms"])
     value = pts * K * world / (t_max * 1e-3)
 
+    # --- the plain FP64 form on the same workload (the north-star ratio) ---------------
+    fp64 = None
+    if not args.fp64 and not args.no_fp64_arm:
+        grp.barrier()
+        d64 = device_phase(data, QD_PREC_FP64, K, W, profile=False)
+        t64 = grp.max(d64["ms"])
+        v64 = pts * K * world / (t64 * 1e-3)
+        fp64 = {"value": v64, "unit": METRIC, "ms_per_step": t64 / K,
+                "ratio": value / v64, "steps": K,
+                "what": "the plain form (complex128 wavepacket, FP64 everywhere) on the same "
+                        "workload and GPU, timed the same way"}
+
     # --- end to end through the drop-in entry point -------------------------------
-    # five repetitions, median reported (each a full call: upload, set-up, K steps,
-    # P(E), download)
+    # each a full call: upload, set-up, K steps, P(E), download; median reported
+    nrep = 5 if pts * 16 < (1 << 30) else 3
     reps = []
-    for _ in range(5):
+    for _ in range(nrep):
         e = copy_workload(data)
         for r in as_runs(e):
             r.time.total_steps = K
             r.time.steps = 0
-        if dist:
-            dist.barrier()
+        grp.barrier()
         t0 = time.perf_counter()
         TimeEvolutionMexCUDA(e)
         reps.append(time.perf_counter() - t0)
-    e2e_s = float(np.median(reps))
-    if dist:
-        import torch
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = grp.max(float(np.median(reps)))
     h2d = sum(r.pot.nbytes + r.psi.nbytes for r in runs) + runs[0].theta.legendre.nbytes
     d2h = sum(r.psi.nbytes + r.CRP.CRP.nbytes for r in runs)
     e2e = {"value": pts * K * world / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
            "seconds": e2e_s, "seconds_each": reps,
-           "entry_point": "qd_time_evolution (TimeEvolutionMexCUDA), median of 5 calls"}
+           "entry_point": f"qd_time_evolution (TimeEvolutionMexCUDA), median of {nrep} calls"}
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
         return
 
-    # --- roofline of the dominant kernel class ----------------------------------------
+    # --- roofline of the two hot kernels ------------------------------------------------
     peak, peak_kind = load_peaks()
     r0 = runs[0]
     nl, nth = int(r0.theta.m) + 1, int(r0.theta.n)
+    nl = max(int(r.theta.m) + 1 for r in runs)
     n12 = int(r0.r1.n) * int(r0.r2.n) * len(runs)
     cb = 16 if args.fp64 else 8        # bytes per complex
     shared_pot = all(np.array_equal(r.pot, r0.pot) for r in runs[1:])
@@ -367,30 +429,25 @@ def run_ours(args):
         "column": n12 * 2 * nl * cb + int(r0.r1.n) * int(r0.r2.n) * nth * cb * npot,
         "lines": n12 * nl * 2 * cb,
     }
-    # DRAM bytes (read + write) per launch from one ncu capture each (cold caches:
-    # ncu flushes them before every captured launch); the batch figures were
-    # captured on 32 (c2j0) or 4 (c4) runs and scale with the runs.  Sources: the
-    # ncu summaries column_tc_and_slice_rf2_c1_128x128x64.md,
-    # column_tc_and_slice_rf_batch32_128x96x64.md and
-    # column_tc_and_slice_rf4_c4_4runs_256x192x128.md under profiles/.
-    traffic_ncu = {("c1", "column"): 16.89e6, ("c1", "lines"): 9.30e6,
-                   ("c2j0", "column"): 373.7e6 / 32, ("c2j0", "lines"): 379.7e6 / 32,
-                   ("c4", "column"): 568.4e6 / 4, ("c4", "lines"): 360.6e6 / 4}
-    names = ["column", "lines", "flux_prep", "flux_accum", "crp"]
-    per = {names[i]: kclass[i] for i in range(min(5, len(kclass)))}
-    step_ms = t_max / K
+    per = dev.get("kclass_ms", {})
+    kernels = {}
+    for k in ("column", "lines"):
+        tr = None
+        if not args.fp64 and (args.workload, k) in TRAFFIC_NCU:
+            b, nr = TRAFFIC_NCU[(args.workload, k)]
+            tr = b * len(runs) / nr
+        kernels[k] = roofline_entry(k, alg[k], per.get(k), peak, peak_kind, tr)
     dom = max(("column", "lines"), key=lambda k: per.get(k, 0.0))
-    dom_ms = per.get(dom, float("nan"))
-    achieved = alg[dom] / (dom_ms * 1e-3) / 1e9 if dom_ms and dom_ms > 0 else None
-    tr = traffic_ncu.get((args.workload, dom)) if not args.fp64 else None
-    if tr is not None and args.workload in ("c2j0", "c4"):
-        tr *= len(runs)
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None,
-                "traffic": tr, "traffic_unit": "bytes per launch (ncu)",
-                "alg_bytes_per_launch": alg[dom], "avg_launch_ms": dom_ms,
-                "kernel_class_ms": per}
+    roofline = dict(kernels[dom])
+    roofline["kernels"] = {k: {x: kernels[k][x] for x in ("achieved", "frac", "avg_launch_ms",
+                                                          "alg_bytes_per_launch", "traffic")}
+                           for k in kernels}
+    roofline["kernel_class_ms"] = per
+    step_ms = t_max / K
+    step_bytes = 36 if not args.fp64 else 72
+    roofline["whole_step"] = {"alg_bytes_per_grid_pt_step": step_bytes,
+                              "achieved": pts * step_bytes / (step_ms * 1e-3) / 1e9,
+                              "frac": pts * step_bytes / (step_ms * 1e-3) / 1e9 / peak}
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -405,15 +462,58 @@ def run_ours(args):
             "config": {"workload": desc, "grid_points": pts,
                        "precision": "FP64 plain" if args.fp64 else
                        "complex64 + 3xTF32 Legendre + FP64 flux accumulation",
-                       "l2": "flushed before every step (256 MiB write, then read back so no dirty lines remain; outside the timed spans)",
+                       "l2": "flushed before every step (256 MiB written, then read back so "
+                             "no dirty lines remain; outside the timed spans)",
                        "parallelism": f"replicas x{world}"},
-            "value_l2_resident": pts * K / (ms_warm * 1e-3),
+            "value_l2_resident": pts * K / (dev["ms_warm"] * 1e-3),
+            "value_plain_call": pts * K / dev["plain_s"],
+            "fp64_plain": fp64,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clk.summary(), "gpu_launches": launches, **EXTRA,
+            "clocks": clk.summary(), "gpu_launches": dev["launches"], **EXTRA,
             "pe_curves_per_hour_e2e": curves_per_hour}
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+
+
+def run_compare_libs(args):
+    """This library's column and l-space passes against the same passes on
+    cuFFT and cuBLAS (the reference GPU code's design), per step of the
+    workload, on one GPU.  Prints one JSON line."""
+    from qd_b200 import QD_PREC_FP32, QD_PREC_FP64
+    from qd_b200 import libcompare as LC
+    from qd_b200.timeevolution import set_device
+    set_device(0)
+    LC.set_device(0)
+    data, desc = build_workload(args.workload, QD_PREC_FP32, args.runs)
+    runs = as_runs(data)
+    r0 = runs[0]
+    n1, n2, nth = int(r0.r1.n), int(r0.r2.n), int(r0.theta.n)
+    nl = max(int(r.theta.m) + 1 for r in runs)
+    K = max(args.steps, 10)
+    ours = {}
+    for name, prec in (("complex64", QD_PREC_FP32), ("fp64", QD_PREC_FP64)):
+        dev = device_phase(data, prec, K, 3)
+        ours[name] = {"column_ms": dev["kclass_ms"]["column"],
+                      "lspace_ms": dev["kclass_ms"]["lines"], "step_ms": dev["ms"] / K}
+    lib = {"lspace_cufft_c2c_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), False, K),
+           "lspace_cufft_z2z_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), True, K)}
+    for c in LC.COMPUTE:
+        lib[f"column_cublas_{c}_ms"] = LC.column_cublas_ms(n1, n2, nth, nl, len(runs), c, K)
+    c64, f64 = ours["complex64"], ours["fp64"]
+    ratios = {
+        "lspace_complex64": lib["lspace_cufft_c2c_ms"] / c64["lspace_ms"],
+        "lspace_fp64": lib["lspace_cufft_z2z_ms"] / f64["lspace_ms"],
+        "column_complex64_vs_fp32_bf16x9": lib["column_cublas_fp32_bf16x9_ms"] / c64["column_ms"],
+        "column_complex64_vs_fp32_simt": lib["column_cublas_fp32_simt_ms"] / c64["column_ms"],
+        "column_complex64_vs_tf32": lib["column_cublas_tf32_ms"] / c64["column_ms"],
+        "column_fp64": lib["column_cublas_fp64_ms"] / f64["column_ms"],
+    }
+    print(json.dumps({"compare_libs": {"workload": desc, "steps": K, "ours": ours,
+                                       "library": lib, "library_over_ours": ratios,
+                                       "note": "library forms: one batched cufftPlanMany 2-D "
+                                               "transform pair with the phases as elementwise "
+                                               "kernels; strided-batched cublasGemmEx Legendre "
+                                               "pair with the potential phase elementwise; ours: "
+                                               "per-kernel-class CUDA events of the propagator"}}))
 
 
 def main():
@@ -422,14 +522,20 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1", "c0", "c2", "c2j0", "c3", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c0", "c2", "c2j0", "c3", "c4"])
     ap.add_argument("--runs", type=int, default=64, help="runs of the c2j0 batch")
     ap.add_argument("--fp64", action="store_true", help="plain FP64 form instead of complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true",
+                    help="skip the plain FP64 form's rate on the same workload")
+    ap.add_argument("--compare-libs", action="store_true",
+                    help="time the column and l-space passes against cuBLAS / cuFFT forms")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.compare_libs:
+        run_compare_libs(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -48,6 +48,7 @@ extern "C" {
 #define QD_ERR_UNSUPPORTED -6  /* size/option not supported by the kernels    */
 #define QD_ERR_IO          -7  /* file read/write error (.grids, checkpoint)  */
 #define QD_ERR_DEVICE      -8  /* device-side status word reported a failure  */
+#define QD_ERR_STOPPED     -9  /* a progress callback asked to stop           */
 
 /* arithmetic of the propagation */
 #define QD_PREC_FP64  0  /* plain form: complex128 psi, FP64 everywhere       */
@@ -82,11 +83,14 @@ typedef struct qd_time {
   int32_t steps;
 } qd_time;
 
-/* Called every steps_to_copy_psi_from_device_to_host steps with the current
- * theta-space psi (host copy, same layout as qd_data.psi) -- the C ABI
- * counterpart of options.wave_to_matlab (common/wave2matlab.C:26-34,
- * common-cuda/evolutionCUDA2.cu:540-546).  Return 0 to continue, non-zero to
- * stop the propagation with QD_ERR_INVALID. */
+/* The C ABI counterpart of options.wave_to_matlab (common/wave2matlab.C:26-34,
+ * common-cuda/evolutionCUDA2.cu:540-546).  qd_time_evolution /
+ * qd_time_evolution_batch call it whenever time.steps reaches a multiple of
+ * steps_to_copy_psi_from_device_to_host, after writing that step's psi (the
+ * caller's array, passed again as `psi`), time.steps and CRP.CRP into the
+ * run's struct; `norm` is the run's wavepacket norm after the step.  Return
+ * 0 to continue, non-zero to stop the call with QD_ERR_STOPPED (the struct
+ * then holds the state of that step). */
 typedef int (*qd_progress_fn)(int32_t step, double norm, const double *psi,
                               void *ctx);
 
@@ -95,7 +99,10 @@ typedef int (*qd_progress_fn)(int32_t step, double norm, const double *psi,
 typedef struct qd_options {
   const char    *wave_to_matlab;  /* kept for schema parity; not executed   */
   const char    *test_name;
-  int32_t        steps_to_copy_psi_from_device_to_host; /* 0 = never       */
+  /* N > 0: every N steps (time.steps % N == 0) qd_time_evolution writes psi,
+   * time.steps and CRP.CRP back and calls progress (the reference's GPU loop
+   * computes P(E) and copies psi back on those steps); 0 = only at the end */
+  int32_t        steps_to_copy_psi_from_device_to_host;
   int32_t        precision;       /* QD_PREC_FP64 (default) or QD_PREC_FP32 */
   qd_progress_fn progress;        /* optional                               */
   void          *progress_ctx;

@@ -4,7 +4,9 @@
 
 Output: quantum-dynamics_b200/lib/libqd.so.  Each .cu is compiled with nvcc
 for sm_100a only; the object files are linked into one shared library with
-the CUDA runtime linked statically.
+the CUDA runtime linked statically.  Also lib/libqd_libcmp.so from
+compare/qd_libcmp.cu: the same passes on cuFFT and cuBLAS, which only the
+benchmark's library comparison loads (the propagator never links them).
 """
 import glob
 import os
@@ -16,6 +18,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libqd.so")
+CMP_SRC = os.path.join(HERE, "compare", "qd_libcmp.cu")
+CMP_LIB = os.path.join(HERE, "lib", "libqd_libcmp.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -56,6 +60,9 @@ def build(force=False, verbose=False):
         raise RuntimeError("nvcc failed for: " + ", ".join(failed))
     if force or procs or _newer(objs, LIB):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        subprocess.run(cmd, check=True)
+    if force or _newer([CMP_SRC], CMP_LIB):
+        cmd = [NVCC] + ARCH + FLAGS + ["-shared", CMP_SRC, "-o", CMP_LIB, "-lcufft", "-lcublas"]
         subprocess.run(cmd, check=True)
     return LIB
 

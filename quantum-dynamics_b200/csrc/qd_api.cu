@@ -143,6 +143,22 @@ bool all_finite(const double *a, size_t n)
   return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
 }
 
+// Makes the handle's device current for one API call and restores the
+// caller's afterwards: the handle's stream and buffers belong to that device.
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int dev)
+  {
+    if (cudaGetDevice(&prev) != cudaSuccess) { cudaGetLastError(); prev = -1; return; }
+    if (prev == dev) prev = -1;
+    else if (cudaSetDevice(dev) != cudaSuccess) { cudaGetLastError(); prev = -1; }
+  }
+  ~DevGuard()
+  {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 
 // error reporting for the other translation units of the library (qd_err.h)
@@ -154,6 +170,8 @@ int qd_set_error(int code, const char *msg)
 void qd_count_launches(int n) { g_launches += n; }
 
 struct qd_handle {
+  int dev = 0;                    // the device current at creation: its stream and buffers
+  bool failed = false;            // a propagation stopped on a corrupted state
   qd_data *data = nullptr;        // run 0 (holds the fields shared by the batch)
   std::vector<qd_data *> runs;    // all runs of the batch
   int nruns = 1;
@@ -668,21 +686,30 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
   // rounding (FP64 1e-8, complex64 1e-4 relative) means a corrupted state or
   // an absorber above 1.  With more angular functions than quadrature nodes
   // the reference's transform pair itself may raise the norm: no guard.
+  // All norms of the call are checked before any is recorded; a failed check
+  // leaves the handle refusing further steps (its state is the corrupted one).
   const double scale = h->data->r1.dr * h->data->r2.dr;
   const double grow_tol = h->prec == QD_PREC_FP64 ? 1e-8 : 1e-4;
+  const size_t have = h->norms_host.size();
   for (long s = 0; s < (long)n * R; s++) {
     const double v = nb[s] * scale;
     const int step = h->steps - n + (int)(s / R) + 1, run = (int)(s % R);
-    if (!std::isfinite(v))
+    if (!std::isfinite(v)) {
+      h->failed = true;
       return set_err(QD_ERR_NONFINITE, "non-finite wavepacket norm at step %d (run %d)", step, run);
-    if (h->norm_guard && h->norms_host.size() >= (size_t)R) {
-      const double pv = h->norms_host[h->norms_host.size() - R];   // same run, one step earlier
-      if (v > pv * (1.0 + grow_tol))
+    }
+    const bool has_prev = s >= R || have >= (size_t)R;
+    if (h->norm_guard && has_prev) {
+      // same run, one step earlier
+      const double pv = s >= R ? nb[s - R] * scale : h->norms_host[have - R + run];
+      if (v > pv * (1.0 + grow_tol)) {
+        h->failed = true;
         return set_err(QD_ERR_NONFINITE, "wavepacket norm grew from %.17g to %.17g at step %d (run %d):"
                        " a step only loses norm, through the absorbers", pv, v, step, run);
+      }
     }
-    h->norms_host.push_back(v);
   }
+  for (long s = 0; s < (long)n * R; s++) h->norms_host.push_back(nb[s] * scale);
   return QD_OK;
 }
 
@@ -720,6 +747,8 @@ int validate_batch(const qd_data *runs, int n)
         same(b.theta.x, a.theta.x, a.theta.n) && same(b.theta.w, a.theta.w, a.theta.n) &&
         b.time.time_step == a.time.time_step && b.time.steps == a.time.steps &&
         b.options.precision == a.options.precision &&
+        b.options.steps_to_copy_psi_from_device_to_host ==
+            a.options.steps_to_copy_psi_from_device_to_host &&
         same(b.dump1.dump, a.dump1.dump, a.r1.n) && same(b.dump2.dump, a.dump2.dump, a.r2.n) &&
         b.CRP.calculate_CRP == a.CRP.calculate_CRP &&
         (!a.CRP.calculate_CRP ||
@@ -728,8 +757,8 @@ int validate_batch(const qd_data *runs, int n)
           b.CRP.n_energies == a.CRP.n_energies));
     if (!ok)
       return set_err(QD_ERR_INVALID, "run %d differs from run 0 in a field the batch shares "
-                     "(grids, theta nodes and weights, time, options.precision, dumps, CRP "
-                     "settings)", r);
+                     "(grids, theta nodes and weights, time, options.precision and "
+                     "steps_to_copy_psi_from_device_to_host, dumps, CRP settings)", r);
   }
   return QD_OK;
 }
@@ -745,6 +774,7 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   }
   qd_handle *h = new qd_handle();
   *out = h;
+  CU(cudaGetDevice(&h->dev));
   h->data = const_cast<qd_data *>(d);
   h->nruns = nruns;
   for (int r = 0; r < nruns; r++) h->runs.push_back(const_cast<qd_data *>(&runs[r]));
@@ -1012,7 +1042,7 @@ int energies(qd_handle *h, int run, double out4[4])
 }
 
 // ---- checkpoint / restore ----------------------------------------------------
-constexpr uint64_t CKPT_MAGIC = 0x32544b5044514251ull;   // file tag, layout version 2
+constexpr uint64_t CKPT_MAGIC = 0x33544b5044514251ull;   // file tag, layout version 3
 
 struct CkptHeader {
   uint64_t magic;
@@ -1020,6 +1050,8 @@ struct CkptHeader {
   int32_t steps, started, last_finalized, ring_fill, flux_pending;
   int32_t basis;               // l-space representation: 0 psi_l, 1 psi_l / sqrt(l+1/2)
   int64_t acc_done;
+  int32_t ring;                // steps held by the flux history ring (QD_RING)
+  int32_t reserved;
 };
 
 // The complex64 tensor-core column pass keeps psi_l in the orthonormal basis.
@@ -1034,6 +1066,7 @@ int checkpoint(qd_handle *h, const char *path)
   hd.steps = h->steps; hd.started = h->started; hd.last_finalized = h->last_finalized;
   hd.ring_fill = h->ring_fill; hd.flux_pending = h->flux_pending; hd.acc_done = h->acc_done;
   hd.basis = lspace_basis(h);
+  hd.ring = QD_RING;
   const size_t csz = h->prec == QD_PREC_FP64 ? sizeof(double2) : sizeof(float2);
   std::vector<std::pair<const void *, size_t>> blocks;
   const size_t nq = (size_t)h->nth * h->n1;
@@ -1073,7 +1106,13 @@ int restore(qd_handle *h, const char *path)
   CkptHeader hd{};
   if (fread(&hd, sizeof hd, 1, f) != 1 || hd.magic != CKPT_MAGIC) {
     fclose(f);
-    return set_err(QD_ERR_IO, "\"%s\" is not a propagator checkpoint", path);
+    return set_err(QD_ERR_IO, "\"%s\" is not a propagator checkpoint of this layout version",
+                   path);
+  }
+  if (hd.ring != QD_RING) {
+    fclose(f);
+    return set_err(QD_ERR_INVALID, "checkpoint \"%s\" holds a flux history ring of %d steps, "
+                   "this library %d", path, hd.ring, QD_RING);
   }
   if (hd.prec != h->prec || hd.nruns != h->nruns || hd.n1 != h->n1 || hd.n2 != h->n2 ||
       hd.nth != h->nth || hd.nl != h->nl || hd.ne != (h->do_crp ? h->ne : 0) ||
@@ -1117,7 +1156,14 @@ int restore(qd_handle *h, const char *path)
   h->steps = hd.steps; h->started = hd.started; h->last_finalized = hd.last_finalized;
   h->ring_fill = hd.ring_fill; h->flux_pending = hd.flux_pending; h->acc_done = hd.acc_done;
   h->norms_host = norms;
+  h->failed = false;
   return QD_OK;
+}
+
+int refuse_failed(const qd_handle *h)
+{
+  return set_err(QD_ERR_NONFINITE, "the handle's last propagation stopped on a corrupted "
+                 "wavepacket (step %d); restore a checkpoint or create a new handle", h->steps);
 }
 
 }  // namespace
@@ -1162,6 +1208,8 @@ int qd_n_runs(qd_handle *h, int32_t *n_out)
 
 int qd_destroy(qd_handle *h)
 {
+  if (!h) return QD_OK;
+  DevGuard g(h->dev);
   delete h;
   return QD_OK;
 }
@@ -1170,6 +1218,8 @@ int qd_propagate(qd_handle *h, int32_t n_steps)
 {
   if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
   if (n_steps < 0) return set_err(QD_ERR_INVALID, "n_steps < 0");
+  if (h->failed) return refuse_failed(h);
+  DevGuard g(h->dev);
   if (h->prec == QD_PREC_FP64) return propagate<double>(h, n_steps);
   return propagate<float>(h, n_steps);
 }
@@ -1178,6 +1228,8 @@ int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes, doubl
 {
   if (!h || !device_ms) return set_err(QD_ERR_INVALID, "NULL argument");
   if (n_steps < 0 || flush_bytes < 0) return set_err(QD_ERR_INVALID, "negative argument");
+  if (h->failed) return refuse_failed(h);
+  DevGuard g(h->dev);
   if (h->prec == QD_PREC_FP64) return propagate<double>(h, n_steps, (size_t)flush_bytes, device_ms);
   return propagate<float>(h, n_steps, (size_t)flush_bytes, device_ms);
 }
@@ -1185,6 +1237,7 @@ int qd_propagate_timed(qd_handle *h, int32_t n_steps, int64_t flush_bytes, doubl
 int qd_get_psi_run(qd_handle *h, int32_t run, double *psi_out)
 {
   if (!h || !psi_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return get_psi(h, run, psi_out);
 }
 
@@ -1193,6 +1246,7 @@ int qd_get_psi(qd_handle *h, double *psi_out) { return qd_get_psi_run(h, 0, psi_
 int qd_get_crp_run(qd_handle *h, int32_t run, double *crp_out)
 {
   if (!h || !crp_out) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return get_crp(h, run, crp_out);
 }
 
@@ -1201,6 +1255,7 @@ int qd_get_crp(qd_handle *h, double *crp_out) { return qd_get_crp_run(h, 0, crp_
 int qd_download(qd_handle *h)
 {
   if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
+  DevGuard g(h->dev);
   for (int r = 0; r < h->nruns; r++) {
     TRY(get_psi(h, r, h->runs[r]->psi));
     if (h->do_crp && h->started) TRY(get_crp(h, r, h->runs[r]->CRP.CRP));
@@ -1252,6 +1307,7 @@ int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written)
 int qd_energies_run(qd_handle *h, int32_t run, double out4[4])
 {
   if (!h || !out4) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return energies(h, run, out4);
 }
 
@@ -1260,22 +1316,61 @@ int qd_energies(qd_handle *h, double out4[4]) { return qd_energies_run(h, 0, out
 int qd_checkpoint(qd_handle *h, const char *path)
 {
   if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return checkpoint(h, path);
 }
 
 int qd_restore(qd_handle *h, const char *path)
 {
   if (!h || !path) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return restore(h, path);
 }
 
+// The MEX drop-in.  With options.steps_to_copy_psi_from_device_to_host = N
+// > 0 it does what the reference's GPU loop does every N steps
+// (common-cuda/evolutionCUDA2.cu:540-546: P(E) on steps % N == 0, psi copied
+// back to the host and the Matlab script run): whenever time.steps reaches a
+// multiple of N it writes psi, time.steps and CRP.CRP of every run into the
+// caller's arrays and calls options.progress of each run that has one.  A
+// non-zero return stops the call with QD_ERR_STOPPED, the arrays holding
+// that step's state.
 int qd_time_evolution_batch(qd_data *runs, int32_t n_runs)
 {
   if (!runs || n_runs < 1) return set_err(QD_ERR_INVALID, "need at least one run");
+  const int every = runs[0].options.steps_to_copy_psi_from_device_to_host;
+  if (every < 0)
+    return set_err(QD_ERR_INVALID, "options.steps_to_copy_psi_from_device_to_host = %d", every);
   qd_handle *h = nullptr;
   TRY(qd_create_batch(runs, n_runs, &h));
-  int rc = qd_propagate(h, runs[0].time.total_steps);
-  if (rc == QD_OK) rc = qd_download(h);
+  const int total = runs[0].time.total_steps;
+  int rc = QD_OK;
+  if (every == 0) {
+    rc = qd_propagate(h, total);
+    if (rc == QD_OK) rc = qd_download(h);
+  } else {
+    bool fresh = true;                  // the caller's arrays hold the current state
+    for (int done = 0; done < total && rc == QD_OK;) {
+      const int n = std::min(every - h->steps % every, total - done);
+      rc = qd_propagate(h, n);
+      if (rc != QD_OK) break;
+      done += n;
+      fresh = false;
+      if (h->steps % every != 0) continue;
+      rc = qd_download(h);
+      if (rc != QD_OK) break;
+      fresh = true;
+      const size_t last = h->norms_host.size() - (size_t)n_runs;
+      for (int r = 0; r < n_runs && rc == QD_OK; r++) {
+        const qd_options &o = runs[r].options;
+        if (o.progress && o.progress(h->steps, h->norms_host[last + r], runs[r].psi,
+                                     o.progress_ctx) != 0)
+          rc = set_err(QD_ERR_STOPPED, "the progress callback of run %d stopped the "
+                       "propagation at step %d", r, h->steps);
+      }
+    }
+    if (rc == QD_OK && !fresh) rc = qd_download(h);
+  }
   qd_destroy(h);
   return rc;
 }
@@ -1336,9 +1431,10 @@ namespace {
 constexpr int QD_MAX_DEVICES = 64;
 std::atomic<double2 *> g_energy_scratch_at[QD_MAX_DEVICES];   // per device, set once
 
-// Device address of g_energy_scratch on the current device, looked up on the
-// first call for that device (cudaGetSymbolAddress; two threads racing here
-// both store the same address).
+// Device address of g_energy_scratch on the current device (the handle's:
+// the entry point makes it current), looked up on the first call for that
+// device (cudaGetSymbolAddress; two threads racing here both store the same
+// address).
 int energy_scratch(double2 **out)
 {
   int dev = 0;
@@ -1399,5 +1495,6 @@ int energies_noalloc(qd_handle *h, int run, double out4[4])
 extern "C" int qd_energies_noalloc(qd_handle *h, int32_t run, double out4[4])
 {
   if (!h || !out4) return set_err(QD_ERR_INVALID, "NULL argument");
+  DevGuard g(h->dev);
   return energies_noalloc(h, run, out4);
 }

@@ -19,6 +19,7 @@ QD_ERR_NONFINITE = -5
 QD_ERR_UNSUPPORTED = -6
 QD_ERR_IO = -7
 QD_ERR_DEVICE = -8
+QD_ERR_STOPPED = -9
 
 QD_PREC_FP64 = 0
 QD_PREC_FP32 = 1

@@ -1,7 +1,7 @@
-"""Regenerate the golden fixtures in tests/golden/ (run in a container that
-has the reference checkout at /root/reference):
+"""Regenerate the golden fixtures in tests/golden/ (run where the reference
+checkout is present, its location in QD_REFERENCE_DIR):
 
-    python tests/golden/make_golden.py
+    QD_REFERENCE_DIR=<checkout> python tests/golden/make_golden.py
 
 * grids/<n>-LegendreGauss.grids   copied verbatim from the reference's
   GaussLegendre/ tables (32-digit Gauss-Legendre nodes and weights).
@@ -22,7 +22,7 @@ sys.path.insert(0, os.path.join(REPO, "quantum-dynamics_b200"))
 from qd_b200 import systems as S  # noqa: E402
 from oracle import pyoracle as O  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("QD_REFERENCE_DIR", "")
 GRIDS_N = (8, 12, 40, 41, 64, 128)
 
 # small cases: (name, builder kwargs)
@@ -58,8 +58,8 @@ def save_case(name, kw):
 
 
 def main():
-    if not os.path.isdir(REF):
-        sys.exit("reference checkout not found at " + REF)
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set QD_REFERENCE_DIR to the reference checkout (now: %r)" % REF)
     os.makedirs(os.path.join(HERE, "grids"), exist_ok=True)
     for n in GRIDS_N:
         src = os.path.join(REF, "GaussLegendre", f"{n}-LegendreGauss.grids")

@@ -52,9 +52,12 @@ def test_spline_reproduces_the_table_at_its_nodes(oracle):
 
 
 def test_fixture_matches_the_reference_files():
-    ref = "/root/reference/FH2/HSW"
+    root = os.environ.get("QD_REFERENCE_DIR")
+    if not root:
+        pytest.skip("QD_REFERENCE_DIR (the reference checkout) is not set")
+    ref = os.path.join(root, "FH2", "HSW")
     if not os.path.isdir(ref):
-        pytest.skip("reference checkout not present")
+        pytest.skip(f"no reference checkout at {root}")
     t = read_tables(ref)
     f = np.load(TABLES)
     for k, v in t.items():

@@ -2,9 +2,16 @@
 static device array (no device allocation) -- against the allocating entry
 point qd_energies_run, both called through the C ABI.
 
-Collected last on purpose: it must pass in a fresh process (the first call on
-the device looks up the static scratch) and after every other test.
+Collected last on purpose, so that a run that stops at the first failure has
+run every other test first.  In a full run these cases follow the other
+tests in the same process; test_noalloc_first_call_in_a_fresh_process runs
+the entry point in a new process, where its first call on the device looks
+up the static scratch's address.
 """
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -73,3 +80,36 @@ def test_noalloc_rejects_grids_above_the_static_scratch():
         # the allocating entry point still serves this size
         e = energies(L.qd_energies_run, p, 0)
         assert np.all(np.isfinite(e))
+
+
+FRESH = r"""
+import sys
+import numpy as np
+sys.path[:0] = [{repo!r}, {pkg!r}]
+from qd_b200 import _abi, systems as S, QD_PREC_FP64
+from qd_b200.timeevolution import Propagator, set_device
+set_device(0)
+L = _abi.lib()
+base = S.build_case("f+h2", 48, 40, 24, m=23, total_steps=12, n_energies=5,
+                    precision=QD_PREC_FP64)
+with Propagator(base) as p:
+    p.propagate(12)
+    out = []
+    for fn in (L.qd_energies_noalloc, L.qd_energies_noalloc, L.qd_energies_run):
+        e = np.zeros(4)
+        _abi.check(fn(p._h, 0, e.ctypes.data_as(_abi.c_double_p)))
+        out.append(e)
+for e in out[:2]:
+    assert np.abs(e - out[2]).max() <= 1e-12 * np.abs(out[2]).max(), (e, out[2])
+print("fresh-process noalloc ok")
+"""
+
+
+def test_noalloc_first_call_in_a_fresh_process():
+    here = os.path.dirname(os.path.abspath(__file__))
+    repo = os.path.dirname(here)
+    code = FRESH.format(repo=repo, pkg=os.path.join(repo, "quantum-dynamics_b200"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh-process noalloc ok" in r.stdout
