@@ -207,6 +207,19 @@ int qd_get_norms(qd_handle *h, double *norms_out, int32_t n);
 /* Kinetic, rotational, potential and total energy of the current psi
  * (timeEvol.C:256-283, 323-360, 390-436), hartree. */
 int qd_energies(qd_handle *h, double out4[4]);
+/* Energies inside the propagation, the reference's per-step diagnostics
+ * (potential_energy, rotational_energy, kinetic_energy_for_legendre_psi;
+ * timeEvol.C:256-283, 323-360, 390-436) at an interval: with every > 0, on
+ * each step whose count time.steps is a multiple of `every`, the step's own
+ * kernels add FP64 partial sums (kinetic and rotational in the l-space pass,
+ * potential in the column pass that forms that step's theta-space
+ * wavepacket), copied back once per qd_propagate call.  0 turns it off
+ * (the default). */
+int qd_set_energy_interval(qd_handle *h, int32_t every);
+/* The newest min(cap, recorded) energy records of one run, oldest first, five
+ * doubles each: step, E_kin, E_rot, E_pot, E_total (hartree); n_out = records
+ * written. */
+int qd_get_energy_log_run(qd_handle *h, int32_t run, double *out, int32_t cap, int32_t *n_out);
 /* Steps propagated so far (the handle's time.steps). */
 int qd_steps(qd_handle *h, int32_t *steps_out);
 /* Average device time per step (ms) of each kernel class over the last
@@ -265,7 +278,8 @@ int qd_energies_noalloc(qd_handle *h, int32_t run, double out4[4]);
 /* ---- setup helpers (the Matlab-side L4 of the reference) --------------- */
 
 /* Gauss-Legendre nodes and weights from a "<n>-LegendreGauss.grids" file in
- * dir (format of GaussLegendre/*.grids, reader common/GaussLegendre2.m:1-31):
+ * dir (format of the reference's GaussLegendre/<n>-LegendreGauss.grids files, reader
+ * common/GaussLegendre2.m:1-31):
  * ceil(n/2) lines "x w" of the non-negative half, mirrored; x ascending. */
 int qd_read_grids(const char *dir, int32_t n, double *x, double *w);
 

@@ -6,7 +6,8 @@ Output: quantum-dynamics_b200/lib/libqd.so.  Each .cu is compiled with nvcc
 for sm_100a only; the object files are linked into one shared library with
 the CUDA runtime linked statically.  Also lib/libqd_libcmp.so from
 compare/qd_libcmp.cu: the same passes on cuFFT and cuBLAS, which only the
-benchmark's library comparison loads (the propagator never links them).
+benchmark's library comparison loads (the propagator never links them); and
+bin/qd_run from cli/qd_run.cpp, the run-file driver over the C ABI.
 """
 import glob
 import os
@@ -18,6 +19,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "lib", "libqd.so")
+RUN_SRC = os.path.join(HERE, "cli", "qd_run.cpp")
+RUN_BIN = os.path.join(HERE, "bin", "qd_run")
 CMP_SRC = os.path.join(HERE, "compare", "qd_libcmp.cu")
 CMP_LIB = os.path.join(HERE, "lib", "libqd_libcmp.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -60,6 +63,12 @@ def build(force=False, verbose=False):
         raise RuntimeError("nvcc failed for: " + ", ".join(failed))
     if force or procs or _newer(objs, LIB):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        subprocess.run(cmd, check=True)
+    if force or _newer([RUN_SRC, LIB, os.path.join(REPO, "include", "qd.h")], RUN_BIN):
+        os.makedirs(os.path.dirname(RUN_BIN), exist_ok=True)
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", f"-I{os.path.join(REPO, 'include')}",
+               RUN_SRC, "-o", RUN_BIN, f"-L{os.path.dirname(LIB)}", "-lqd",
+               "-Wl,-rpath,$ORIGIN/../lib"]
         subprocess.run(cmd, check=True)
     if force or _newer([CMP_SRC], CMP_LIB):
         cmd = [NVCC] + ARCH + FLAGS + ["-shared", CMP_SRC, "-o", CMP_LIB, "-lcufft", "-lcublas"]
