@@ -5,42 +5,56 @@
 // CTA (or per 2- or 4-CTA cluster), with every 1-D transform done as two
 // register passes.
 //
+// Both phases are separable in (R, r): Rot(dt/2) = D1(i) D2(j) with
+// D1 = exp(-i l(l+1) I_R(i) dt/2), D2 likewise with I_r(j), and the kinetic
+// phase is K1(k_i) K2(k_j).  A diagonal factor in i commutes with any
+// operator along j and vice versa, so the slice operator is the product of
+// a row operator and a column operator,
+//     [D1 IFFT_R K1 FFT_R D1] (each row j)  x  [D2 IFFT_r K2 FFT_r D2] (each column i),
+// which is applied in that order: the row operator works on whole rows, the
+// column operator on whole columns, and the slice goes back to global memory
+// straight from the column passes.  The arithmetic is that of the reference's
+// 2-D transform pair, regrouped (rounding differs at the 1e-7 level).
+//
 // A length N = A*B transform (n = a + A b, k = c + B d) is
 //   pass 1, one item per a:  B-point DFT over b in registers, times W_N^{a c}
 //   pass 2, one item per c:  A-point DFT over a in registers -> X[c + B d]
-// so a 2-D transform costs two shared-memory round trips per dimension
-// instead of one per radix stage.  The slice lives in shared memory in ONE
-// padded layout for the whole step, every pass works in place, and only
-// six barriers separate the seven passes:
-//   P1  global -> regs: Rot/2, row pass 1 (B1-pt), twiddle      -> smem
-//   P2  row pass 2 (A1-pt)                                       in place
-//   P3  column pass 1 (B2-pt), twiddle                           in place
-//   P4  column pass 2 (A2-pt), kinetic phase, inverse column
-//       pass 1 (A2-pt), twiddle                                  in place
-//   P5  inverse column pass 2 (B2-pt)                            in place
-//   P6  inverse row pass 1 (A1-pt over a block), twiddle         in place
-//   P7  inverse row pass 2 (B1-pt), Rot/2 -> global
-// Row layout: block c (c < B1) holds slots 0..A1-1 at s + (A1+1) c; row
-// stride RS = N1 + B1 (= 8 mod 16 complex).  With this padding every warp
-// access of every pass touches each shared-memory bank at most twice (the
-// minimum for 8-byte elements), and global loads and stores are whole
-// 64- or 128-byte segments.  The forward row transform leaves frequency
-// k = c + B1 d at slot d of block c; the inverse row transform reads that
-// order directly (its decomposition is the transposed one, A = B1, B = A1).
+// and its inverse mirrors it (an A-point inverse DFT over d per c, times
+// W_N^{-a c}, then a B-point inverse DFT over c per a).  Pass 2 of the forward
+// transform, the phase and pass 1 of the inverse share one item, so each 1-D
+// operator costs three register passes and two shared-memory round trips.
+// The slice lives in shared memory in ONE padded layout, every pass works in
+// place, and five barriers separate the six passes:
+//   Pa  global -> regs: D1, row pass 1 (B1-pt), twiddle               -> smem
+//   Pb  row pass 2 (A1-pt), K1, inverse row pass 1 (A1-pt)            in place
+//   Pc  twiddle, inverse row pass 2 (B1-pt), D1                       in place
+//   Pd  D2, column pass 1 (B2-pt), twiddle                            in place
+//   Pe  column pass 2 (A2-pt), K2/(n1 n2), inverse column pass 1, tw. in place
+//   Pf  inverse column pass 2 (B2-pt), D2                             -> global
+// Row layout: element i of a row sits at slot i % A1 of block i / A1, slot s
+// of block c at s + (A1+1) c; row stride RS = N1 + B1 (= 8 mod 16 complex).
+// Between Pa and Pc the row holds its transform at slot d of block c
+// (frequency c + B1 d).  With this padding every warp access of every pass
+// touches each shared-memory bank at most twice (the minimum for 8-byte
+// elements), and global loads and stores are whole 64- or 128-byte segments.
 //
-// The kinetic phase tables (kc1 permuted to the column-counter order, kc2),
-// rc1[l] and the N2-point roots are staged in shared memory by the prologue,
-// which runs before the previous kernel's results are waited on.
+// The phase tables (rc1[l] and rc2[l], kc1, kc2) and the N2-point roots are
+// staged in shared memory by the prologue, which runs before the previous
+// kernel's results are waited on.
+//
+// Energy steps (LineParams::esum): Pb, Pe and Pf also sum, in FP64, the
+// kinetic energy from the row and column transforms (Parseval along the other
+// dimension) and the rotational energy of the step's final l-space values.
 //
 // A slice may also run on a 2-CTA cluster (for small batches, where one CTA
 // per slice leaves most SMs idle): each CTA then keeps half the rows for the
 // row passes and half the columns, over all rows, for the column passes; the
-// two transposes between them are bulk shared-memory-to-shared-memory copies
-// of whole row halves, so no pass touches the other CTA's memory itself.
-// A 256 x 192 slice (384 KB) runs on a 4-CTA cluster, a quarter of the rows
-// and of the columns per CTA; its transposes swap row parts between the CTAs
-// in place (registers, cluster barrier, remote stores), so each CTA holds
-// only its own 101 KB of rows and two clusters' CTAs share an SM.
+// one transpose between them is a set of bulk shared-memory-to-shared-memory
+// copies of whole row halves, so no pass touches the other CTA's memory
+// itself.  A 256 x 192 slice (384 KB) runs on a 4-CTA cluster, a quarter of
+// the rows and of the columns per CTA; its transpose swaps row parts between
+// the CTAs in place (registers, cluster barrier, remote stores), so each CTA
+// holds only its own 101 KB of rows and two clusters' CTAs share an SM.
 //
 // The 6-, 12-, 16-, 24- and 32-point DFTs are P x Q compositions whose
 // internal twiddles are compensated constants (value + residual), like the
@@ -189,18 +203,18 @@ template <int N1, int N2, int NT, int CL> struct RfShape {
   static constexpr int HR = N2 / CL;                  // rows held by one CTA
   static constexpr int HW = RS / CL;                  // column part width: B1 / CL whole blocks
   static constexpr int BPO = B2 / CL;                 // column-pass row groups per CTA's rows
-  // CL = 4: the transposes swap row parts between the CTAs in place (SWAP),
+  // CL = 4: the transpose swaps row parts between the CTAs in place (SWAP),
   // so a CTA holds only its row array and two CTAs fit on an SM; CL = 2
-  // keeps the peer's rows of its column part in a second array, filled and
-  // emptied by bulk copies
+  // receives the peer's rows of its column part in a second array, filled
+  // by bulk copies
   static constexpr bool SWAP = CL == 4;
   static constexpr int PSLOTS = CL == 1 || SWAP ? 0 : CL - 1;
   static constexpr int P1_UNROLL = 2;                // row items per thread loaded together
   static constexpr int SWAP_ROUNDS = 4;              // row rounds of the in-place transpose
   // own rows [HR][RS]; CL = 2: the peer's rows of this CTA's column part
-  // [HR][HW]; rc1[l], W_N2, kc1 in column-counter order, kc2; CL = 2: two
-  // mbarriers
-  static constexpr size_t TABLES = 2 * (N1 + N2);
+  // [HR][HW]; rc1[l], kc1 (N1 each), W_N2, kc2, rc2[l] (N2 each); CL = 2:
+  // one mbarrier
+  static constexpr size_t TABLES = 2 * N1 + 3 * N2;
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (size_t)PSLOTS * HR * HW +
                                                    TABLES) + (PSLOTS > 0 ? 16 : 0);
   static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row part, one bulk copy
@@ -210,9 +224,6 @@ template <int N1, int N2, int NT, int CL> struct RfShape {
                             HW == (B1 / CL) * (A1 + 1) && HALF_BYTES % 16 == 0),
                 "cluster split: whole row blocks per column part, whole column row groups per CTA");
 };
-
-__device__ __forceinline__ float2 rot_at(const float2 *r1, float2 rj, int i)
-{ return cmul(r1[i], rj); }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -308,16 +319,14 @@ __device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
 
 // CL = 2 or 4: a CL-CTA thread-block cluster per slice.  CTA `rank` runs
 // the row passes on rows [rank HR, (rank+1) HR) and the column passes on
-// column part `rank` (row blocks rank B1/CL .. (rank+1) B1/CL - 1) over all
-// N2 rows.  CL = 2: its own rows in place in its row array, the peer's
-// rows in a second array; the two transposes are bulk copies of whole row
-// halves (544 bytes) between the CTAs' shared memories (after P2 each CTA
-// sends the peer's half of its own rows, after P5 it sends the peer's rows
-// back; an mbarrier in the receiving CTA counts the bytes in).  CL = 4:
-// both transposes are the in-place swap of swap_parts, after which row
-// part o of the row array holds CTA o's rows in this CTA's column part.
-// Every load and store of the passes is local.  CL = 1 keeps the slice in
-// one array in place.
+// column part `rank` (row blocks rank B1/CL .. (rank+1) B1/CL - 1, columns
+// rank N1/CL .. (rank+1) N1/CL - 1) over all N2 rows.  CL = 2: its own rows
+// in place in its row array, the peer's rows in a second array, filled after
+// Pc by bulk copies of whole row halves (544 bytes) from the peer (an
+// mbarrier in the receiving CTA counts the bytes in).  CL = 4: the in-place
+// swap of swap_parts, after which row part o of the row array holds CTA o's
+// rows in this CTA's column part.  Every load and store of the passes is
+// local.  CL = 1 keeps the slice in one array in place.
 template <int N1, int N2, int NT, int CL>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
@@ -326,12 +335,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
   float2 *R = reinterpret_cast<float2 *>(smem4);    // own rows [HR][RS]
-  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column half [HR][HW]
+  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column part [HR][HW]
   float2 *r1 = P + Sh::PSLOTS * HR * HW;             // rc1[l][0..N1)
-  float2 *t2 = r1 + N1;                              // W_N2^k, k < N2
-  float2 *k1 = t2 + N2;                              // kc1[k(q)], q < N1
-  float2 *k2 = k1 + N1;                              // kc2
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(k2 + N2);   // CL = 2: [0] P filled, [1] R's other half
+  float2 *k1 = r1 + N1;                              // kc1
+  float2 *t2 = k1 + N1;                              // W_N2^k, k < N2
+  float2 *k2 = t2 + N2;                              // kc2
+  float2 *r2 = k2 + N2;                              // rc2[l][0..N2)
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(r2 + N2);   // CL = 2: the peer's rows are in
+  __shared__ double red[32];                         // energy steps: block sums
   const int tid = threadIdx.x;
   pdl_trigger();
   if ((int)blockIdx.x >= p.nruns * p.nl * CL) {      // extra CTAs: flux preparation
@@ -346,11 +357,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     if (tid == 0) {
       const uint32_t tx = (CL - 1) * HR * Sh::HALF_BYTES;   // from every peer, every row
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[0])));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[1])));
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                    :: "r"(smem_addr(&mbar[0])), "r"(tx) : "memory");
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                   :: "r"(smem_addr(&mbar[1])), "r"(tx) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -361,19 +369,26 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
   const float2 *tw1 = reinterpret_cast<const float2 *>(p.tw1);
   const float2 *tw2 = reinterpret_cast<const float2 *>(p.tw2);
-  const float2 *rc2 = p.rc2 + l * N2;
   for (int e = tid; e < N1; e += NT) {
     r1[e] = __ldg(p.rc1 + l * N1 + e);
-    k1[e] = __ldg(p.kc1 + (e / A1) + B1 * (e % A1));
+    k1[e] = __ldg(p.kc1 + e);
   }
   for (int e = tid; e < N2; e += NT) {
     t2[e] = __ldg(tw2 + e);
     k2[e] = __ldg(p.kc2 + e);
+    r2[e] = __ldg(p.rc2 + l * N2 + e);
   }
   pdl_wait();                                        // psi_l: the column pass's output
   __syncthreads();
+  // energy step: this thread's shares of sum_k T1 |row FFT|^2, of sum T2 |column
+  // FFT|^2 and of sum (I1 + I2) |psi_l|^2 (the kinetic sums before their phases,
+  // whose moduli are one)
+  const bool en = p.esum != nullptr;
+  double e_k1 = 0.0, e_k2 = 0.0, e_r = 0.0;
 
-  // P1: items (j, a) of this CTA's rows; elements i = a + A1 b from global
+  // ---- the row operator D1 IFFT_R K1 FFT_R D1 on this CTA's rows ------------------
+  // Pa: items (j, a): elements i = a + A1 b from global, D1, B1-point DFT over
+  // b, W^{a c} -> slot a of block c
   {
     const int a = tid % A1;
     float2 w[B1];
@@ -382,19 +397,19 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll (Sh::P1_UNROLL)
     for (int e = tid; e < HR * A1; e += NT) {
       const int j = e / A1, jg = j0 + j;
-      const float2 rj = __ldg(rc2 + jg);
       float2 v[B1];
 #pragma unroll
       for (int b = 0; b < B1; b++) v[b] = g[jg * N1 + a + A1 * b];
 #pragma unroll
-      for (int b = 0; b < B1; b++) v[b] = cmul(v[b], rot_at(r1, rj, a + A1 * b));
+      for (int b = 0; b < B1; b++) v[b] = cmul(v[b], r1[a + A1 * b]);
       Dft<B1, -1>::run(v);
 #pragma unroll
       for (int c = 0; c < B1; c++) R[j * RS + a + (A1 + 1) * c] = c ? cmul(v[c], w[c]) : v[c];
     }
   }
   __syncthreads();
-  // P2: items (j, c): block c, slots a -> frequency c + B1 d at slot d
+  // Pb: items (j, c): the A1-point DFT over the slots a of block c gives
+  // frequency c + B1 d at d; K1; the A1-point inverse DFT over d gives slot a
   for (int e = tid; e < HR * B1; e += NT) {
     const int j = e / B1, c = e % B1;
     float2 *blk = R + j * RS + (A1 + 1) * c;
@@ -402,8 +417,37 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll
     for (int a = 0; a < A1; a++) v[a] = blk[a];
     Dft<A1, -1>::run(v);
+    if (en) {
 #pragma unroll
-    for (int d = 0; d < A1; d++) blk[d] = v[d];
+      for (int d = 0; d < A1; d++)
+        e_k1 += (double)(v[d].x * v[d].x + v[d].y * v[d].y) * __ldg(p.T1 + c + B1 * d);
+    }
+#pragma unroll
+    for (int d = 0; d < A1; d++) v[d] = cmul(v[d], k1[c + B1 * d]);
+    Dft<A1, +1>::run(v);
+#pragma unroll
+    for (int a = 0; a < A1; a++) blk[a] = v[a];
+  }
+  __syncthreads();
+  // Pc: items (j, a): slot a of every block c, W^{-a c}, B1-point inverse DFT
+  // over c -> element i = a + A1 b, D1 -> slot a of block b (the same slots)
+  {
+    const int a = tid % A1;
+    float2 w[B1];
+#pragma unroll
+    for (int c = 0; c < B1; c++) w[c] = cconj(__ldg(tw1 + a * c));
+#pragma unroll 2
+    for (int e = tid; e < HR * A1; e += NT) {
+      const int j = e / A1;
+      float2 v[B1];
+#pragma unroll
+      for (int c = 0; c < B1; c++) v[c] = R[j * RS + a + (A1 + 1) * c];
+#pragma unroll
+      for (int c = 1; c < B1; c++) v[c] = cmul(v[c], w[c]);
+      Dft<B1, +1>::run(v);
+#pragma unroll
+      for (int b = 0; b < B1; b++) R[j * RS + a + (A1 + 1) * b] = cmul(v[b], r1[a + A1 * b]);
+    }
   }
   bool ok = true;
   if constexpr (Sh::SWAP) {
@@ -423,12 +467,17 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
                    peer_addr(smem_addr(&mbar[0]), peer));
     }
     ok = mbar_wait0(smem_addr(&mbar[0]));            // the peers' rows of this part are in
+    // this CTA's incoming copies are complete; the peers wait on this
+    // barrier at exit, so no CTA leaves while a copy out of it may run
+    cluster_arrive_release();
+    if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
   } else {
     __syncthreads();
   }
-  // column passes: column counter q = q0 + qq (frequency k(q) = q / A1 + B1 (q % A1))
-  // at offset pcol(qq) of this CTA's part; row A2 b + r (b < B2) is held by
-  // CTA b / BPO, as its row A2 (b % BPO) + r
+
+  // ---- the column operator D2 IFFT_r K2 FFT_r D2 on this CTA's columns ------------
+  // column counter qq: column i = q0 + qq at offset pcol(qq) of this CTA's
+  // part; row A2 b + r (b < B2) is held by CTA b / BPO, as its row A2 (b % BPO) + r
   constexpr int BPO = Sh::BPO;
   auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
   float2 *cb[Sh::SWAP ? 1 : CL];                     // row 0 of CTA o's rows, this part
@@ -445,18 +494,18 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     else return cb[b / BPO][(inner + A2 * (b % BPO)) * cs[b / BPO] + pcol(qq)];
   };
   constexpr int QC = N1 / CL;
-  // P3: items (q, a'): rows a' + A2 b'
+  // Pd: items (q, a'): rows a' + A2 b, D2, B2-point DFT over b, W^{a' c} -> rows a' + A2 c
   for (int e = tid; e < QC * A2; e += NT) {
     const int qq = e % QC, ap = e / QC;
     float2 v[B2];
 #pragma unroll
-    for (int b = 0; b < B2; b++) v[b] = at(b, ap, qq);
+    for (int b = 0; b < B2; b++) v[b] = cmul(at(b, ap, qq), r2[ap + A2 * b]);
     Dft<B2, -1>::run(v);
 #pragma unroll
     for (int c = 0; c < B2; c++) at(c, ap, qq) = c ? cmul(v[c], t2[ap * c]) : v[c];
   }
   __syncthreads();
-  // P4: items (q, c'): rows a' + A2 c'; forward pass 2, kinetic phase, inverse pass 1
+  // Pe: items (q, c'): rows a' + A2 c'; forward pass 2, K2 / (n1 n2), inverse pass 1
   for (int e = tid; e < QC * B2; e += NT) {
     const int qq = e % QC, cp = e / QC;
     float2 *col;
@@ -472,20 +521,25 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
         if (cp / BPO == o) { cbase = cb[o]; cst = cs[o]; }
       col = cbase + A2 * (cp % BPO) * cst + pcol(qq);
     }
-    const float2 kq = k1[q0 + qq];
     float2 v[A2];
 #pragma unroll
     for (int a = 0; a < A2; a++) v[a] = col[a * cst];
     Dft<A2, -1>::run(v);
+    if (en) {
+#pragma unroll
+      for (int d = 0; d < A2; d++)
+        e_k2 += (double)(v[d].x * v[d].x + v[d].y * v[d].y) * __ldg(p.T2 + cp + B2 * d);
+    }
 #pragma unroll
     for (int d = 0; d < A2; d++)
-      v[d] = cmul(v[d], cscale2(cmul(kq, k2[cp + B2 * d]), p.kscale, p.kscale_lo));
+      v[d] = cmul(v[d], cscale2(k2[cp + B2 * d], p.kscale, p.kscale_lo));
     Dft<A2, +1>::run(v);
 #pragma unroll
     for (int cc = 0; cc < A2; cc++) col[cc * cst] = cc ? cmul(v[cc], cconj(t2[cp * cc])) : v[cc];
   }
   __syncthreads();
-  // P5: items (q, c''): rows c'' + A2 a'' -> natural rows c'' + A2 d'', in place
+  // Pf: items (q, c''): rows c'' + A2 a -> natural rows j = c'' + A2 d, D2 -> global
+#pragma unroll 2
   for (int e = tid; e < QC * A2; e += NT) {
     const int qq = e % QC, cc = e / QC;
     float2 v[B2];
@@ -493,85 +547,33 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     for (int a = 0; a < B2; a++) v[a] = at(a, cc, qq);
     Dft<B2, +1>::run(v);
 #pragma unroll
-    for (int d = 0; d < B2; d++) at(d, cc, qq) = v[d];
-  }
-  if constexpr (Sh::SWAP) {
-    __syncthreads();
-    swap_parts<NT, CL, HR, HW, RS, Sh::SWAP_ROUNDS>(R, rank, tid);    // the rows back to their owners
-  } else if constexpr (CL > 1) {
-    // every peer's rows of this part -> back into that peer's row array
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    for (int e = tid; e < (CL - 1) * HR; e += NT) {
-      const int pi = e / HR, j = e % HR;               // slot pi holds peer pi (< rank) or pi + 1
-      const uint32_t peer = pi < rank ? pi : pi + 1;
-      bulk_to_peer(peer_addr(smem_addr(R + j * RS + HW * rank), peer),
-                   smem_addr(P + (pi * HR + j) * HW), Sh::HALF_BYTES,
-                   peer_addr(smem_addr(&mbar[1]), peer));
+    for (int d = 0; d < B2; d++) {
+      const int j = cc + A2 * d;
+      g[j * N1 + q0 + qq] = cmul(v[d], r2[j]);
     }
-    ok = mbar_wait0(smem_addr(&mbar[1])) && ok;      // the other half of the own rows is back
-    cluster_arrive_release();                        // this CTA's incoming copies are complete
-    if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
-  } else {
-    __syncthreads();
-  }
-  // P6: items (j, blk): inverse row pass 1 over the block's A1 slots
-  // The twiddle W^{-bk c} of slot c of block bk is applied in P6 while
-  // A1 <= 16 (A1 twiddles per thread, kept in registers); at A1 = 32 that
-  // would double the live registers of the 32-point DFT, so P7, whose thread
-  // holds one slot c of every block, applies it instead (B1 twiddles per
-  // thread).  The products are the same either way.
-  constexpr bool TW6 = A1 <= 16;
-  {
-    const int bk = tid % B1;
-    float2 w[TW6 ? A1 : 1];
-    if constexpr (TW6) {
+    if (en) {
+      const double i1 = __ldg(p.I1 + q0 + qq);
 #pragma unroll
-      for (int c = 0; c < A1; c++) w[c] = cconj(__ldg(tw1 + bk * c));
-    }
-    for (int e = tid; e < HR * B1; e += NT) {
-      const int j = e / B1;
-      float2 *blk = R + j * RS + (A1 + 1) * bk;
-      float2 v[A1];
-#pragma unroll
-      for (int s = 0; s < A1; s++) v[s] = blk[s];
-      Dft<A1, +1>::run(v);
-#pragma unroll
-      for (int c = 0; c < A1; c++) {
-        if constexpr (TW6) blk[c] = c ? cmul(v[c], w[c]) : v[c];
-        else blk[c] = v[c];
-      }
+      for (int d = 0; d < B2; d++)
+        e_r += (double)(v[d].x * v[d].x + v[d].y * v[d].y) * (i1 + __ldg(p.I2 + cc + A2 * d));
     }
   }
-  __syncthreads();
-  // P7: items (j, c'): slot c' of every block -> i = c' + A1 d', Rot/2, store
-  float2 w7[TW6 ? 1 : B1];                           // A1 = 32: W^{-b c'} of this thread's slot
-  if constexpr (!TW6) {
-#pragma unroll
-    for (int b = 0; b < B1; b++) w7[b] = cconj(__ldg(tw1 + b * (tid % A1)));
-  }
-#pragma unroll 2
-  for (int e = tid; e < HR * A1; e += NT) {
-    const int j = e / A1, c = e % A1, jg = j0 + j;
-    const float2 rj = __ldg(rc2 + jg);
-    float2 v[B1];
-#pragma unroll
-    for (int b = 0; b < B1; b++) v[b] = R[j * RS + c + (A1 + 1) * b];
-    if constexpr (!TW6) {
-      if (c) {
-#pragma unroll
-        for (int b = 0; b < B1; b++) v[b] = cmul(v[b], w7[b]);
-      }
-    }
-    Dft<B1, +1>::run(v);
-#pragma unroll
-    for (int d = 0; d < B1; d++)
-      g[jg * N1 + c + A1 * d] = cmul(v[d], rot_at(r1, rj, c + A1 * d));
+  if (en) {
+    // E_kin (dr1 dr2 applied on the host) = [n2 S1 + S2 / n1] / (n1 n2): S1 sums
+    // T1 over the row transforms of D1 psi, S2 sums T2 over the column transforms
+    // of the row operator's output, which carries the factor n1 of the
+    // unnormalised row transform pair (Parseval along the other dimension)
+    const int run = sl / p.nl, ll = sl - run * p.nl;
+    const double wl = p.orth ? 1.0 : 1.0 / (ll + 0.5);
+    const double jj = (double)l;                     // rotational quantum number j = K + l
+    const double ek = block_sum(e_k1 / N1 + e_k2 / ((double)N1 * N1 * N2), red);
+    if (tid == 0) atomicAdd(p.esum + 3 * run, ek * wl);
+    const double er = block_sum(e_r, red);
+    if (tid == 0) atomicAdd(p.esum + 3 * run + 1, er * jj * (jj + 1.0) * wl);
   }
   // CL = 2: no CTA leaves while its shared memory may still be the source of
   // a copy (a peer arrives only once all of its incoming copies are
-  // complete); CL = 4 touches no peer's memory after the second swap's
-  // final barrier
+  // complete); CL = 4 touches no peer's memory after the swap's final barrier
   if constexpr (Sh::PSLOTS > 0) cluster_wait();
 }
 

@@ -53,6 +53,9 @@ struct ColumnParams {
   long set_stride;
   const int *run_nl;
   const int *run_order;    // tensor-core pass: tile order over runs (null: 0, 1, ...)
+  // energy step (null: none): per run r, esum[3 r + 2] += sum_k w_k sum_ij V |psi|^2 of the
+  // theta-space wavepacket after B, before the absorber (potential_energy, timeEvol.C:256-283)
+  double *esum;
 };
 
 struct FluxParams {
@@ -126,6 +129,14 @@ struct LineParams {
   const int *run_k;
   int jrows;
   int *status;             // device status word: bounded waits that ran out (0 = ok)
+  // energy step (null: none): per run r, esum[3 r] += the kinetic energy sum (the
+  // (T1 + T2) |FFT2 psi_l|^2 / (n1 n2) of kinetic_energy_for_legendre_psi,
+  // timeEvol.C:390-436) and esum[3 r + 1] += sum j(j+1) (I1 + I2) |psi_l|^2 after the
+  // second Rot(dt/2) (rotational_energy, timeEvol.C:323-360), both with the l-space
+  // weight 1 / (l + 1/2) (orth = 0; orth = 1: the state is psi_l / sqrt(l + 1/2), weight 1)
+  double *esum;
+  const double *T1, *T2, *I1, *I2;
+  int orth;
 };
 
 // Programmatic dependent launch: a hot kernel lets the next one start its
