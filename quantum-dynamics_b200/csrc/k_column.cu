@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
   __syncthreads();
 
   if (mode != COL_HEAD) {
-    double nsum = 0.0;
+    double nsum = 0.0, esum = 0.0;
     C *surf = reinterpret_cast<C *>(p.surf) + (long)run * p.surf_nrows * p.nth * p.n1;
     for (int e = threadIdx.x; e < p.nth * TP; e += blockDim.x) {
       const int k = e / TP, t = e % TP;
@@ -132,6 +132,11 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
       if (q >= p.n12) continue;
       const int j = (int)(q / p.n1), i = (int)(q % p.n1);
       C v = B[k * TP + t];
+      const long g = (long)k * p.n12 + q;
+      if (p.esum) {                               // potential energy, before the absorber
+        const double2 z = to_z(v);
+        esum += p.w[k] * (z.x * z.x + z.y * z.y) * p.pot[voff + g];
+      }
       if (p.d1) v = cscale(v, (R)(p.d1[i] * p.d2[j]));
       if (p.do_flux && j >= p.surf_j0 && j < p.surf_j0 + p.surf_nrows)
         surf[((long)(j - p.surf_j0) * p.nth + k) * p.n1 + i] = v;
@@ -139,7 +144,6 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
         const double2 z = to_z(v);
         nsum += p.w[k] * (z.x * z.x + z.y * z.y);
       }
-      const long g = (long)k * p.n12 + q;
       if (p.out_z) p.psi_z[zoff + g] = to_z(v);
       if (mode == COL_MID) v = cmul(v, vphase(p, voff + g, v));
       B[k * TP + t] = v;
@@ -147,6 +151,10 @@ __global__ void __launch_bounds__(256) k_column(ColumnParams p, int mode, int TP
     if (p.norm_out) {
       const double s = block_sum(nsum, red);
       if (threadIdx.x == 0) atomicAdd(p.norm_out + run, s);
+    }
+    if (p.esum) {
+      const double s = block_sum(esum, red);
+      if (threadIdx.x == 0) atomicAdd(p.esum + 3 * run + 2, s);
     }
     if (mode == COL_TAIL) return;
     __syncthreads();

@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     const bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
                       j < p.surf_j0 + p.surf_nrows;
     // slow tiles form the scaled theta-space state (EX: frow is uniform per tile)
-    const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow;
+    const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow || p.esum;
     float n_l = 0.f, sc = 1.f;
 
     if (mode != COL_HEAD) {
@@ -471,6 +471,20 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     if (mode != COL_HEAD) {
       tmem_ld_all<H>(my_d, dv);
       if (slow) {                               // whole-tile branch: the fast tiles skip it
+        if (p.esum) {                           // potential energy, before the absorber
+          double ep = 0.0;
+#pragma unroll
+          for (int u = 0; u < H; u++) {
+            const int k = c0 + u;
+            if (EX || (qok && k < nth)) {
+              const float x = dv[u] * sc;
+              ep += (double)(x * x) * p.pot[voff + (size_t)k * n12 + q];
+            }
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) ep += __shfl_xor_sync(0xffffffffu, ep, o);
+          if (lane == 0) atomicAdd(p.esum + 3 * run + 2, ep);
+        }
 #pragma unroll
         for (int u = 0; u < H; u++) {
           const int k = c0 + u;

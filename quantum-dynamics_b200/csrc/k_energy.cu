@@ -4,32 +4,48 @@
 //   E_rot = sum_l l(l+1)/(l+1/2) sum_ij |F psi|^2 (I1 + I2)   rotational_energy     :323-360
 //   E_kin = sum_k w_k sum_ij |DFT psi|^2 (T1 + T2) / (n1 n2)  kinetic_energy_for_psi :285-321
 // each multiplied by dr1 dr2 on the host.
+#include <algorithm>
 #include "qd_kernels.h"
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_e_pot_rot(EnergyParams e)
+// a tile of TQ grid columns at a time: their theta-space values are read
+// once into shared memory ([n_theta][TQ]), then every order l is contracted
+// from there
+__global__ void __launch_bounds__(256) k_e_pot_rot(EnergyParams e, int TQ)
 {
+  extern __shared__ double2 zt[];
   __shared__ double red[32];
   double srot = 0.0, spot = 0.0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < e.n12;
-       q += (long)gridDim.x * blockDim.x) {
-    const int j = (int)(q / e.n1), i = (int)(q % e.n1);
-    for (int k = 0; k < e.nth; k++) {
-      const double2 z = e.psi_z[(long)k * e.n12 + q];
-      spot += e.w[k] * (z.x * z.x + z.y * z.y) * e.pot[(long)k * e.n12 + q];
+  const long ntile = (e.n12 + TQ - 1) / TQ;
+  for (long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const long q0 = tile * TQ;
+    __syncthreads();                               // the previous tile's reads are done
+    for (int x = threadIdx.x; x < e.nth * TQ; x += blockDim.x) {
+      const int k = x / TQ, t = x % TQ;
+      const long q = q0 + t;
+      double2 z = make_double2(0.0, 0.0);
+      if (q < e.n12) {
+        z = e.psi_z[(long)k * e.n12 + q];
+        spot += e.w[k] * (z.x * z.x + z.y * z.y) * e.pot[(long)k * e.n12 + q];
+      }
+      zt[x] = z;
     }
-    const double I = e.I1[i] + e.I2[j];
-    for (int l = e.K == 0 ? 1 : 0; l < e.nl; l++) {   // j(j+1) = 0 only for j = 0
+    __syncthreads();
+    for (int x = threadIdx.x; x < e.nl * TQ; x += blockDim.x) {
+      const int l = x / TQ, t = x % TQ;
+      const long q = q0 + t;
+      if (q >= e.n12 || (e.K == 0 && l == 0)) continue;   // j(j+1) = 0 only for j = 0
       double2 c = make_double2(0.0, 0.0);
       for (int k = 0; k < e.nth; k++) {
-        const double2 z = e.psi_z[(long)k * e.n12 + q];
+        const double2 z = zt[k * TQ + t];
         const double wp = e.WP[k * e.nl + l];
         c.x += z.x * wp;
         c.y += z.y * wp;
       }
+      const int j = (int)(q / e.n1), i = (int)(q % e.n1);
       const double jr = (double)(e.K + l);           // j = K + l (centrifugal sudden)
-      srot += (c.x * c.x + c.y * c.y) * I * jr * (jr + 1) / (l + 0.5);
+      srot += (c.x * c.x + c.y * c.y) * (e.I1[i] + e.I2[j]) * jr * (jr + 1) / (l + 0.5);
     }
   }
   srot = block_sum(srot, red);
@@ -61,7 +77,14 @@ int energies_launches() { return 5; }
 
 cudaError_t launch_energies(const EnergyParams &e, cudaStream_t s)
 {
-  k_e_pot_rot<<<148, 256, 0, s>>>(e);
+  const int TQ = (int)std::max(1L, std::min(32L, (long)(96 * 1024 / (16 * e.nth))));
+  const size_t sm = sizeof(double2) * e.nth * TQ;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_e_pot_rot, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    attr_set = true;
+  }
+  k_e_pot_rot<<<2 * 148, 256, sm, s>>>(e, TQ);
   cudaError_t err = cudaMemcpyAsync(e.scratch, e.psi_z, sizeof(double2) * e.n12 * e.nth,
                                     cudaMemcpyDeviceToDevice, s);
   if (err != cudaSuccess) return err;

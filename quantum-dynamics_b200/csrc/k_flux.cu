@@ -40,11 +40,12 @@ __global__ void __launch_bounds__(256) k_flux_phase(AccumParams p)
 // phi[e][q] += sum_t phase[e][t] psi_s[t][q] (and dphi with the gradient), a
 // complex FP64 GEMM per run.  CTA tile: GE energies x GQ surface points x
 // {psi_s, d psi_s}; each thread owns 4 energies x 4 columns (2 points x 2
-// fields) in registers.  KT steps of phases and history are staged in shared
-// memory by asynchronous copies into two buffers, so the next KT steps load
-// while the current ones are multiplied; the history is read from HBM once
-// per energy tile.
-constexpr int GE = 64, GQ = 32, KT = 10;
+// fields) in registers, GE / 4 x 16 threads.  KT steps of phases and history
+// are staged in shared memory by asynchronous copies into two buffers, so the
+// next KT steps load while the current ones are multiplied; the history is
+// read from HBM once per energy tile.  The variant (GE, KT) is picked per
+// shape by the autotuner.
+constexpr int GQ = 32;
 
 __device__ __forceinline__ void cp16(void *dst, const void *src, bool valid)
 {
@@ -54,21 +55,23 @@ __device__ __forceinline__ void cp16(void *dst, const void *src, bool valid)
                : "memory");
 }
 
-__global__ void __launch_bounds__(256) k_flux_gemm(AccumParams p)
+template <int GE, int KT>
+__global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
 {
+  constexpr int NT = GE * 4;                    // threads: GE / 4 energy groups x 16
   __shared__ double2 As[2][GE][KT + 1];         // phases (padded rows)
   __shared__ double2 Bs[2][KT][2 * GQ];         // cols 0..GQ-1 psi_s, GQ..2GQ-1 gradient
   const int tid = threadIdx.x;
-  const int te = tid >> 4, tc = tid & 15;       // 16 energy groups x 16 column groups
+  const int te = tid >> 4, tc = tid & 15;       // GE/4 energy groups x 16 column groups
   const int e0 = blockIdx.x * GE, q0 = blockIdx.y * GQ, run = blockIdx.z;
   const double2 *ph = p.phase + ((size_t)run * p.ne) * TMAX;
   auto stage = [&](int buf, int t0) {
-    for (int x = tid; x < GE * KT; x += 256) {
+    for (int x = tid; x < GE * KT; x += NT) {
       const int e = x / KT, t = x % KT;
       const bool ok = e0 + e < p.ne && t0 + t < p.nt;
       cp16(&As[buf][e][t], ok ? ph + (size_t)(e0 + e) * TMAX + t0 + t : ph, ok);
     }
-    for (int x = tid; x < KT * 2 * GQ; x += 256) {
+    for (int x = tid; x < KT * 2 * GQ; x += NT) {
       const int t = x / (2 * GQ), c = x % (2 * GQ), q = q0 + (c % GQ);
       const bool ok = t0 + t < p.nt && q < p.nq;
       const size_t o = ok ? ((size_t)(t0 + t) * p.nruns + run) * p.nq + q : 0;
@@ -96,7 +99,7 @@ __global__ void __launch_bounds__(256) k_flux_gemm(AccumParams p)
     for (int k = 0; k < KT; k++) {             // rows past nt were zero-filled
       double2 a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = As[buf][te + 16 * i][k];
+      for (int i = 0; i < 4; i++) a[i] = As[buf][te + (GE / 4) * i][k];
 #pragma unroll
       for (int j = 0; j < 4; j++) b[j] = Bs[buf][k][tc + 16 * j];
 #pragma unroll
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(256) k_flux_gemm(AccumParams p)
   // load wait for the one before, since phi and dphi may alias as far as the
   // compiler knows)
   auto at = [&](int i, int j) -> double2 * {
-    const int e = e0 + te + 16 * i, c = tc + 16 * j, q = q0 + (c % GQ);
+    const int e = e0 + te + (GE / 4) * i, c = tc + 16 * j, q = q0 + (c % GQ);
     if (e >= p.ne || q >= p.nq) return nullptr;
     return (c < GQ ? p.fai : p.dfai) + ((size_t)run * p.ne + e) * p.nq + q;
   };
@@ -157,6 +160,12 @@ __global__ void __launch_bounds__(256) k_crp(CrpParams p)
   if (threadIdx.x == 0) p.crp[b] = s / p.eta_sq[b] * p.dr1_mu2;
 }
 
+template <int GE, int KT> void launch_gemm(const AccumParams &p, cudaStream_t s)
+{
+  dim3 grid((p.ne + GE - 1) / GE, (p.nq + GQ - 1) / GQ, p.nruns);
+  k_flux_gemm<GE, KT><<<grid, GE * 4, 0, s>>>(p);
+}
+
 }  // namespace
 
 template <typename R>
@@ -169,14 +178,20 @@ cudaError_t launch_flux_prep(const FluxParams &p, cudaStream_t s)
 template cudaError_t launch_flux_prep<float>(const FluxParams &, cudaStream_t);
 template cudaError_t launch_flux_prep<double>(const FluxParams &, cudaStream_t);
 
+int flux_variants() { return 4; }
+
 cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 {
   if (p.nt <= 0) return cudaSuccess;
   if (p.nt > TMAX) return cudaErrorInvalidValue;
   const int n = p.nruns * p.ne * p.nt;
   k_flux_phase<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, s>>>(p);
-  dim3 grid((p.ne + GE - 1) / GE, (p.nq + GQ - 1) / GQ, p.nruns);
-  k_flux_gemm<<<grid, 256, 0, s>>>(p);
+  switch (p.variant) {   // (energies per CTA, steps per staged chunk)
+    case 1: launch_gemm<64, 5>(p, s); break;
+    case 2: launch_gemm<32, 10>(p, s); break;
+    case 3: launch_gemm<32, 15>(p, s); break;
+    default: launch_gemm<64, 10>(p, s); break;
+  }
   return cudaGetLastError();
 }
 

@@ -48,10 +48,25 @@ __global__ void __launch_bounds__(256) k_rows(LineParams p, int dir)
   __syncthreads();
   C *res = smem_fft_lines<C>(bufA, bufB, p.pl1, nrows, p.n1, 1, false,
                              reinterpret_cast<const C *>(p.tw1), dir);
+  double er = 0.0;                               // energy step: sum (I1 + I2) |psi_l|^2
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     C v = res[e];
-    if (dir > 0) v = cmul(v, Phase<R>::rot(p, l, j0 + e / p.n1, e % p.n1));
+    if (dir > 0) {
+      const int j = j0 + e / p.n1, i = e % p.n1;
+      v = cmul(v, Phase<R>::rot(p, l, j, i));
+      if (p.esum) {
+        const double2 z = to_z(v);
+        er += (z.x * z.x + z.y * z.y) * (p.I1[i] + p.I2[j]);
+      }
+    }
     slice[e] = v;
+  }
+  if (dir > 0 && p.esum) {
+    __shared__ double red[32];
+    const int run = sl / p.nl, ll = sl - run * p.nl;
+    const double wl = p.orth ? 1.0 : 1.0 / (ll + 0.5);
+    const double s = block_sum(er, red);
+    if (threadIdx.x == 0) atomicAdd(p.esum + 3 * run + 1, s * (double)l * (l + 1.0) * wl);
   }
 }
 
@@ -83,9 +98,21 @@ __global__ void __launch_bounds__(256) k_cols(LineParams p)
     }
     return;
   }
+  double ek = 0.0;                               // energy step: sum (T1 + T2) |FFT2 psi_l|^2
   for (int e = threadIdx.x; e < nel; e += blockDim.x) {
     const int j = e / ncols, c = e % ncols;
+    if (p.esum) {
+      const double2 z = to_z(res[j * cb + c]);
+      ek += (z.x * z.x + z.y * z.y) * (p.T1[i0 + c] + p.T2[j]);
+    }
     res[j * cb + c] = cmul(res[j * cb + c], Phase<R>::kin(p, j, i0 + c));
+  }
+  if (p.esum) {
+    __shared__ double red[32];
+    const int run = sl / p.nl, ll = sl - run * p.nl;
+    const double wl = p.orth ? 1.0 : 1.0 / (ll + 0.5);
+    const double s = block_sum(ek, red);
+    if (threadIdx.x == 0) atomicAdd(p.esum + 3 * run, s * wl / (double)p.n12);
   }
   __syncthreads();
   res = smem_fft_lines<C>(res, other, p.pl2, ncols, 1, cb, true, tw2, +1);

@@ -199,6 +199,7 @@ struct qd_handle {
   float2 *d_rc1 = nullptr, *d_rc2 = nullptr, *d_kc1 = nullptr, *d_kc2 = nullptr;
   int *d_lstatus = nullptr;       // status word of the l-space kernels (0 = ok)
   int slice_cluster = 0;          // l-space kernel (LineParams::cluster code)
+  int flux_variant = 0;           // flux-accumulation GEMM tile variant (tune_flux)
   double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
   void *d_lpsi = nullptr;
@@ -211,6 +212,16 @@ struct qd_handle {
   int norms_cap = 0;
   TcPlan tc;                      // tensor-core column pass (FP32), if usable
   bool use_tc = false;
+  // energies inside the propagation (qd_set_energy_interval)
+  int energy_every = 0;
+  double *d_esum = nullptr;       // [slot][run][3] sums of the current call
+  int esum_cap = 0;
+  double *esum_col = nullptr;     // slot of the next column / l-space launch (null: none)
+  double *esum_lines = nullptr;
+  bool lines_split = false;       // this step's l-space pass on the split kernels
+  std::vector<double> energy_log; // records: step, run, E_kin, E_rot, E_pot
+  double2 *d_escratch = nullptr;  // on-demand energies: DFT scratch and sums
+  double *d_esums3 = nullptr;
 
   FftPlan pl1, pl2;
   int ring_fill = 0;
@@ -273,6 +284,7 @@ struct qd_handle {
     if (st) cudaStreamSynchronize(st);
     for (void *p : allocs) cudaFreeAsync(p, st);
     if (d_norms) cudaFreeAsync(d_norms, st);
+    if (d_esum) cudaFreeAsync(d_esum, st);
     if (d_flush) cudaFreeAsync(d_flush, st);
     tc_plan_destroy(tc, st);
     if (st) cudaStreamSynchronize(st);
@@ -404,8 +416,7 @@ int check_status(qd_handle *h)
   return QD_OK;
 }
 
-template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double *norm_out,
-                                       bool out_z)
+ColumnParams column_params(qd_handle *h)
 {
   ColumnParams p{};
   p.n1 = h->n1; p.n2 = h->n2; p.nth = h->nth; p.nl = h->nl; p.n12 = h->n12;
@@ -414,14 +425,24 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
   p.P = h->d_P; p.WP = h->d_WP; p.P32 = h->d_P32; p.WP32 = h->d_WP32;
   p.P32lo = h->d_P32lo; p.WP32lo = h->d_WP32lo;
   p.expV = h->d_expV; p.expV32 = h->d_expV32; p.pot = h->d_pot; p.dt = h->dt;
-  p.prestep = (mode == COL_HEAD && h->steps == 0);
   p.d1 = h->have_dump ? h->d_d1 : nullptr;
   p.d2 = h->have_dump ? h->d_d2 : nullptr;
-  p.do_flux = flux ? 1 : 0;
   p.surf = h->d_surf; p.surf_j0 = h->surf_j0; p.surf_nrows = 2 * h->h + 1;
-  p.w = h->d_w; p.norm_out = norm_out; p.out_z = out_z ? 1 : 0;
+  p.w = h->d_w;
   p.run_set = h->d_run_set; p.set_stride = (long)h->nth * h->nl; p.run_nl = h->d_run_nl;
   p.run_order = h->d_run_order;
+  return p;
+}
+
+template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double *norm_out,
+                                       bool out_z)
+{
+  ColumnParams p = column_params(h);
+  p.prestep = (mode == COL_HEAD && h->steps == 0);
+  p.do_flux = flux ? 1 : 0;
+  p.norm_out = norm_out;
+  p.out_z = out_z ? 1 : 0;
+  p.esum = mode == COL_HEAD ? nullptr : h->esum_col;
   cudaError_t e;
   TRY(prof_mark(h, -1));
   if (sizeof(R) == 4 && h->use_tc) e = launch_column_tc(h->tc, p, mode, h->st);
@@ -433,10 +454,22 @@ template <typename R> int issue_column(qd_handle *h, int mode, bool flux, double
     // the surface rows of this step go to ring slot ring_fill; with the fused
     // slice kernel that preparation rides along in the next l-space launch
     h->flux_pending = h->ring_fill;
-    if (!(sizeof(R) == 4 && h->slice_cluster > 0) || mode == COL_TAIL)
+    if (!(sizeof(R) == 4 && h->slice_cluster > 0 && !h->lines_split) || mode == COL_TAIL)
       TRY(issue_flux_prep<R>(h));
   }
   return QD_OK;
+}
+
+AccumParams accum_params(const qd_handle *h)
+{
+  AccumParams a{};
+  a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
+  a.nruns = h->nruns;
+  a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
+  a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
+  a.phase = h->d_phase;
+  a.variant = h->flux_variant;
+  return a;
 }
 
 // ring bookkeeping after the flux preparation of a step has been issued
@@ -445,12 +478,7 @@ int after_flux_prep(qd_handle *h)
   h->flux_pending = -1;
   h->ring_fill++;
   if (h->ring_fill == QD_RING) {
-    AccumParams a{};
-    a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
-    a.nruns = h->nruns;
-    a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
-    a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
-    a.phase = h->d_phase;
+    const AccumParams a = accum_params(h);
     TRY(prof_mark(h, -1));
     CU(launch_flux_accum(a, h->st));
     g_launches += flux_accum_launches();
@@ -486,6 +514,8 @@ LineParams line_params(qd_handle *h, bool f32)
   p.pl1 = h->pl1; p.pl2 = h->pl2;
   p.run_k = h->d_run_k; p.jrows = h->jrows;
   p.status = h->d_lstatus;
+  p.T1 = h->d_T1; p.T2 = h->d_T2; p.I1 = h->d_I1; p.I2 = h->d_I2;
+  p.orth = h->prec == QD_PREC_FP32 && h->use_tc ? 1 : 0;
   return p;
 }
 
@@ -557,9 +587,108 @@ int tune_slice(qd_handle *h)
   return QD_OK;
 }
 
+// Times `launch` (reps launches after one warm-up) on the handle's stream, ms
+// per launch; a negative value if a launch failed.
+template <typename F> float time_launches(qd_handle *h, F launch, int reps = 3)
+{
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float ms = -1.f;
+  bool ok = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+  ok = ok && launch() == cudaSuccess && cudaEventRecord(e0, h->st) == cudaSuccess;
+  for (int i = 0; i < reps && ok; i++) ok = launch() == cudaSuccess;
+  ok = ok && cudaEventRecord(e1, h->st) == cudaSuccess &&
+       cudaStreamSynchronize(h->st) == cudaSuccess &&
+       cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    ms = -1.f;
+  } else {
+    ms /= reps;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return ms;
+}
+
+// Autotuner of the flux-accumulation GEMM: each tile variant accumulates one
+// full chunk of (still zero) history into the handle's phi_E, which is
+// cleared again afterwards; the fastest is kept per shape for the process.
+// QD_FLUX_VARIANT=0..3 forces a variant.
+int tune_flux(qd_handle *h)
+{
+  h->flux_variant = 0;
+  if (!h->do_crp) return QD_OK;
+  if (const char *force = getenv("QD_FLUX_VARIANT")) {
+    const int v = atoi(force);
+    h->flux_variant = v >= 0 && v < flux_variants() ? v : 0;
+    return QD_OK;
+  }
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, int>, int> chosen;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, h->n1, h->nth, h->ne, h->nruns);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = chosen.find(key);
+    if (it != chosen.end()) {
+      h->flux_variant = it->second;
+      return QD_OK;
+    }
+  }
+  AccumParams a = accum_params(h);
+  a.nt = QD_RING;
+  a.t0 = 0;
+  float best = 1e30f;
+  for (int v = 0; v < flux_variants(); v++) {
+    a.variant = v;
+    const float ms = time_launches(h, [&] { return launch_flux_accum(a, h->st); });
+    if (ms >= 0.f && ms < best) { best = ms; h->flux_variant = v; }
+  }
+  const size_t bytes = sizeof(double2) * (size_t)h->nth * h->n1 * h->ne * h->nruns;
+  CU(cudaMemsetAsync(h->d_fai, 0, bytes, h->st));
+  CU(cudaMemsetAsync(h->d_dfai, 0, bytes, h->st));
+  std::lock_guard<std::mutex> lock(mu);
+  chosen[key] = h->flux_variant;
+  return QD_OK;
+}
+
+// Autotuner of the complex64 column pass: the tensor-core kernel against the
+// SIMT one, both on the handle's zero l-space buffer (a zero wavepacket stays
+// zero); the faster is kept per shape for the process.  QD_COLUMN_PATH forces
+// the choice.
+int tune_column(qd_handle *h)
+{
+  if (h->prec != QD_PREC_FP32 || !h->use_tc || getenv("QD_COLUMN_PATH")) return QD_OK;
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, int, int, int>, bool> chosen;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, h->n1, h->n2, h->nth, h->nl, h->nruns, h->nsets);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = chosen.find(key);
+    if (it != chosen.end()) {
+      h->use_tc = it->second;
+      return QD_OK;
+    }
+  }
+  ColumnParams p = column_params(h);
+  const float tc = time_launches(h, [&] { return launch_column_tc(h->tc, p, COL_MID, h->st); });
+  const float simt = time_launches(h, [&] { return launch_column<float>(p, COL_MID, h->st); });
+  CU(cudaMemsetAsync(h->d_lpsi, 0, sizeof(float2) * h->n12 * h->nl * h->nruns, h->st));
+  if (tc < 0.f) return set_err(QD_ERR_CUDA, "tensor-core column pass failed while tuning");
+  h->use_tc = !(simt >= 0.f && simt < tc);
+  std::lock_guard<std::mutex> lock(mu);
+  chosen[key] = h->use_tc;
+  return QD_OK;
+}
+
 template <typename R> int issue_lines(qd_handle *h)
 {
   LineParams p = line_params(h, sizeof(R) == 4);
+  p.esum = h->esum_lines;
+  if (h->lines_split) p.cluster = 0;            // energy step on a kernel without the sums
   const bool fused_flux = p.cluster > 0 && h->flux_pending >= 0;
   if (fused_flux) {
     p.flux = flux_params(h);
@@ -585,12 +714,7 @@ template <typename R> int issue_lines(qd_handle *h)
 int flush_accum(qd_handle *h)
 {
   if (h->ring_fill == 0) return QD_OK;
-  AccumParams a{};
-  a.nq = h->nth * h->n1; a.ne = h->ne; a.nt = h->ring_fill; a.t0 = h->acc_done;
-  a.nruns = h->nruns;
-  a.dt = h->dt; a.energies = h->d_energies; a.ring_psi = h->d_ring_psi;
-  a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
-  a.phase = h->d_phase;
+  const AccumParams a = accum_params(h);
   CU(launch_flux_accum(a, h->st));
   g_launches += flux_accum_launches();
   h->acc_done += h->ring_fill;
@@ -643,7 +767,32 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
     h->norms_cap = n * R;
   }
   CU(cudaMemsetAsync(h->d_norms, 0, sizeof(double) * n * R, h->st));
+  // energy steps of this call: t in (steps0, steps0 + n] with t % every == 0.
+  // Step t's kinetic and rotational sums come from its l-space launch, its
+  // potential sum from the next column launch (B of step t), all into slot
+  // t / every - steps0 / every - 1 of d_esum.
+  const int every = h->energy_every, steps0 = h->steps;
+  const int nslots = every > 0 ? (steps0 + n) / every - steps0 / every : 0;
+  if (nslots > 0) {
+    if (h->esum_cap < nslots * R * 3) {
+      if (h->d_esum) cudaFreeAsync(h->d_esum, h->st);
+      h->d_esum = nullptr;
+      CU(cudaMallocAsync(&h->d_esum, sizeof(double) * nslots * R * 3, h->st));
+      h->esum_cap = nslots * R * 3;
+    }
+    CU(cudaMemsetAsync(h->d_esum, 0, sizeof(double) * nslots * R * 3, h->st));
+  }
+  auto slot = [&](int t) -> double * {
+    if (every <= 0 || t <= steps0 || t > steps0 + n || t % every) return nullptr;
+    return h->d_esum + (long)(t / every - steps0 / every - 1) * R * 3;
+  };
+  const bool split_ok = h->prec == QD_PREC_FP64 || h->slice_cluster == 0 ||
+                        slice_is_rf(h->slice_cluster);
   for (int s = 0; s < n; s++) {
+    const bool redo = !h->started || (s == 0 && h->last_finalized);
+    h->esum_col = redo ? nullptr : slot(h->steps);
+    h->esum_lines = slot(h->steps + 1);
+    h->lines_split = h->esum_lines && !split_ok;
     if (timed && flush_bytes) {       // L2 flush outside the timed spans: write, then read back
       CU(cudaMemsetAsync(h->d_flush, s & 0xff, flush_bytes, h->st));
       CU(launch_l2_read(h->d_flush, flush_bytes, h->st));
@@ -661,13 +810,20 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
     h->steps++;
     if (timed && s < n - 1) CU(cudaEventRecord(h->events[2 * s + 1], h->st));
   }
+  h->esum_col = slot(h->steps);
+  h->esum_lines = nullptr;
+  h->lines_split = false;
   TRY(issue_column<Real>(h, COL_TAIL, h->do_crp, h->d_norms + (long)(n - 1) * R, false));
+  h->esum_col = nullptr;
   h->last_finalized = true;
   TRY(compute_crp(h));
   if (timed) CU(cudaEventRecord(h->events[2 * n - 1], h->st));
-  std::vector<double> nb((size_t)n * R);
+  std::vector<double> nb((size_t)n * R), eb((size_t)nslots * R * 3);
   CU(cudaMemcpyAsync(nb.data(), h->d_norms, sizeof(double) * n * R, cudaMemcpyDeviceToHost,
                      h->st));
+  if (nslots > 0)
+    CU(cudaMemcpyAsync(eb.data(), h->d_esum, sizeof(double) * nslots * R * 3,
+                       cudaMemcpyDeviceToHost, h->st));
   CU(cudaStreamSynchronize(h->st));
   TRY(prof_collect(h));
   TRY(check_status(h));
@@ -710,6 +866,14 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
     }
   }
   for (long s = 0; s < (long)n * R; s++) h->norms_host.push_back(nb[s] * scale);
+  for (int e = 0; e < nslots; e++) {
+    const int t = (steps0 / every + 1 + e) * every;
+    for (int r = 0; r < R; r++) {
+      const double *v = &eb[((size_t)e * R + r) * 3];
+      const double rec[5] = {(double)t, (double)r, v[0] * scale, v[1] * scale, v[2] * scale};
+      h->energy_log.insert(h->energy_log.end(), rec, rec + 5);
+    }
+  }
   return QD_OK;
 }
 
@@ -961,7 +1125,9 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     if (rc == QD_OK) h->use_tc = true;
     else if (rc != QD_ERR_UNSUPPORTED) return rc;
   }
+  TRY(tune_column(h));
   TRY(tune_slice(h));
+  TRY(tune_flux(h));
   CU(cudaStreamSynchronize(h->st));
   return QD_OK;
 }
@@ -1016,22 +1182,19 @@ int energies(qd_handle *h, int run, double out4[4])
   e.w = h->d_w; e.P = h->d_P + soff; e.WP = h->d_WP + soff; e.K = h->run_k[run];
   e.T1 = h->d_T1; e.T2 = h->d_T2; e.I1 = h->d_I1; e.I2 = h->d_I2;
   e.tw1 = h->d_tw1_64; e.tw2 = h->d_tw2_64; e.pl1 = h->pl1; e.pl2 = h->pl2;
-  double *dsum = nullptr;
-  double2 *scratch = nullptr;
-  CU(cudaMalloc(&dsum, 3 * sizeof(double)));
-  cudaError_t err = cudaMalloc(&scratch, sizeof(double2) * h->n12 * h->nth);
-  if (err != cudaSuccess) { cudaFree(dsum); CU(err); }
-  e.sums = dsum;
-  e.scratch = scratch;
-  err = cudaMemsetAsync(dsum, 0, 3 * sizeof(double), h->st);
-  if (err == cudaSuccess) err = launch_energies(e, h->st);
+  // the DFT scratch and the sums stay with the handle (its memory pool)
+  // after the first call
+  if (!h->d_escratch) {
+    TRY(h->alloc(h->d_escratch, (size_t)h->n12 * h->nth));
+    TRY(h->alloc(h->d_esums3, 3));
+  }
+  e.sums = h->d_esums3;
+  e.scratch = h->d_escratch;
+  CU(cudaMemsetAsync(e.sums, 0, 3 * sizeof(double), h->st));
+  CU(launch_energies(e, h->st));
   double s[3] = {0, 0, 0};
-  if (err == cudaSuccess)
-    err = cudaMemcpyAsync(s, dsum, sizeof s, cudaMemcpyDeviceToHost, h->st);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(h->st);
-  cudaFree(dsum);
-  cudaFree(scratch);
-  CU(err);
+  CU(cudaMemcpyAsync(s, e.sums, sizeof s, cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
   g_launches += energies_launches();
   const double dd = h->data->r1.dr * h->data->r2.dr;
   out4[0] = s[0] * dd / ((double)h->n1 * h->n2);   // kinetic (unnormalised DFT)
@@ -1312,6 +1475,34 @@ int qd_energies_run(qd_handle *h, int32_t run, double out4[4])
 }
 
 int qd_energies(qd_handle *h, double out4[4]) { return qd_energies_run(h, 0, out4); }
+
+int qd_set_energy_interval(qd_handle *h, int32_t every)
+{
+  if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
+  if (every < 0) return set_err(QD_ERR_INVALID, "energy interval %d < 0", every);
+  h->energy_every = every;
+  return QD_OK;
+}
+
+int qd_get_energy_log_run(qd_handle *h, int32_t run, double *out, int32_t cap, int32_t *n_out)
+{
+  if (!h || !n_out || cap < 0 || (cap > 0 && !out)) return set_err(QD_ERR_INVALID, "bad argument");
+  if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
+  std::vector<const double *> mine;
+  for (size_t i = 0; i + 5 <= h->energy_log.size(); i += 5)
+    if ((int)h->energy_log[i + 1] == run) mine.push_back(&h->energy_log[i]);
+  const size_t k = std::min(mine.size(), (size_t)cap), first = mine.size() - k;
+  for (size_t i = 0; i < k; i++) {
+    const double *r = mine[first + i];
+    out[5 * i] = r[0];
+    out[5 * i + 1] = r[2];
+    out[5 * i + 2] = r[3];
+    out[5 * i + 3] = r[4];
+    out[5 * i + 4] = r[2] + r[3] + r[4];
+  }
+  *n_out = (int32_t)k;
+  return QD_OK;
+}
 
 int qd_checkpoint(qd_handle *h, const char *path)
 {

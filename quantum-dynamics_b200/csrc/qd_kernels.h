@@ -188,9 +188,11 @@ struct AccumParams {
   const double *energies;
   const double2 *ring_psi, *ring_g;
   double2 *fai, *dfai;
-  double2 *phase;          // workspace [nruns][ne][128] for the chunk's e^{iEt} factors
+  double2 *phase;          // workspace [nruns][ne][FLUX_CHUNK] for the chunk's e^{iEt} factors
+  int variant;             // GEMM tile variant, 0 .. flux_variants() - 1 (the autotuner's choice)
 };
 int flux_accum_launches();
+int flux_variants();
 
 struct CrpParams {
   int n1, nth, ne, nruns;

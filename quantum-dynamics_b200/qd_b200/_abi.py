@@ -203,6 +203,9 @@ def lib():
         "qd_get_norms_run": (C.c_int, [H, C.c_int32, c_double_p, C.c_int32]),
         "qd_energies_run": (C.c_int, [H, C.c_int32, c_double_p]),
         "qd_energies_noalloc": (C.c_int, [H, C.c_int32, c_double_p]),
+        "qd_set_energy_interval": (C.c_int, [H, C.c_int32]),
+        "qd_get_energy_log_run": (C.c_int, [H, C.c_int32, c_double_p, C.c_int32,
+                                            P(C.c_int32)]),
         "qd_read_grids": (C.c_int, [C.c_char_p, C.c_int32, c_double_p, c_double_p]),
         "qd_legendre_matrix": (C.c_int, [C.c_int32, C.c_int32, c_double_p, c_double_p]),
         "qd_cs_legendre": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, c_double_p, c_double_p]),

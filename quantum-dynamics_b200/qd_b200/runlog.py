@@ -13,10 +13,13 @@ record is written per chunk:
 `absorbed` the norm each run lost during the chunk (through the absorbers
 only: the propagator is unitary otherwise), counted from the norm after the
 previous record's last step, or, for the first record of a handle that has
-made no step before, from the end of the chunk's first step; `energies` are those of run 0, in
-hartree, computed on the device in FP64 (omitted with energies=False).  The
-time is the wall clock around the chunk, which ends when the chunk's norms are
-back on the host.
+made no step before, from the end of the chunk's first step; `energies` are those of run 0
+after the chunk's last step, in hartree, summed on the device in FP64 by the
+step's own kernels (qd_set_energy_interval; chunks end on multiples of
+`interval`, the first one shortened to reach one) or, for a last chunk that
+ends elsewhere, by the on-demand energies path (omitted with energies=False).
+The time is the wall clock around the chunk, which ends when the chunk's norms
+are back on the host.
 """
 import json
 import time
@@ -38,9 +41,11 @@ def propagate_logged(prop, n_steps, interval, out, energies=True, clock=time.per
             prev = [float(prop.norms(1, r)[0]) for r in range(runs)]
         except Exception:           # no norm recorded by this handle yet
             prev = None
+    if energies:
+        prop.set_energy_interval(interval)
     done = 0
     while done < n_steps:
-        k = min(interval, n_steps - done)
+        k = min(interval - prop.steps % interval, n_steps - done)
         t0 = clock()
         prop.propagate(k)
         norms = [prop.norms(k, r) for r in range(runs)]
@@ -53,11 +58,17 @@ def propagate_logged(prop, n_steps, interval, out, energies=True, clock=time.per
                "grid_pt_steps_per_s": points * k / dt if dt > 0 else None,
                "norm": last, "absorbed": [a - b for a, b in zip(start, last)]}
         if energies:
-            e = prop.energies(0)
+            log = prop.energy_log(0, 1)
+            if len(log) and int(log[-1][0]) == prop.steps:
+                e = log[-1][1:]
+            else:
+                e = prop.energies(0)
             rec["energies"] = {"kinetic": float(e[0]), "rotational": float(e[1]),
                                "potential": float(e[2]), "total": float(e[3])}
         out.write(json.dumps(rec) + "\n")
         out.flush()
         records.append(rec)
         prev = last
+    if energies:
+        prop.set_energy_interval(0)
     return records

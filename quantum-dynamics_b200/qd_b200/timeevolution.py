@@ -119,6 +119,21 @@ class Propagator:
         check(lib().qd_energies_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p)))
         return out
 
+    def set_energy_interval(self, every):
+        """Energies inside the propagation on every step whose count is a
+        multiple of `every` (0: off); read them with energy_log()."""
+        check(lib().qd_set_energy_interval(self._h, int(every)))
+        return self
+
+    def energy_log(self, run=0, cap=1 << 20):
+        """Recorded energies of one run: array (n, 5) of step, E_kin, E_rot,
+        E_pot, E_total (hartree), oldest first."""
+        out = np.empty((int(cap), 5))
+        n = C.c_int32()
+        check(lib().qd_get_energy_log_run(self._h, int(run), out.ctypes.data_as(_abi.c_double_p),
+                                          int(cap), C.byref(n)))
+        return out[:n.value].copy()
+
     def checkpoint(self, path):
         check(lib().qd_checkpoint(self._h, str(path).encode()))
 
