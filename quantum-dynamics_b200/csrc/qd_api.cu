@@ -159,6 +159,129 @@ struct DevGuard {
   }
 };
 
+// Copies between the caller's (pageable) arrays and the device through
+// page-locked staging buffers, allocated once per process and reused: host
+// threads copy one chunk at a time into a staging buffer -- checking the
+// words for NaN/Inf on the way when asked, while they are in cache -- and the
+// copy engine moves each chunk as soon as it is staged, so the host copy of
+// chunk c overlaps the transfer of chunk c - 1.  One transfer at a time per
+// process; without page-locked memory the copies fall back to plain
+// cudaMemcpyAsync from the caller's arrays.
+class Staging {
+ public:
+  static constexpr size_t CHUNK = size_t(32) << 20;   // bytes per staging buffer
+  static constexpr int NBUF = 4;
+  static constexpr size_t LARGE = size_t(64) << 20;   // transfers from this size on use it
+
+  static Staging &get()
+  {
+    static Staging s;
+    return s;
+  }
+  // host -> device; *finite (if given) = no word of src is NaN/Inf
+  cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t st, bool *finite)
+  {
+    if (finite) *finite = true;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (bytes < LARGE || !ready()) {
+      if (finite) *finite = all_finite(static_cast<const double *>(src), bytes / 8);
+      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    }
+    bool ok_all = true;
+    for (size_t off = 0, c = 0; off < bytes; off += CHUNK, c++) {
+      const int b = (int)(c % NBUF);
+      cudaError_t e = cudaEventSynchronize(ev_[b]);     // the buffer's last transfer is done
+      if (e != cudaSuccess) return e;
+      const size_t n = std::min(CHUNK, bytes - off);
+      ok_all = copy_scan(buf_[b], static_cast<const char *>(src) + off, n, finite != nullptr) &&
+               ok_all;
+      e = cudaMemcpyAsync(static_cast<char *>(dst) + off, buf_[b], n, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
+      if (e != cudaSuccess) return e;
+    }
+    if (finite) *finite = ok_all;
+    return cudaSuccess;
+  }
+  // device -> host; returns once dst holds the data
+  cudaError_t download(void *dst, const void *src, size_t bytes, cudaStream_t st)
+  {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (bytes < LARGE || !ready()) {
+      cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+      return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+    }
+    const size_t nch = (bytes + CHUNK - 1) / CHUNK;
+    auto issue = [&](size_t c) -> cudaError_t {
+      const int b = (int)(c % NBUF);
+      const size_t off = c * CHUNK, n = std::min(CHUNK, bytes - off);
+      cudaError_t e = cudaEventSynchronize(ev_[b]);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(buf_[b], static_cast<const char *>(src) + off, n,
+                            cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
+      return e;
+    };
+    for (size_t c = 0; c < nch && c < (size_t)NBUF - 1; c++) {
+      cudaError_t e = issue(c);
+      if (e != cudaSuccess) return e;
+    }
+    for (size_t c = 0; c < nch; c++) {
+      const int b = (int)(c % NBUF);
+      cudaError_t e = cudaEventSynchronize(ev_[b]);
+      if (e != cudaSuccess) return e;
+      const size_t off = c * CHUNK, n = std::min(CHUNK, bytes - off);
+      copy_scan(static_cast<char *>(dst) + off, buf_[b], n, false);
+      if (c + NBUF - 1 < nch) {
+        e = issue(c + NBUF - 1);
+        if (e != cudaSuccess) return e;
+      }
+    }
+    return cudaSuccess;
+  }
+
+ private:
+  Staging() = default;
+  bool ready()
+  {
+    if (tried_) return ok_;
+    tried_ = true;
+    ok_ = true;
+    for (int b = 0; b < NBUF && ok_; b++)
+      ok_ = cudaHostAlloc(&buf_[b], CHUNK, cudaHostAllocPortable) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ev_[b], cudaEventDisableTiming) == cudaSuccess;
+    if (ok_)
+      for (int b = 0; b < NBUF && ok_; b++) ok_ = cudaEventRecord(ev_[b], 0) == cudaSuccess;
+    if (!ok_) cudaGetLastError();
+    return ok_;
+  }
+  // memcpy over up to eight threads; with scan, also the NaN/Inf test of the
+  // copied words
+  static bool copy_scan(void *dst, const void *src, size_t n, bool scan)
+  {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned nt = std::max(1u, std::min(8u, hw));
+    const size_t part = (n / nt + 63) & ~size_t(63);
+    std::vector<char> ok(nt, 1);
+    std::vector<std::thread> th;
+    auto work = [&](unsigned t) {
+      const size_t a = std::min(n, t * part), z = std::min(n, a + part);
+      if (a >= z) return;
+      std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, z - a);
+      if (scan)
+        ok[t] = finite_words(reinterpret_cast<const double *>(static_cast<const char *>(dst) + a),
+                             (z - a) / 8);
+    };
+    for (unsigned t = 1; t < nt; t++) th.emplace_back(work, t);
+    work(0);
+    for (std::thread &x : th) x.join();
+    return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
+  }
+  std::mutex mu_;
+  bool tried_ = false, ok_ = false;
+  void *buf_[NBUF] = {};
+  cudaEvent_t ev_[NBUF] = {};
+};
+
 }  // namespace
 
 // error reporting for the other translation units of the library (qd_err.h)
@@ -325,8 +448,12 @@ int validate(const qd_data *d)
     return set_err(QD_ERR_INVALID, "centrifugal-sudden block J = %d, K = %d: need 0 <= K <= J",
                    d->cs.J, d->cs.K);
   const size_t npt = (size_t)n1 * n2 * nth;
-  if (!all_finite(d->pot, npt)) return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
-  if (!all_finite(d->psi, 2 * npt)) return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
+  // arrays of Staging::LARGE bytes or more are checked while they are staged
+  // for the upload (create), smaller ones here
+  if (npt * sizeof(double) < Staging::LARGE && !all_finite(d->pot, npt))
+    return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
+  if (2 * npt * sizeof(double) < Staging::LARGE && !all_finite(d->psi, 2 * npt))
+    return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
   if (d->CRP.calculate_CRP) {
     const qd_crp &c = d->CRP;
     if (c.n_energies < 1 || !c.energies || !c.eta_sq || !c.CRP)
@@ -995,9 +1122,11 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   const int npot = shared_pot ? 1 : nruns;
   h->vrun = shared_pot ? 0 : npt;
   TRY(h->alloc(h->d_pot, npt * npot));
-  for (int r = 0; r < npot; r++)
-    CU(cudaMemcpyAsync(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt,
-                       cudaMemcpyHostToDevice, h->st));
+  for (int r = 0; r < npot; r++) {
+    bool fin = true;
+    CU(Staging::get().upload(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt, h->st, &fin));
+    if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: pot contains NaN/Inf", r);
+  }
   TRY(upload(h, h->d_w, d->theta.w, h->nth));
   // each set's legendre matrix padded to nl functions (zero rows beyond its own)
   const size_t sstride = (size_t)h->nth * h->nl;
@@ -1091,9 +1220,12 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   }
   h->d_lpsi = lp;
   TRY(h->alloc(h->d_psi_z, npt * nruns));
-  for (int r = 0; r < nruns; r++)
-    CU(cudaMemcpyAsync(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt,
-                       cudaMemcpyHostToDevice, h->st));
+  for (int r = 0; r < nruns; r++) {
+    bool fin = true;
+    CU(Staging::get().upload(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt, h->st,
+                             &fin));
+    if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
+  }
   if (h->do_crp) {
     const size_t nq = (size_t)h->nth * h->n1;
     unsigned char *b = nullptr;
@@ -1146,9 +1278,8 @@ int get_psi(qd_handle *h, int run, double *psi_out)
   if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
   const long npt = h->n12 * h->nth;
   TRY(stage_psi(h));
-  CU(cudaMemcpyAsync(psi_out, h->d_psi_z + (long)run * npt, sizeof(double2) * npt,
-                     cudaMemcpyDeviceToHost, h->st));
-  CU(cudaStreamSynchronize(h->st));
+  CU(Staging::get().download(psi_out, h->d_psi_z + (long)run * npt, sizeof(double2) * npt,
+                             h->st));
   return QD_OK;
 }
 

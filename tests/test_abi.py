@@ -83,6 +83,25 @@ def test_nonfinite_found_in_large_inputs(qdlib, where):
     assert not h.value
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("where", ["pot", "psi"])
+def test_nonfinite_found_while_staging_large_inputs(qdlib, where):
+    # arrays of 64 MiB or more are checked while they are copied into the
+    # page-locked staging buffers of the upload
+    d = S.build_case("h+h2", 256, 256, 128, m=63, total_steps=1, n_energies=5,
+                     n_gradient_points=5)
+    assert d.pot.nbytes >= 64 << 20
+    if where == "pot":
+        d.pot[-1, -1, -3] = np.inf
+    else:
+        d.psi[-1, -2, -1] = complex(np.nan, 0.0)
+    c = _abi.to_c(d)
+    h = C.c_void_p()
+    assert qdlib.qd_create(C.byref(c), C.byref(h)) == _abi.QD_ERR_NONFINITE
+    assert where.encode() in qdlib.qd_last_error()
+    assert not h.value
+
+
 def test_unsupported_fft_size(qdlib):
     d = S.build_case("h+h2", 14, 12, 8, m=6, total_steps=1, n_energies=5, n_gradient_points=5)
     c = _abi.to_c(d)
