@@ -392,13 +392,18 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   // every thread observes each mbarrier completion itself before it reads
   // what the asynchronous operation wrote
   bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
+  // MID: the tile's A1 is already in TMEM and its GEMM1 issued -- done at the
+  // end of the previous tile, as soon as that tile's GEMM2 output was in
+  // registers, so that GEMM1 runs under the previous tile's norm exchange and
+  // stores
+  bool a_ready = false;
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
     int nlr = nl;                               // orders stored for this run
     if constexpr (MS) {
       const int set = t.run_set ? t.run_set[run] : 0;
-      if (set != loaded) {                      // a run with another angular basis
+      if (!a_ready && set != loaded) {          // a run with another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
         if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
@@ -422,24 +427,27 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
 
     if (mode != COL_HEAD) {
       // ---- A1 = psi'_l tile into TMEM, its norm, GEMM1 --------------------------------
-      float nl_part = 0.f;
+      if (!a_ready) {
+        float nl_part = 0.f;
 #pragma unroll
-      for (int u = 0; u < H; u += 4) {
-        put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
-        nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
-                  fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
+        for (int u = 0; u < H; u += 4) {
+          put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
+          nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
+                    fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
+        if (!is_im) xch[grp * TPTS + pt] = nl_part;
+        if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
+        __syncthreads();
+        if (tid == 0) {
+          tc_fence_after();
+          gemm_split_ts<S, false>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
+          mma_commit(mb1);
+        }
       }
-      tmem_wait_st();
-      tc_fence_before();
-      nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
-      if (!is_im) xch[grp * TPTS + pt] = nl_part;
-      if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        gemm_split_ts<S, false>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
-        mma_commit(mb1);
-      }
+      a_ready = false;
 #pragma unroll
       for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
@@ -581,7 +589,40 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     }
     no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
     if (!is_im) xch[3 * NG * TPTS + grp * TPTS + pt] = no_part;
+    // the next tile's A1 into TMEM and its GEMM1, while this tile finishes:
+    // GEMM2 has completed (its A2 is free) and this thread's D is in ov
+    const int nxt = tile + (int)gridDim.x;
+    const bool ahead = mode == COL_MID && nxt < tend;
+    if (ahead) {
+      if constexpr (MS) {
+        const int set = t.run_set ? t.run_set[QD_RUN_OF(nxt)] : 0;
+        if (set != loaded) {                    // no MMA reads the image now
+          if (tid == 0) QD_LOAD_IMAGES(set);
+          if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+          ph3 ^= 1;
+          loaded = set;
+        }
+      }
+      float nl_part = 0.f;
+#pragma unroll
+      for (int u = 0; u < H; u += 4) {
+        put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
+        nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
+                  fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
+      }
+      tmem_wait_st();
+      nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
+      if (!is_im) xch[grp * TPTS + pt] = nl_part;
+      asm volatile("cp.async.wait_group 0;" ::: "memory");   // the next tile's evs
+    }
+    tc_fence_before();
     __syncthreads();
+    if (ahead && tid == 0) {
+      tc_fence_after();
+      gemm_split_ts<S, false>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
+      mma_commit(mb1);
+    }
+    a_ready = ahead;
     float n_o = 0.f;
 #pragma unroll
     for (int g = 0; g < NG; g++) n_o += xch[3 * NG * TPTS + g * TPTS + pt];
