@@ -323,6 +323,8 @@ struct qd_handle {
   int *d_lstatus = nullptr;       // status word of the l-space kernels (0 = ok)
   int slice_cluster = 0;          // l-space kernel (LineParams::cluster code)
   int flux_variant = 0;           // flux-accumulation GEMM tile variant (tune_flux)
+  bool psi_z_valid = false;       // d_psi_z holds the theta-space state of every run
+  bool crp_valid = false;         // d_crp holds P(E) of the accumulated flux
   double2 *d_tw1_64 = nullptr, *d_tw2_64 = nullptr;
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
   void *d_lpsi = nullptr;
@@ -851,7 +853,7 @@ int flush_accum(qd_handle *h)
 
 int compute_crp(qd_handle *h)
 {
-  if (!h->do_crp) return QD_OK;
+  if (!h->do_crp || h->crp_valid) return QD_OK;
   TRY(flush_accum(h));
   CrpParams c{};
   c.n1 = h->n1; c.nth = h->nth; c.ne = h->ne; c.w = h->d_w; c.eta_sq = h->d_eta;
@@ -862,6 +864,7 @@ int compute_crp(qd_handle *h)
   CU(launch_crp(c, h->st));
   g_launches++;
   TRY(prof_mark(h, PROF_CRP));
+  h->crp_valid = true;
   return QD_OK;
 }
 
@@ -873,6 +876,8 @@ template <typename Real> int propagate(qd_handle *h, int n, size_t flush_bytes =
     return QD_OK;
   }
   const bool timed = device_ms != nullptr;
+  h->psi_z_valid = false;
+  h->crp_valid = false;
   if (timed) {
     while (h->events.size() < (size_t)(2 * n + 2)) {
       cudaEvent_t e;
@@ -1265,11 +1270,13 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
 }
 
 // theta-space psi of every run into d_psi_z (B psi_l and the absorber)
+// (once per propagated state: qd_download reads every run from one staging)
 int stage_psi(qd_handle *h)
 {
-  if (!h->started) return QD_OK;              // d_psi_z still holds the input
+  if (!h->started || h->psi_z_valid) return QD_OK;   // d_psi_z holds the input / the state
   if (h->prec == QD_PREC_FP64) TRY(issue_column<double>(h, COL_TAIL, false, nullptr, true));
   else TRY(issue_column<float>(h, COL_TAIL, false, nullptr, true));
+  h->psi_z_valid = true;
   return QD_OK;
 }
 
@@ -1448,6 +1455,8 @@ int restore(qd_handle *h, const char *path)
   fclose(f);
   if (!ok) return set_err(QD_ERR_IO, "\"%s\" is truncated", path);
   h->steps = hd.steps; h->started = hd.started; h->last_finalized = hd.last_finalized;
+  h->psi_z_valid = false;
+  h->crp_valid = false;
   h->ring_fill = hd.ring_fill; h->flux_pending = hd.flux_pending; h->acc_done = hd.acc_done;
   h->norms_host = norms;
   h->failed = false;
