@@ -398,6 +398,7 @@ template <int CL> cudaError_t launch_cl(const LineParams &p, cudaStream_t s)
 
 int slice_cluster_ok(int n1, int n2, int cl)
 {
+  if (cl == SLICE_RF4W) return slice_rf_wide_ok(n1, n2) ? 1 : 0;
   if (slice_is_rf(cl)) return slice_rf_threads(n1, n2, slice_ctas(cl)) > 0;
   if (cl != 1 && cl != 2 && cl != 4) return 0;
   if (n1 % cl || n2 % cl) return 0;
@@ -415,6 +416,7 @@ cudaError_t launch_slice(const LineParams &p, cudaStream_t s)
     case SLICE_RF: return launch_slice_rf(p, 1, s);
     case SLICE_RF2: return launch_slice_rf(p, 2, s);
     case SLICE_RF4: return launch_slice_rf(p, 4, s);
+    case SLICE_RF4W: return launch_slice_rf_wide(p, s);
     case 1: return launch_cl<1>(p, s);
     case 2: return launch_cl<2>(p, s);
     case 4: return launch_cl<4>(p, s);

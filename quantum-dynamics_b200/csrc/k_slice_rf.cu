@@ -194,8 +194,10 @@ template <int SGN> struct Dft<32, SGN> {
   static __device__ __forceinline__ void run(float2 *v) { DftPxQ<32, 4, 8, SGN>::run(v); }
 };
 
-template <int N1, int N2, int NT, int CL> struct RfShape {
-  static constexpr int A1 = N1 == 64 ? 8 : N1 == 256 ? 32 : 16;   // row pass 2 radix (B1 = 8)
+// A1X: row pass 2 radix (0: the default of the size, B1 = 8; 16 for N1 = 256
+// gives B1 = 16, i.e. twice the row-pass-2 items at half their registers)
+template <int N1, int N2, int NT, int CL, int A1X = 0> struct RfShape {
+  static constexpr int A1 = A1X ? A1X : N1 == 64 ? 8 : N1 == 256 ? 32 : 16;   // row pass 2 radix
   static constexpr int B1 = N1 / A1;
   static constexpr int A2 = N2 / 8;                   // column pass 2 radix (B2 = 8)
   static constexpr int B2 = 8;
@@ -218,7 +220,9 @@ template <int N1, int N2, int NT, int CL> struct RfShape {
   static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (size_t)PSLOTS * HR * HW +
                                                    TABLES) + (PSLOTS > 0 ? 16 : 0);
   static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row part, one bulk copy
-  static_assert(B1 == 8 && RS % 16 == 8, "row layout");
+  // 8 B1 blocks of A1 + 1 slots with RS = 8 mod 16, or 16 blocks with RS = 0
+  // mod 16: either way a warp's access of any pass touches each bank pair twice
+  static_assert((B1 == 8 && RS % 16 == 8) || (B1 == 16 && RS % 16 == 0), "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
   static_assert(CL == 1 || ((CL == 2 || CL == 4) && B1 % CL == 0 && HR == BPO * A2 &&
                             HW == (B1 / CL) * (A1 + 1) && HALF_BYTES % 16 == 0),
@@ -327,10 +331,10 @@ __device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
 // swap of swap_parts, after which row part o of the row array holds CTA o's
 // rows in this CTA's column part.  Every load and store of the passes is
 // local.  CL = 1 keeps the slice in one array in place.
-template <int N1, int N2, int NT, int CL>
+template <int N1, int N2, int NT, int CL, int A1X>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
-  using Sh = RfShape<N1, N2, NT, CL>;
+  using Sh = RfShape<N1, N2, NT, CL, A1X>;
   constexpr int A1 = Sh::A1, B1 = Sh::B1, A2 = Sh::A2, B2 = Sh::B2, RS = Sh::RS;
   constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
@@ -577,11 +581,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   if constexpr (Sh::PSLOTS > 0) cluster_wait();
 }
 
-template <int N1, int N2, int NT, int CL>
+template <int N1, int N2, int NT, int CL, int A1X = 0>
 cudaError_t launch_rf(const LineParams &p, cudaStream_t s)
 {
-  constexpr size_t sm = RfShape<N1, N2, NT, CL>::SMEM;
-  cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT, CL>,
+  constexpr size_t sm = RfShape<N1, N2, NT, CL, A1X>::SMEM;
+  cudaError_t e = cudaFuncSetAttribute(k_slice_rf<N1, N2, NT, CL, A1X>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
@@ -605,7 +609,7 @@ cudaError_t launch_rf(const LineParams &p, cudaStream_t s)
   }
   cfg.attrs = attr;
   cfg.numAttrs = na;
-  cudaLaunchKernelEx(&cfg, k_slice_rf<N1, N2, NT, CL>, p);
+  cudaLaunchKernelEx(&cfg, k_slice_rf<N1, N2, NT, CL, A1X>, p);
   return cudaGetLastError();
 }
 
@@ -638,6 +642,14 @@ cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s)
   } else if (cl == 4) {
     if (p.n1 == 256 && p.n2 == 192) return launch_rf<256, 192, 256, 4>(p, s);
   }
+  return cudaErrorInvalidValue;
+}
+
+// the 4-CTA kernel with 16 x 16 row transforms (built for 256 x 192)
+bool slice_rf_wide_ok(int n1, int n2) { return n1 == 256 && n2 == 192; }
+cudaError_t launch_slice_rf_wide(const LineParams &p, cudaStream_t s)
+{
+  if (p.n1 == 256 && p.n2 == 192) return launch_rf<256, 192, 256, 4, 16>(p, s);
   return cudaErrorInvalidValue;
 }
 

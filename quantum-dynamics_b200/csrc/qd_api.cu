@@ -652,7 +652,7 @@ LineParams line_params(qd_handle *h, bool f32)
 // 1, 2 and 4 CTAs per slice, the register-FFT slice kernel on 1, 2 or 4
 // CTAs per slice (where built) and the split kernels on a scratch wavepacket and keep the
 // fastest; the choice is kept for later handles of the same shapes.
-// QD_SLICE_CLUSTER=0|1|2|4|8|9|10 forces a choice (8 = the register-FFT
+// QD_SLICE_CLUSTER=0|1|2|4|8|9|10|11 forces a choice (8 = the register-FFT
 // kernel, 9 and 10 = the same on a 2- and a 4-CTA cluster).
 int tune_slice(qd_handle *h)
 {
@@ -689,7 +689,7 @@ int tune_slice(qd_handle *h)
   LineParams p = line_params(h, true);
   p.lpsi = scratch;
   float best = 1e30f;
-  for (int cl : {0, 1, 2, 4, SLICE_RF, SLICE_RF2, SLICE_RF4}) {
+  for (int cl : {0, 1, 2, 4, SLICE_RF, SLICE_RF2, SLICE_RF4, SLICE_RF4W}) {
     if (cl > 0 && !slice_cluster_ok(h->n1, h->n2, cl)) continue;
     p.cluster = cl;
     bool ok = true;

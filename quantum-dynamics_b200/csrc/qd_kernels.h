@@ -227,16 +227,23 @@ constexpr int FLUX_CHUNK = 250;
 constexpr int SLICE_RF = 8;    // LineParams::cluster value of the register-FFT slice kernel
 constexpr int SLICE_RF2 = 9;   // the same on a 2-CTA cluster per slice
 constexpr int SLICE_RF4 = 10;  // the same on a 4-CTA cluster per slice
+constexpr int SLICE_RF4W = 11; // the 4-CTA form with 16 x 16 row transforms
 inline bool slice_is_rf(int cluster)
-{ return cluster == SLICE_RF || cluster == SLICE_RF2 || cluster == SLICE_RF4; }
+{
+  return cluster == SLICE_RF || cluster == SLICE_RF2 || cluster == SLICE_RF4 ||
+         cluster == SLICE_RF4W;
+}
 inline int slice_ctas(int cluster)           // CTAs per slice
 {
-  return cluster == SLICE_RF ? 1 : cluster == SLICE_RF2 ? 2 : cluster == SLICE_RF4 ? 4 : cluster;
+  return cluster == SLICE_RF ? 1 : cluster == SLICE_RF2 ? 2
+       : cluster == SLICE_RF4 || cluster == SLICE_RF4W ? 4 : cluster;
 }
 int slice_cluster_ok(int n1, int n2, int cluster);
 int slice_rf_threads(int n1, int n2, int cl); // threads per CTA, 0 if the shape is not built
 int slice_threads(int n1, int n2, int cluster);
 cudaError_t launch_slice_rf(const LineParams &p, int cl, cudaStream_t s);
+bool slice_rf_wide_ok(int n1, int n2);
+cudaError_t launch_slice_rf_wide(const LineParams &p, cudaStream_t s);
 cudaError_t launch_slice(const LineParams &p, cudaStream_t s);
 cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const double *w,
                                      const double *legendre, double *P, double *WP,
