@@ -3,11 +3,10 @@
 //
 // Same work as k_column.cu (B, dump, flux rows, norm, V, F; see there for the
 // reference functions), with both Legendre contractions as back-to-back
-// GEMMs per tile of 64 grid columns (S = n_l, n_theta padded to 16), in the
-// orthonormal basis described below (Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k)):
-//   GEMM1  D[128 x S] = A1[128 x S] * B1[S x S]    A1 = psi'_l tile, B1[l][k] = Q[k][l]
+// GEMMs per tile of 64 grid columns (S = n_l, n_theta padded to 16):
+//   GEMM1  D[128 x S] = A1[128 x S] * B1[S x S]    A1 = psi_l tile, B1[l][k] = P_l(x_k)
 //   theta-space ops on D (tcgen05.ld -> registers) -> A2 (TMEM)
-//   GEMM2  D[128 x S] = A2[128 x S] * B2[S x S]    B2[k][l] = Q[k][l]
+//   GEMM2  D[128 x S] = A2[128 x S] * B2[S x S]    B2[k][l] = (l+1/2) w_k P_l(x_k)
 // The 128 GEMM rows are the real and imaginary parts of the 64 complex
 // points (row 2p = Re, 2p+1 = Im), so the complex-by-real transform is one
 // real GEMM.  FP32 accuracy from TF32 units by split products (3xTF32)
@@ -16,17 +15,17 @@
 //
 // Data placement: the A operands live in tensor memory (written by the
 // threads with tcgen05.st; each thread owns one TMEM lane = one GEMM row and
-// a quarter of its columns), the constant B operand in shared memory, the
-// accumulator in TMEM.  Both GEMMs read ONE image of the matrix Q[k][l]
-// (hi | lo, 128-byte swizzle, built once on the host; rows k, l along the
-// swizzled row): GEMM1 as B1[l][k] = Q[k][l] with K = l contiguous (K-major),
-// GEMM2 as B2[k][l] = Q[k][l] with N = l contiguous (MN-major, the transpose
-// bit of the instruction descriptor).  The tile's exp(-i V dt) values are
-// staged into shared memory by asynchronous copies issued while the previous
-// tile finishes.  512 threads per CTA.  TMEM per CTA: [Ahi | Alo | D], S
-// columns each.  S <= 64: two CTAs per SM overlap each other's load / MMA /
-// epilogue phases.  S = 96, 128 (n_theta up to 128): one CTA per SM (512
-// TMEM columns), the image (128 KB at S = 128) resident for the launch.
+// a quarter of its columns), the constant B images in shared memory (K-major,
+// 128-byte swizzle, built once on the host), the accumulator in TMEM.  The
+// tile's exp(-i V dt) values are staged into shared memory by asynchronous
+// copies issued while the previous tile finishes.  512 threads per CTA.  TMEM
+// per CTA: [Ahi | Alo | D], S columns each.  S <= 64: two CTAs per SM overlap
+// each other's load / MMA / epilogue phases.  S = 96, 128 (n_theta up to 128):
+// one CTA per SM (512 TMEM columns); at S = 128 the four operand images
+// (256 KB) do not fit in shared memory together, so the CTA keeps one GEMM's
+// pair: B2 is copied over B1 as soon as GEMM1 has completed, and the next
+// tile's B1 over B2 as soon as GEMM2 has, each copy overlapping the work
+// between the two GEMMs or after them.
 //
 // Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
 // smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
@@ -58,9 +57,11 @@ constexpr int MROWS = 128;        // GEMM rows per tile
 constexpr int NTHREADS = 512;
 constexpr int MAXS = 128;         // max padded n_l / n_theta handled here
 // per-size resources: TMEM columns (Ahi | Alo | D, S each, rounded up to a
-// power of two) and CTAs per SM
+// power of two), CTAs per SM, and whether both GEMMs' operand images stay in
+// shared memory (else the CTA streams B1 and B2 in turn through one buffer)
 __host__ __device__ constexpr uint32_t tmem_cols(int S) { return 3 * S <= 256 ? 256u : 512u; }
 __host__ __device__ constexpr int ctas_per_sm(int S) { return 3 * S <= 256 ? 2 : 1; }
+__host__ __device__ constexpr bool stream_images(int S) { return S > 96; }
 constexpr long WAIT_LIMIT = 1L << 22;   // mbarrier polls before giving up
 
 
@@ -100,27 +101,22 @@ __device__ __forceinline__ float tf32_rna(float x)
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
-// shared-memory matrix descriptor of an SW128 operand.  K-major (rows along N,
-// K along the 128-byte row): SBO = 1024 B between 8-row groups, LBO unused.
-// MN-major (rows along K, N along the row): LBO = the byte distance between
-// the 32-element N atoms, SBO = 1024 B between 8-row K groups.
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes = 16)
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr)
 {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3fffu);          // start address
-  d |= (uint64_t)((lbo_bytes >> 4) & 0x3fffu) << 16; // LBO
+  d |= (uint64_t)1u << 16;                          // LBO (unused for SW128 K-major)
   d |= (uint64_t)(1024u >> 4) << 32;                // SBO: 8 rows x 128 B
   d |= (uint64_t)1u << 46;                          // descriptor version (sm100)
   d |= (uint64_t)2u << 61;                          // SWIZZLE_128B
   return d;
 }
 
-// kind::tf32 instruction descriptor: D f32, A/B tf32, A K-major, B K-major
-// (or MN-major with the transpose bit 16), M=128, N
-__host__ __device__ constexpr uint32_t make_idesc(int N, bool b_mn = false)
+// kind::tf32 instruction descriptor: D f32, A/B tf32, both K-major, M=128, N
+__host__ __device__ constexpr uint32_t make_idesc(int N)
 {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (b_mn ? (1u << 16) : 0u) |
-         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(MROWS >> 4) << 24);
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(MROWS >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar)
@@ -153,7 +149,7 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 struct TcDev {
-  const float4 *mats;    // image sets (Q hi|lo), set_bytes apart
+  const float4 *mats;    // image sets (B1 hi|lo, B2 hi|lo), set_bytes apart
   uint32_t set_bytes;
   const int *run_set;    // image set of each run (null: set 0)
   const int *run_order;  // tile order: virtual run v is run_order[v], runs of a set adjacent
@@ -217,16 +213,13 @@ __device__ __forceinline__ void mma_tf32_ts(uint32_t dtmem, uint32_t atmem, uint
       : "r"(dtmem), "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// D = A * B over K = S, A in TMEM columns [ahi, ahi+S) and [alo, alo+S), B the
-// image at b (hi | lo, b_bytes apart; element (r, c) at sw128_off(r, c, S)):
-// MN = false reads it as B[c][r] (K = c, K-major), MN = true as B[r][c]
-// (K = r, N = c along the row, MN-major).  The small split terms first,
-// the main one last.
-template <int S, bool MN>
+// D = A * B over K = S, A in TMEM columns [ahi, ahi+S) and [alo, alo+S), B at
+// b (hi | lo, b_bytes apart): the small split terms first, main last
+template <int S>
 __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint32_t alo,
                                               uint32_t b, int b_bytes)
 {
-  constexpr uint32_t idesc = make_idesc(S, MN);
+  constexpr uint32_t idesc = make_idesc(S);
 #pragma unroll 1
   for (int term = 0; term < 3; term++) {
     // term 0: Ahi*Blo, 1: Alo*Bhi, 2: Ahi*Bhi
@@ -234,13 +227,8 @@ __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint
     const uint32_t bt = b + (term == 0 ? b_bytes : 0);
 #pragma unroll
     for (int kk = 0; kk < S; kk += 8) {
-      if constexpr (MN) {             // K rows kk..kk+7: one 1024-byte swizzle atom row group
-        mma_tf32_ts(dtmem, a + kk, make_desc(bt + (uint32_t)kk * 128u, (uint32_t)S * 128u),
-                    idesc, (term | kk) ? 1u : 0u);
-      } else {                        // K columns kk..kk+7 within the 128-byte rows
-        const uint32_t boff = (uint32_t)((kk >> 5) * S * 128 + ((kk & 31) >> 3) * 32);
-        mma_tf32_ts(dtmem, a + kk, make_desc(bt + boff), idesc, (term | kk) ? 1u : 0u);
-      }
+      const uint32_t boff = (uint32_t)((kk >> 5) * S * 128 + ((kk & 31) >> 3) * 32);
+      mma_tf32_ts(dtmem, a + kk, make_desc(bt + boff), idesc, (term | kk) ? 1u : 0u);
     }
   }
 }
@@ -268,13 +256,15 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   constexpr int H = S / NG;                    // K columns per thread (one group)
   constexpr int NKA = (S + 31) / 32;           // 128-byte swizzle atoms along K
   constexpr int B_BYTES = NKA * S * 128;
+  constexpr bool STREAM = stream_images(S);    // B1 and B2 take turns in one buffer
   constexpr uint32_t TMEM_COLS = tmem_cols(S);
   static_assert(H % 4 == 0, "column group must be a multiple of 4");
   extern __shared__ unsigned char smem_raw[];
   const uint32_t base_u = smem_u32(smem_raw);
   unsigned char *base = smem_raw + ((1024u - (base_u & 1023u)) & 1023u);
-  unsigned char *Bq = base;                     // Q image, hi | lo
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(base + 2 * B_BYTES);
+  unsigned char *B1 = base;                     // hi | lo
+  unsigned char *B2 = STREAM ? base : B1 + 2 * B_BYTES;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(base + (STREAM ? 2 : 4) * B_BYTES);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *sw = xch + 4 * NG * TPTS;                        // [S] sqrt(w_k), 0 beyond n_theta
@@ -305,25 +295,35 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   const int tbeg = blockIdx.x, tend = ntiles;
 #define QD_DIV(x, m) ((int)(((uint64_t)(uint32_t)(x) * (m)) >> 40))
 #define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[QD_DIV(tl, t.m_tpr)] : QD_DIV(tl, t.m_tpr))
-  const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the image copy
-  // the image (hi | lo, 2 B_BYTES, a multiple of 16) of set `st` by bulk
-  // asynchronous copies from this GPU's global memory into this CTA's shared
-  // memory, completing on mbar[3]
-#define QD_LOAD_IMAGES(st)                                                             \
+  const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
+  // images [first, first + count) of set `st` (B1 hi, B1 lo, B2 hi, B2 lo,
+  // B_BYTES each, multiples of 16) by bulk asynchronous copies from this
+  // GPU's global memory into this CTA's shared memory at B1, completing on
+  // mbar[3]
+#define QD_LOAD_B(st, first, count)                                                    \
   do {                                                                                 \
-    const uint32_t total = 2 * B_BYTES, chunk = 16384;                                 \
+    const uint32_t total = (count) * B_BYTES, chunk = 16384;                           \
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"              \
                  :: "r"(mb3), "r"(total) : "memory");                                  \
-    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes; \
+    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes + \
+                      (size_t)(first) * B_BYTES;                                       \
     for (uint32_t off = 0; off < total; off += chunk) {                                \
       const uint32_t n = total - off < chunk ? total - off : chunk;                    \
       asm volatile(                                                                    \
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" \
-          :: "r"(smem_u32(Bq) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
+          :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
     }                                                                                  \
+  } while (0)
+  // the images one launch of this mode needs resident: all four, or with
+  // STREAM the pair of the mode's single GEMM (B2 for HEAD) or B1 to start MID
+#define QD_LOAD_IMAGES(st)                                                             \
+  do {                                                                                 \
+    if (!STREAM) QD_LOAD_B(st, 0, 4);                                                  \
+    else QD_LOAD_B(st, mode == COL_HEAD ? 2 : 0, 2);                                   \
   } while (0)
 #define QD_SET_OF(tl) (MS && t.run_set ? t.run_set[QD_RUN_OF(tl)] : 0)
   int loaded = tbeg < tend ? QD_SET_OF(tbeg) : 0;   // image set in smem
+  bool img_pending = false;                     // a streamed image copy not yet waited on
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
@@ -392,18 +392,23 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   // every thread observes each mbarrier completion itself before it reads
   // what the asynchronous operation wrote
   bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
-  // MID: the tile's A1 is already in TMEM and its GEMM1 issued -- done at the
-  // end of the previous tile, as soon as that tile's GEMM2 output was in
-  // registers, so that GEMM1 runs under the previous tile's norm exchange and
-  // stores
+  // MID without image streaming: the tile's A1 is already in TMEM and its
+  // GEMM1 issued -- done at the end of the previous tile, as soon as that
+  // tile's GEMM2 output was in registers, so that GEMM1 runs under the
+  // previous tile's norm exchange and stores
   bool a_ready = false;
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
     int nlr = nl;                               // orders stored for this run
+    if (STREAM && mode == COL_MID && img_pending) {   // B1 of this tile, issued last tile
+      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+      ph3 ^= 1;
+      img_pending = false;
+    }
     if constexpr (MS) {
       const int set = t.run_set ? t.run_set[run] : 0;
-      if (!a_ready && set != loaded) {          // a run with another angular basis
+      if (!a_ready && !(STREAM && mode == COL_MID) && set != loaded) {   // another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
         if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         __syncthreads();
         if (tid == 0) {
           tc_fence_after();
-          gemm_split_ts<S, false>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
+          gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
           mma_commit(mb1);
         }
       }
@@ -453,6 +458,10 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
+      if (STREAM && mode == COL_MID) {          // B1 is free: B2 of this tile's set in its place
+        if (tid == 0) QD_LOAD_B(QD_SET_OF(tile), 2, 2);
+        img_pending = true;
+      }
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
         float nt_part = 0.f, dv[H];
         tmem_ld_all<H>(my_d, dv);
@@ -571,15 +580,24 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
+    if (STREAM && mode == COL_MID) {            // B2 in place
+      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
+      ph3 ^= 1;
+      img_pending = false;
+    }
     if (tid == 0) {
       tc_fence_after();
-      gemm_split_ts<S, true>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
+      gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
       mma_commit(mb2);
     }
     if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
+    if (STREAM && mode == COL_MID && tile + (int)gridDim.x < tend) {   // B1 of the next tile
+      if (tid == 0) QD_LOAD_B(QD_SET_OF(tile + (int)gridDim.x), 0, 2);
+      img_pending = true;
+    }
     float no_part = 0.f, ov[H];
     tmem_ld_all<H>(my_d, ov);
 #pragma unroll
@@ -589,14 +607,15 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     }
     no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
     if (!is_im) xch[3 * NG * TPTS + grp * TPTS + pt] = no_part;
-    // the next tile's A1 into TMEM and its GEMM1, while this tile finishes:
-    // GEMM2 has completed (its A2 is free) and this thread's D is in ov
+    // without streaming: the next tile's A1 into TMEM and its GEMM1, while
+    // this tile finishes (GEMM2 has completed, so its A2 is free, and this
+    // thread's D is in ov)
     const int nxt = tile + (int)gridDim.x;
-    const bool ahead = mode == COL_MID && nxt < tend;
+    const bool ahead = !STREAM && mode == COL_MID && nxt < tend;
     if (ahead) {
       if constexpr (MS) {
         const int set = t.run_set ? t.run_set[QD_RUN_OF(nxt)] : 0;
-        if (set != loaded) {                    // no MMA reads the image now
+        if (set != loaded) {                    // no MMA reads the images now
           if (tid == 0) QD_LOAD_IMAGES(set);
           if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
           ph3 ^= 1;
@@ -619,7 +638,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     __syncthreads();
     if (ahead && tid == 0) {
       tc_fence_after();
-      gemm_split_ts<S, false>(D, Ahi, Alo, smem_u32(Bq), B_BYTES);
+      gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
       mma_commit(mb1);
     }
     a_ready = ahead;
@@ -643,12 +662,14 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
 #undef QD_PREFETCH_A
 #undef QD_STAGE_EV
 #undef QD_LOAD_IMAGES
+#undef QD_LOAD_B
 #undef QD_SET_OF
 #undef QD_RUN_OF
 #undef QD_DIV
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
+  if (STREAM && img_pending) mbar_wait(mb3, ph3);        // (bounded; after a failed wait)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -716,13 +737,12 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 
 template <int S> constexpr int smem_bytes_for()
 {
-  return 1024 + 2 * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 +
+  return 1024 + (stream_images(S) ? 2 : 4) * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 +
          4 * NG * TPTS * 4 + 2 * S * 4 +
-         S * TPTS * 8;   // Q image, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
+         S * TPTS * 8;   // B images, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
 static_assert(smem_bytes_for<128>() <= 227 * 1024 && smem_bytes_for<96>() <= 227 * 1024,
               "shared memory of the largest column tiles");
-static_assert(2 * smem_bytes_for<64>() <= 227 * 1024, "two CTAs per SM at S <= 64");
 
 // the kernel sizes built: S is n_l / n_theta padded up to one of them
 int kernel_size(int n)
@@ -782,7 +802,7 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
   }
   const int nka = (S + 31) / 32;
   const int bb = nka * S * 128;
-  const size_t set_bytes = 2 * (size_t)bb;
+  const size_t set_bytes = 4 * (size_t)bb;
   std::vector<unsigned char> img(set_bytes * nsets, 0);
   auto put = [&](unsigned char *img2, int r, int k, double val) {     // hi | lo
     const float h = tf32_round_host((float)val);
@@ -791,17 +811,15 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
     std::memcpy(img2 + off, &h, 4);
     std::memcpy(img2 + bb + off, &l, 4);
   };
-  // one image per set, element (k, l) = Q[k][l] at sw128_off(k, l, S): GEMM1
-  // reads it with K = l, GEMM2 (transposed) with K = k.  With the completion
-  // the columns l >= m hold the extra orders GEMM2 forms for the norm; GEMM1
-  // multiplies them by A columns that are zero (orders a run does not store).
   for (int t = 0; t < nsets; t++) {
-    unsigned char *b = img.data() + t * set_bytes;
+    unsigned char *b1 = img.data() + t * set_bytes, *b2 = b1 + 2 * bb;
     const int m = nl_set[t];
-    const int cols = renorm ? nth : m;                   // orders formed by GEMM2
+    const int rows2 = renorm ? nth : m;                  // output orders formed by GEMM2
     const std::vector<double> &q2 = renorm ? Qx[t] : Q[t];
-    for (int k = 0; k < nth; k++)
-      for (int l = 0; l < cols; l++) put(b, k, l, q2[(size_t)l * nth + k]);
+    for (int k = 0; k < nth; k++) {
+      for (int l = 0; l < m; l++) put(b1, k, l, Q[t][(size_t)l * nth + k]);   // B1: row k, K = l
+      for (int l = 0; l < rows2; l++) put(b2, l, k, q2[(size_t)l * nth + k]); // B2: row l, K = k
+    }
   }
   // from the device's stream-ordered pool, like the handle's other buffers;
   // a copy from pageable memory has read `img` when it returns

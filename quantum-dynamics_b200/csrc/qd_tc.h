@@ -7,8 +7,8 @@ struct TcPlan {
   int nth = 0, nl = 0;          // n_theta; n_l of the state layout (max over the sets)
   int S = 0;                    // max(n_l, n_theta) padded to 16 (MMA N and K)
   int renorm = 0;               // per-column isometry rescaling (orthonormal Q columns)
-  int nsets = 0;                // angular bases (one operand image each)
-  size_t set_bytes = 0;         // bytes of one image: Q hi|lo (both GEMMs read it)
+  int nsets = 0;                // angular bases (one operand image set each)
+  size_t set_bytes = 0;         // bytes of one image set: B1 hi|lo, B2 hi|lo
   void *mats = nullptr;         // device: the image sets, then an int status word
   size_t mats_bytes = 0;
   int smem_bytes = 0;

@@ -48,9 +48,10 @@ def TimeEvolutionMexCUDA(data):
     struct or a list of structs propagated together as a batch."""
     runs = data if isinstance(data, (list, tuple)) else [data]
     arr = _c_runs(runs)
-    check(lib().qd_time_evolution_batch(arr, len(runs)))
-    for d, c in zip(runs, arr):
+    rc = lib().qd_time_evolution_batch(arr, len(runs))
+    for d, c in zip(runs, arr):      # time.steps also when a progress callback stopped the call
         _abi.from_c(c, d)
+    check(rc)
     return data
 
 
