@@ -392,6 +392,23 @@ def run_ours(args):
                 "what": "the plain form (complex128 wavepacket, FP64 everywhere) on the same "
                         "workload and GPU, timed the same way"}
 
+    # --- the same passes in their library forms (context for the FP64 ratio) -------------
+    libform = None
+    if not args.fp64 and not args.no_lib_compare and world == 1:
+        lib = library_form(data, max(K, 5))
+        ours_ms = dev["kclass_ms"].get("column", 0.0) + dev["kclass_ms"].get("lines", 0.0)
+        lib64 = lib["column_cublas_fp64_ms"] + lib["lspace_cufft_z2z_ms"]
+        lib32 = lib["column_cublas_fp32_bf16x9_ms"] + lib["lspace_cufft_c2c_ms"]
+        libform = {**lib, "ours_column_plus_lspace_ms": ours_ms,
+                   "library_fp64_column_plus_lspace_ms": lib64,
+                   "library_fp32_column_plus_lspace_ms": lib32,
+                   "ratio_vs_library_fp64": lib64 / ours_ms if ours_ms else None,
+                   "ratio_vs_library_fp32": lib32 / ours_ms if ours_ms else None,
+                   "what": "the column and l-space passes of one step: ours (complex64, per-kernel "
+                           "CUDA events) against cuBLAS Legendre GEMMs + cuFFT 2-D plans + "
+                           "elementwise phase kernels on the same shapes, FP64 (Z2Z, DGEMM) and "
+                           "FP32 (C2C, BF16x9-emulated FP32 GEMM)"}
+
     # --- end to end through the drop-in entry point -------------------------------
     # each a full call: upload, set-up, K steps, P(E), download; median reported
     nrep = 5 if pts * 16 < (1 << 30) else 3
@@ -467,11 +484,28 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "value_l2_resident": pts * K / (dev["ms_warm"] * 1e-3),
             "value_plain_call": pts * K / dev["plain_s"],
-            "fp64_plain": fp64,
+            "fp64_plain": fp64, "library_form": libform,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clk.summary(), "gpu_launches": dev["launches"], **EXTRA,
             "pe_curves_per_hour_e2e": curves_per_hour}
     print(json.dumps(line))
+
+
+def library_form(data, reps):
+    """ms per step of the column and l-space passes in their library forms
+    (cuFFT plans, cuBLAS GEMMs, elementwise phase kernels) on the workload's
+    shapes, from lib/libqd_libcmp.so."""
+    from qd_b200 import libcompare as LC
+    LC.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    runs = as_runs(data)
+    r0 = runs[0]
+    n1, n2, nth = int(r0.r1.n), int(r0.r2.n), int(r0.theta.n)
+    nl = max(int(r.theta.m) + 1 for r in runs)
+    lib = {"lspace_cufft_c2c_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), False, reps),
+           "lspace_cufft_z2z_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), True, reps)}
+    for c in LC.COMPUTE:
+        lib[f"column_cublas_{c}_ms"] = LC.column_cublas_ms(n1, n2, nth, nl, len(runs), c, reps)
+    return lib
 
 
 def run_compare_libs(args):
@@ -494,10 +528,7 @@ def run_compare_libs(args):
         dev = device_phase(data, prec, K, 3)
         ours[name] = {"column_ms": dev["kclass_ms"]["column"],
                       "lspace_ms": dev["kclass_ms"]["lines"], "step_ms": dev["ms"] / K}
-    lib = {"lspace_cufft_c2c_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), False, K),
-           "lspace_cufft_z2z_ms": LC.lspace_cufft_ms(n1, n2, nl, len(runs), True, K)}
-    for c in LC.COMPUTE:
-        lib[f"column_cublas_{c}_ms"] = LC.column_cublas_ms(n1, n2, nth, nl, len(runs), c, K)
+    lib = library_form(data, K)
     c64, f64 = ours["complex64"], ours["fp64"]
     ratios = {
         "lspace_complex64": lib["lspace_cufft_c2c_ms"] / c64["lspace_ms"],
@@ -528,6 +559,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="skip the plain FP64 form's rate on the same workload")
+    ap.add_argument("--no-lib-compare", action="store_true",
+                    help="skip the library forms of the passes in the default line")
     ap.add_argument("--compare-libs", action="store_true",
                     help="time the column and l-space passes against cuBLAS / cuFFT forms")
     args = ap.parse_args()
