@@ -429,6 +429,10 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     // slow tiles form the scaled theta-space state (EX: frow is uniform per tile)
     const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow || p.esum;
     float n_l = 0.f, sc = 1.f;
+    // GEMM1 output (theta values) of this thread; with one CTA per SM (128
+    // registers) a slow tile keeps its first TMEM read for the theta-space work
+    constexpr bool KEEP = ctas_per_sm(S) == 1;
+    float dv[H];
 
     if (mode != COL_HEAD) {
       // ---- A1 = psi'_l tile into TMEM, its norm, GEMM1 --------------------------------
@@ -463,10 +467,11 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         img_pending = true;
       }
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
-        float nt_part = 0.f, dv[H];
-        tmem_ld_all<H>(my_d, dv);
+        float nt_part = 0.f, dn[H];
+        float (&dl)[H] = KEEP ? dv : dn;
+        tmem_ld_all<H>(my_d, dl);
 #pragma unroll
-        for (int u = 0; u < H; u++) nt_part = fmaf(dv[u], dv[u], nt_part);
+        for (int u = 0; u < H; u++) nt_part = fmaf(dl[u], dl[u], nt_part);
         nt_part += __shfl_xor_sync(0xffffffffu, nt_part, 1);
         if (!is_im) xch[NG * TPTS + grp * TPTS + pt] = nt_part;
         __syncthreads();
@@ -484,9 +489,8 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
                                                  : nullptr;
     float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
                        : nullptr;
-    float dv[H];
     if (mode != COL_HEAD) {
-      tmem_ld_all<H>(my_d, dv);
+      if (!(KEEP && slow)) tmem_ld_all<H>(my_d, dv);
       if (slow) {                               // whole-tile branch: the fast tiles skip it
         if (p.esum) {                           // potential energy, before the absorber
           double ep = 0.0;
