@@ -327,8 +327,9 @@ int qd_mlp_potential(qd_mlp *m, const qd_radial *R, const qd_radial *r, const qd
 /* theta.legendre of centrifugal-sudden block K: L[l][k] =
  * Pbar_{K+l}^K(x_k) / sqrt(l + 1/2), l = 0..m, with Pbar_j^K the associated
  * Legendre function normalised to one on [-1, 1] (no Condon-Shortley phase),
- * by the standard three-term recurrence in j, FP64 on the host.  K = 0 gives
- * P_l(x_k), the reference's matrix. */
+ * by the standard three-term recurrence in j, one FP64 GPU thread per node.
+ * K = 0 gives P_l(x_k), the reference's matrix (as qd_legendre_matrix).
+ * QD_ERR_INVALID for a node outside [-1, 1]; QD_ERR_CUDA without a GPU. */
 int qd_cs_legendre(int32_t n, int32_t K, int32_t m, const double *x, double *legendre);
 
 /* Initial wavepacket on the GPU in FP64 (H3/InitWavePacket.m:13-31,

@@ -113,20 +113,47 @@ __global__ void k_legendre_matrices(int nth, int nl, const double *w, const doub
   }
 }
 
-// P_0..P_m at each node by the three-term recurrence of LegendreP2.m:9-21;
-// one thread per node; output (m+1) x n column-major.
-__global__ void k_legendre_p2(int n, int m, const double *x, double *out)
+// Angular basis at each node, one thread per node, output (m+1) x n
+// column-major (leg[l + k*(m+1)]).  K = 0: P_0..P_m by the three-term
+// recurrence of LegendreP2.m:9-21, unnormalised as theta.legendre is there.
+// K > 0 (a centrifugal-sudden block, H3/main.m:98-101): the associated
+// functions Pbar_{K+l}^K normalised to one on [-1, 1], started from
+// Pbar_K^K = sqrt(1/2) prod_{j<=K} sqrt((2j+1)/(2j)) (1-x^2)^{1/2} and raised
+// in degree by the standard normalised recurrence, then divided by
+// sqrt(l + 1/2) to the reference's scaling.
+__global__ void k_legendre_basis(int n, int K, int m, const double *x, double *out)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const double xk = x[k];
   double *v = out + (long)k * (m + 1);
-  double p0 = 1.0, p1 = xk;
-  v[0] = 1.0;
-  if (m >= 1) v[1] = xk;
-  for (int i = 2; i <= m; i++) {
-    const double p2 = (2.0 - 1.0 / i) * xk * p1 - (1.0 - 1.0 / i) * p0;
-    v[i] = p2;
+  if (K == 0) {
+    double p0 = 1.0, p1 = xk;
+    v[0] = 1.0;
+    if (m >= 1) v[1] = xk;
+    for (int i = 2; i <= m; i++) {
+      const double p2 = (2.0 - 1.0 / i) * xk * p1 - (1.0 - 1.0 / i) * p0;
+      v[i] = p2;
+      p0 = p1;
+      p1 = p2;
+    }
+    return;
+  }
+  const double s = sqrt(1.0 - xk * xk);
+  double p0 = sqrt(0.5);
+  for (int j = 1; j <= K; j++) p0 *= sqrt((2.0 * j + 1.0) / (2.0 * j)) * s;
+  v[0] = p0 / sqrt(0.5);
+  double p1 = 0.0;
+  if (m >= 1) {
+    p1 = sqrt(2.0 * K + 3.0) * xk * p0;
+    v[1] = p1 / sqrt(1.5);
+  }
+  for (int l = 2; l <= m; l++) {
+    const double j = K + l;
+    const double a = sqrt((4.0 * j * j - 1.0) / (j * j - (double)K * K));
+    const double b = sqrt(((j - 1) * (j - 1) - (double)K * K) / (4.0 * (j - 1) * (j - 1) - 1.0));
+    const double p2 = a * (xk * p1 - b * p0);
+    v[l] = p2 / sqrt(l + 0.5);
     p0 = p1;
     p1 = p2;
   }
@@ -164,9 +191,10 @@ cudaError_t launch_legendre_matrices(int nth, int nl, const double *, const doub
   return cudaGetLastError();
 }
 
-cudaError_t launch_legendre_p2(int n, int m, const double *x, double *legendre, cudaStream_t s)
+cudaError_t launch_legendre_basis(int n, int K, int m, const double *x, double *legendre,
+                                  cudaStream_t s)
 {
-  k_legendre_p2<<<(n + 127) / 128, 128, 0, s>>>(n, m, x, legendre);
+  k_legendre_basis<<<(n + 127) / 128, 128, 0, s>>>(n, K, m, x, legendre);
   return cudaGetLastError();
 }
 

@@ -1730,23 +1730,39 @@ int qd_read_grids(const char *dir, int32_t n, double *x, double *w)
   return QD_OK;
 }
 
-int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre)
+// Both angular-basis entry points: one FP64 kernel launch on the device.
+static int legendre_basis(const char *who, int32_t n, int32_t K, int32_t m, const double *x,
+                          double *legendre)
 {
-  if (!x || !legendre || n < 1 || m < 0) return set_err(QD_ERR_INVALID, "bad argument");
+  if (!x || !legendre || n < 1 || m < 0 || K < 0)
+    return set_err(QD_ERR_INVALID, "%s: bad argument (n %d, K %d, m %d)", who, n, K, m);
+  for (int k = 0; k < n; k++)
+    if (!(std::fabs(x[k]) <= 1.0))
+      return set_err(QD_ERR_INVALID, "%s: node %d (%g) is outside [-1, 1]", who, k, x[k]);
   double *dx = nullptr, *dl = nullptr;
   CU(cudaMalloc(&dx, sizeof(double) * n));
   cudaError_t e = cudaMalloc(&dl, sizeof(double) * (size_t)n * (m + 1));
   if (e != cudaSuccess) { cudaFree(dx); CU(e); }
   int rc = QD_OK;
   if (cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-      launch_legendre_p2(n, m, dx, dl, 0) != cudaSuccess ||
+      launch_legendre_basis(n, K, m, dx, dl, 0) != cudaSuccess ||
       cudaMemcpy(legendre, dl, sizeof(double) * (size_t)n * (m + 1), cudaMemcpyDeviceToHost) !=
           cudaSuccess)
-    rc = set_err(QD_ERR_CUDA, "qd_legendre_matrix: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = set_err(QD_ERR_CUDA, "%s: %s", who, cudaGetErrorString(cudaGetLastError()));
   g_launches++;
   cudaFree(dx);
   cudaFree(dl);
   return rc;
+}
+
+int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre)
+{
+  return legendre_basis("qd_legendre_matrix", n, 0, m, x, legendre);
+}
+
+int qd_cs_legendre(int32_t n, int32_t K, int32_t m, const double *x, double *legendre)
+{
+  return legendre_basis("qd_cs_legendre", n, K, m, x, legendre);
 }
 
 }  // extern "C"

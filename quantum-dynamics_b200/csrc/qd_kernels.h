@@ -249,7 +249,8 @@ cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const dou
                                      const double *legendre, double *P, double *WP,
                                      float *P32, float *WP32, float *P32lo, float *WP32lo,
                                      cudaStream_t s);
-cudaError_t launch_legendre_p2(int n, int m, const double *x, double *legendre, cudaStream_t s);
+cudaError_t launch_legendre_basis(int n, int K, int m, const double *x, double *legendre,
+                                  cudaStream_t s);
 cudaError_t launch_roots(int n, double2 *tw64, float2 *tw32, cudaStream_t s);
 // read a buffer through L2 (the clean-up half of the timed L2 flush)
 cudaError_t launch_l2_read(const void *buf, size_t bytes, cudaStream_t s);

@@ -163,8 +163,10 @@ def test_pes_callback_errors(qdlib):
     assert e.value.code == QD_ERR_PES
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("K", [0, 1, 3])
-def test_cs_legendre_matches_host(qdlib, K):
+def test_cs_legendre_on_gpu_matches_host(qdlib, K):
+    # the device basis against the host restatement systems.cs_legendre
     x, w = S.gauss_legendre(24)
     m = 23 - K
     out = np.empty((24, m + 1))
@@ -172,8 +174,26 @@ def test_cs_legendre_matches_host(qdlib, K):
                                     out.ctypes.data_as(_abi.c_double_p)))
     ref = S.cs_legendre(x, K, m)
     if K == 0:
-        assert np.array_equal(out, S.legendre_p2(m, x))
+        assert np.abs(out - S.legendre_p2(m, x)).max() < 1e-14
     assert np.abs(out - ref).max() < 1e-13
     # the reference's transform pair is the identity on the basis
     Q = np.sqrt(w)[:, None] * np.sqrt(np.arange(m + 1) + 0.5)[None, :] * out
     assert np.abs(Q.T @ Q - np.eye(m + 1)).max() < 1e-12
+
+
+@pytest.mark.parametrize("K", [0, 1, 3])
+def test_cs_legendre_host_is_orthonormal(K):
+    # the host restatement used to build test inputs: orthonormal under the
+    # quadrature for every K
+    x, w = S.gauss_legendre(24)
+    m = 23 - K
+    Q = np.sqrt(w)[:, None] * np.sqrt(np.arange(m + 1) + 0.5)[None, :] * S.cs_legendre(x, K, m)
+    assert np.abs(Q.T @ Q - np.eye(m + 1)).max() < 1e-12
+
+
+def test_cs_legendre_rejects_bad_nodes(qdlib):
+    x = np.array([0.0, 1.5])
+    out = np.empty((2, 2))
+    rc = qdlib.qd_cs_legendre(2, 1, 1, x.ctypes.data_as(_abi.c_double_p),
+                              out.ctypes.data_as(_abi.c_double_p))
+    assert rc == _abi.QD_ERR_INVALID and b"outside" in qdlib.qd_last_error()
