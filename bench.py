@@ -6,7 +6,7 @@
 Workload (default c4, the largest single-GPU configuration): a batch of 32
 F + H2 centrifugal-sudden blocks (J = 0-30, K <= 3, n_j = 128 - K) on a
 256 x 192 x 128 Jacobi grid, 201,326,592 grid points, complex64 wavefunction
-with the 3xTF32 Legendre GEMM and FP64 flux-to-P(E) accumulation, dt = 10 au,
+with the 3xFP16 Legendre GEMM and FP64 flux-to-P(E) accumulation, dt = 10 au,
 P(E) on 241 energies per block.  c2 is the 64-block batch on 128 x 96 x 64,
 c1 one F + H2 J = 0 run on 128 x 128 x 64.  A step is one split-operator
 step of every grid point of the workload, including the flux capture.
@@ -478,7 +478,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32", "data": "synthetic",
             "config": {"workload": desc, "grid_points": pts,
                        "precision": "FP64 plain" if args.fp64 else
-                       "complex64 + 3xTF32 Legendre + FP64 flux accumulation",
+                       "complex64 + 3xFP16 Legendre + FP64 flux accumulation",
                        "l2": "flushed before every step (256 MiB written, then read back so "
                              "no dirty lines remain; outside the timed spans)",
                        "parallelism": f"replicas x{world}"},

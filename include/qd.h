@@ -52,7 +52,7 @@ extern "C" {
 
 /* arithmetic of the propagation */
 #define QD_PREC_FP64  0  /* plain form: complex128 psi, FP64 everywhere       */
-#define QD_PREC_FP32  1  /* complex64 psi, 3xTF32 tensor-core Legendre GEMM,
+#define QD_PREC_FP32  1  /* complex64 psi, 3xFP16 tensor-core Legendre GEMM,
                             FP64 flux-to-P(E) accumulation and norm          */
 
 /* RadialCoordinate (common/MatlabStructures.h:12-39).  r0, k0, delta are the

@@ -1,31 +1,39 @@
 // k_column_tc.cu -- the column pass of the complex64 propagation on the
-// 5th-generation tensor cores (tcgen05, kind::tf32, accumulators in TMEM).
+// 5th-generation tensor cores (tcgen05, kind::f16, accumulators in TMEM).
 //
 // Same work as k_column.cu (B, dump, flux rows, norm, V, F; see there for the
 // reference functions), with both Legendre contractions as back-to-back
 // GEMMs per tile of 64 grid columns (S = n_l, n_theta padded to 16):
-//   GEMM1  D[128 x S] = A1[128 x S] * B1[S x S]    A1 = psi_l tile, B1[l][k] = P_l(x_k)
+//   GEMM1  D[128 x S] = A1[128 x S] * Q^T      A1 = psi'_l tile (K = l)
 //   theta-space ops on D (tcgen05.ld -> registers) -> A2 (TMEM)
-//   GEMM2  D[128 x S] = A2[128 x S] * B2[S x S]    B2[k][l] = (l+1/2) w_k P_l(x_k)
-// The 128 GEMM rows are the real and imaginary parts of the 64 complex
-// points (row 2p = Re, 2p+1 = Im), so the complex-by-real transform is one
-// real GEMM.  FP32 accuracy from TF32 units by split products (3xTF32)
-//   A*B ~ Ahi*Bhi + Ahi*Blo + Alo*Bhi,   A = Ahi + Alo,  Ahi = tf32(A),
-// with the constant Legendre matrices split the same way on the host.
+//   GEMM2  D[128 x S] = A2[128 x S] * Q        (K = k)
+// with Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k) (and its orthonormal
+// completion to n_theta orders, for the output norm).  The 128 GEMM rows are
+// the real and imaginary parts of the 64 complex points (row 2p = Re,
+// 2p+1 = Im), so the complex-by-real transform is one real GEMM.
+//
+// FP32 accuracy from FP16 units by split products (3xFP16):
+//   A*B ~ Ahi*Bhi + Ahi*Blo + Alo*Bhi,  Ahi = fp16(A), Alo = fp16(A - Ahi),
+// the same 11-bit significands as a TF32 split at twice the TF32 MMA rate.
+// FP16's narrow exponent range is handled by exact power-of-two scales: Q is
+// stored times 2^12 (its entries are at most 1, so the low parts stay normal),
+// and each complex point's row pair is scaled by 2^(13-e) with 2^e >= the
+// point's norm, so every scaled entry is at most 2^13 and entries down to
+// 2^-27 of the point's norm keep 11 bits.  The scales are undone on the FP32
+// accumulator outputs, folded into multiplications the epilogue does anyway.
 //
 // Data placement: the A operands live in tensor memory (written by the
-// threads with tcgen05.st; each thread owns one TMEM lane = one GEMM row and
-// a quarter of its columns), the constant B images in shared memory (K-major,
-// 128-byte swizzle, built once on the host), the accumulator in TMEM.  The
-// tile's exp(-i V dt) values are staged into shared memory by asynchronous
-// copies issued while the previous tile finishes.  512 threads per CTA.  TMEM
-// per CTA: [Ahi | Alo | D], S columns each.  S <= 64: two CTAs per SM overlap
-// each other's load / MMA / epilogue phases.  S = 96, 128 (n_theta up to 128):
-// one CTA per SM (512 TMEM columns); at S = 128 the four operand images
-// (256 KB) do not fit in shared memory together, so the CTA keeps one GEMM's
-// pair: B2 is copied over B1 as soon as GEMM1 has completed, and the next
-// tile's B1 over B2 as soon as GEMM2 has, each copy overlapping the work
-// between the two GEMMs or after them.
+// threads with tcgen05.st, two FP16 values per 32-bit column; each thread owns
+// one TMEM lane = one GEMM row and a quarter of its K range), the constant Q
+// image pair (hi | lo) in shared memory, the accumulator in TMEM.  One image
+// serves both GEMMs: stored with rows k and 64 orders l per 128-byte swizzled
+// row, it is the K-major operand of GEMM1 and the MN-major operand of GEMM2.
+// The tile's exp(-i V dt) values are staged into shared memory by
+// asynchronous copies issued while the previous tile finishes.  512 threads
+// per CTA.  S <= 64: two CTAs per SM overlap each other's load / MMA /
+// epilogue phases; S = 96, 128 (n_theta up to 128): one CTA per SM, which
+// issues the next tile's GEMM1 as soon as the current tile's GEMM2 output is
+// in registers.
 //
 // Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
 // smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
@@ -37,8 +45,8 @@
 //   sum_k w_k |psi_theta|^2 = sum_l |psi_l|^2/(l+1/2)
 // (times the absorber squared).  The state is kept in the orthonormal basis
 // psi'_l = psi_l/sqrt(l+1/2), where these norms are plain sums of squares.
-// For n_l < n_theta, GEMM2 also forms the orders n_l..n_theta-1 (rows from the
-// same three-term recurrence) for the norm only; they are not stored.  This
+// For n_l < n_theta, GEMM2 also forms the orders n_l..n_theta-1 (the
+// completion columns of Q) for the norm only; they are not stored.  This
 // fixes the magnitude only; shape and phase stay as computed.
 //
 // One thread issues the MMAs; completion arrives on an mbarrier through
@@ -47,6 +55,7 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include <cuda_fp16.h>
 #include "qd.h"
 #include "qd_tc.h"
 
@@ -56,34 +65,28 @@ constexpr int TPTS = 64;          // complex grid points per tile
 constexpr int MROWS = 128;        // GEMM rows per tile
 constexpr int NTHREADS = 512;
 constexpr int MAXS = 128;         // max padded n_l / n_theta handled here
-// per-size resources: TMEM columns (Ahi | Alo | D, S each, rounded up to a
-// power of two), CTAs per SM, and whether both GEMMs' operand images stay in
-// shared memory (else the CTA streams B1 and B2 in turn through one buffer)
-__host__ __device__ constexpr uint32_t tmem_cols(int S) { return 3 * S <= 256 ? 256u : 512u; }
-__host__ __device__ constexpr int ctas_per_sm(int S) { return 3 * S <= 256 ? 2 : 1; }
-__host__ __device__ constexpr bool stream_images(int S) { return S > 96; }
+constexpr int B_LOG2 = 12;        // Q is stored times 2^12
+constexpr int A_LOG2 = 13;        // scaled A entries are at most 2^13
+// per-size resources: TMEM columns of each A half (S/2 packed columns,
+// rounded up to 16), the allocation (Ahi | Alo | D, a power of two), CTAs per SM
+__host__ __device__ constexpr int a_cols(int S) { return (S / 2 + 15) / 16 * 16; }
+__host__ __device__ constexpr uint32_t tmem_cols(int S)
+{
+  return 2 * a_cols(S) + S <= 64 ? 64u : 2 * a_cols(S) + S <= 128 ? 128u : 256u;
+}
+__host__ __device__ constexpr int ctas_per_sm(int S) { return S <= 64 ? 2 : 1; }
+// bytes of one operand image (hi or lo): 128-byte rows of 64 orders, S rows
+// per 64-order block
+__host__ __device__ constexpr int image_bytes(int S) { return (S + 63) / 64 * S * 128; }
 constexpr long WAIT_LIMIT = 1L << 22;   // mbarrier polls before giving up
 
 
-// byte offset of element (r, k) in a K-major SW128 operand of R rows
-__host__ __device__ __forceinline__ uint32_t sw128_off(int r, int k, int R)
+// byte offset of 16-bit element (r, c) of an operand image of R rows, 64
+// columns per 128-byte swizzled row (16-byte chunk index XOR row mod 8)
+__host__ __device__ __forceinline__ uint32_t sw128_off16(int r, int c, int R)
 {
-  const int a = k >> 5, c = (k & 31) >> 2;
-  return (uint32_t)(a * R * 128 + r * 128 + ((c ^ (r & 7)) << 4) + ((k & 3) << 2));
-}
-
-// host: round to TF32 (nearest even on the 13 dropped bits)
-float tf32_round_host(float x)
-{
-  uint32_t b;
-  std::memcpy(&b, &x, 4);
-  if ((b & 0x7f800000u) != 0x7f800000u) {
-    b += 0xfffu + ((b >> 13) & 1u);
-    b &= 0xffffe000u;
-  }
-  float y;
-  std::memcpy(&y, &b, 4);
-  return y;
+  const int a = c >> 6, ch = (c & 63) >> 3;
+  return (uint32_t)(a * R * 128 + r * 128 + ((ch ^ (r & 7)) << 4) + ((c & 7) << 1));
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -91,32 +94,53 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p)
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// round a finite FP32 value to TF32 (10 stored mantissa bits), to nearest
-// with ties away from zero, on its bit pattern: add half of the dropped
-// 13-bit field to the magnitude and clear the field (a carry moves into the
-// exponent, which is the correct round-up); the same result as
-// cvt.rna.tf32.f32 for finite inputs, in two integer operations
-__device__ __forceinline__ float tf32_rna(float x)
+// 2^k for integer k in [-126, 127]
+__host__ __device__ __forceinline__ float exp2i(int k)
 {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
+#ifdef __CUDA_ARCH__
+  return __int_as_float((k + 127) << 23);
+#else
+  return std::ldexp(1.0f, k);
+#endif
 }
 
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr)
+// e with sqrt(n) <= 2^e for a point norm n >= 0 (from n's exponent field;
+// clamped so that every scale below stays a normal FP32 number)
+__device__ __forceinline__ int norm_exp(float n)
+{
+  const int eb = (__float_as_int(n) >> 23) & 0xff;
+  const int e = eb == 0 ? -60 : (eb - 125) >> 1;
+  return e < -60 ? -60 : e > 60 ? 60 : e;
+}
+
+// shared-memory matrix descriptors, 128-byte swizzle (sm100 format):
+// K-major (GEMM1: 8-row groups 1024 B apart, K inside the row) and MN-major
+// (GEMM2: K rows 128 B apart in 8-row groups 1024 B apart, 64-element MN
+// blocks lbo bytes apart)
+__device__ __forceinline__ uint64_t desc_common(uint32_t saddr)
 {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3fffu);          // start address
-  d |= (uint64_t)1u << 16;                          // LBO (unused for SW128 K-major)
   d |= (uint64_t)(1024u >> 4) << 32;                // SBO: 8 rows x 128 B
   d |= (uint64_t)1u << 46;                          // descriptor version (sm100)
   d |= (uint64_t)2u << 61;                          // SWIZZLE_128B
   return d;
 }
-
-// kind::tf32 instruction descriptor: D f32, A/B tf32, both K-major, M=128, N
-__host__ __device__ constexpr uint32_t make_idesc(int N)
+__device__ __forceinline__ uint64_t make_desc_k(uint32_t saddr)
 {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(MROWS >> 4) << 24);
+  return desc_common(saddr) | ((uint64_t)1u << 16);            // LBO unused (1)
+}
+__device__ __forceinline__ uint64_t make_desc_mn(uint32_t saddr, uint32_t lbo)
+{
+  return desc_common(saddr) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16);
+}
+
+// kind::f16 instruction descriptor: D f32, A/B f16, A K-major, B K- or
+// MN-major, M = 128, N
+__host__ __device__ constexpr uint32_t make_idesc(int N, bool b_mn)
+{
+  return (1u << 4) | (0u << 7) | (0u << 10) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(MROWS >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar)
@@ -149,7 +173,7 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 struct TcDev {
-  const float4 *mats;    // image sets (B1 hi|lo, B2 hi|lo), set_bytes apart
+  const float4 *mats;    // image sets (Q hi|lo), set_bytes apart
   uint32_t set_bytes;
   const int *run_set;    // image set of each run (null: set 0)
   const int *run_order;  // tile order: virtual run v is run_order[v], runs of a set adjacent
@@ -163,12 +187,17 @@ struct TcDev {
 };
 
 
-// tcgen05.st of 4 consecutive 32-bit columns of this thread's lane
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, float a, float b, float c, float d)
+// tcgen05.st of 2 / 4 consecutive 32-bit columns of this thread's lane
+__device__ __forceinline__ void tmem_st2(uint32_t taddr, uint32_t a, uint32_t b)
+{
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};"
+               :: "r"(taddr), "r"(a), "r"(b) : "memory");
+}
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c,
+                                         uint32_t d)
 {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
-               :: "r"(taddr), "r"(__float_as_uint(a)), "r"(__float_as_uint(b)),
-                  "r"(__float_as_uint(c)), "r"(__float_as_uint(d)) : "memory");
+               :: "r"(taddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
@@ -193,42 +222,84 @@ __device__ __forceinline__ void tmem_ld_all(uint32_t taddr, float (&v)[H])
   for (int u = 0; u < H; u++) v[u] = __uint_as_float(r[u]);
 }
 
-// the split of 4 values into the Ahi and Alo TMEM columns (col0 % 4 == 0)
+// hi and lo FP16 parts of two values, each pair packed into one 32-bit
+// column (the even K index in the low half)
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_t &lo)
+{
+  const __half2 h = __floats2half2_rn(x0, x1);
+  const float2 b = __half22float2(h);
+  const __half2 l = __floats2half2_rn(x0 - b.x, x1 - b.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+
+// the split of 4 values (K indices k..k+3, k % 4 == 0) into the Ahi and Alo
+// TMEM columns k/2, k/2+1
 __device__ __forceinline__ void put4_tmem(uint32_t ahi, uint32_t alo, float x0, float x1,
                                           float x2, float x3)
 {
-  const float h0 = tf32_rna(x0), h1 = tf32_rna(x1), h2 = tf32_rna(x2), h3 = tf32_rna(x3);
-  tmem_st4(ahi, h0, h1, h2, h3);
-  tmem_st4(alo, tf32_rna(x0 - h0), tf32_rna(x1 - h1), tf32_rna(x2 - h2), tf32_rna(x3 - h3));
+  uint32_t h0, l0, h1, l1;
+  split2(x0, x1, h0, l0);
+  split2(x2, x3, h1, l1);
+  tmem_st2(ahi, h0, h1);
+  tmem_st2(alo, l0, l1);
 }
 
-__device__ __forceinline__ void mma_tf32_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
-                                            uint32_t idesc, uint32_t accumulate)
+// the split of a thread's H values (K indices c0..c0+H-1) times the point
+// scale sa into its Ahi / Alo columns
+template <int H>
+__device__ __forceinline__ void put_row(uint32_t my_hi, uint32_t my_lo, const float (&v)[H],
+                                        float sa)
+{
+  if constexpr (H % 8 == 0) {
+#pragma unroll
+    for (int u = 0; u < H; u += 8) {
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int x = 0; x < 4; x++) split2(v[u + 2 * x] * sa, v[u + 2 * x + 1] * sa, h[x], l[x]);
+      tmem_st4(my_hi + u / 2, h[0], h[1], h[2], h[3]);
+      tmem_st4(my_lo + u / 2, l[0], l[1], l[2], l[3]);
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < H; u += 4)
+      put4_tmem(my_hi + u / 2, my_lo + u / 2, v[u] * sa, v[u + 1] * sa, v[u + 2] * sa,
+                v[u + 3] * sa);
+  }
+}
+
+__device__ __forceinline__ void mma_f16_ts(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate)
 {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n"
       :
       : "r"(dtmem), "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
-// D = A * B over K = S, A in TMEM columns [ahi, ahi+S) and [alo, alo+S), B at
-// b (hi | lo, b_bytes apart): the small split terms first, main last
-template <int S>
+// D = A * B over K = S, A in TMEM columns [ahi, ahi+S/2) and [alo, alo+S/2)
+// (packed FP16 pairs), B the image pair at b (hi | lo, image_bytes(S) apart):
+// GEMM1 (MN = false) reads it K-major, GEMM2 (MN = true) MN-major.  The small
+// split terms first, the main one last.
+template <int S, bool MN>
 __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint32_t alo,
-                                              uint32_t b, int b_bytes)
+                                              uint32_t b)
 {
-  constexpr uint32_t idesc = make_idesc(S);
+  constexpr uint32_t idesc = make_idesc(S, MN);
+  constexpr int BB = image_bytes(S);
 #pragma unroll 1
   for (int term = 0; term < 3; term++) {
     // term 0: Ahi*Blo, 1: Alo*Bhi, 2: Ahi*Bhi
     const uint32_t a = term == 1 ? alo : ahi;
-    const uint32_t bt = b + (term == 0 ? b_bytes : 0);
+    const uint32_t bt = b + (term == 0 ? BB : 0);
 #pragma unroll
-    for (int kk = 0; kk < S; kk += 8) {
-      const uint32_t boff = (uint32_t)((kk >> 5) * S * 128 + ((kk & 31) >> 3) * 32);
-      mma_tf32_ts(dtmem, a + kk, make_desc(bt + boff), idesc, (term | kk) ? 1u : 0u);
+    for (int kk = 0; kk < S; kk += 16) {
+      uint64_t desc;
+      if constexpr (MN) desc = make_desc_mn(bt + (uint32_t)kk * 128u, (uint32_t)S * 128u);
+      else desc = make_desc_k(bt + (uint32_t)((kk >> 6) * S * 128 + ((kk & 63) >> 4) * 32));
+      mma_f16_ts(dtmem, a + kk / 2, desc, idesc, (term | kk) ? 1u : 0u);
     }
   }
 }
@@ -240,31 +311,34 @@ constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share
 //
 // Orthonormal representation.  The l-space state is kept as
 // psi'_l = psi_l / sqrt(l+1/2) and theta values as sqrt(w_k) psi(theta_k), so
-// both transforms use the same matrix Q[k][l] = sqrt(w_k) sqrt(l+1/2) P_l(x_k)
-// (B: D1 = Q psi', F: psi' = Q^T A2) and every norm is a plain sum of squares.
+// both transforms use the same matrix Q (B: D1 = Q psi', F: psi' = Q^T A2)
+// and every norm is a plain sum of squares.
 // Renormalisation.  The column output is rescaled to the norm the exact
 // transform pair would give, dd^2 * sum_l |psi'_l|^2 per grid column (dd =
 // absorber); the theta-space intermediate needs its own scale only where it
-// leaves the kernel (flux rows, psi_z, the last step of a call: the "slow"
-// tiles), elsewhere GEMM2 runs on V * D1 unscaled and one factor
-// dd sqrt(n_l / n_out) at the store does both.
+// leaves the kernel (flux rows, psi_z, energies, the last step of a call: the
+// "slow" tiles), elsewhere GEMM2 runs on V * D1 as it comes out of GEMM1 and
+// one factor dd sqrt(n_l / n_out) at the store does both.
+// Scales.  A point with l-space norm n_l gets the A scale 2^(13-e), 2^e >=
+// sqrt(n_l) (the exponent pe below); GEMM1's output is then 2^(25-e) times
+// the theta values, so the fast tiles form A2 = 2^-12 * V * D1 (the same
+// scale 2^(13-e), as the transform preserves the norm), and the rescalings
+// to a known norm above are scale-free.
 // MS: runs of the batch have different angular bases (image sets, orders stored)
 template <int S, int MODE, bool EX, bool MS>
 __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnParams p, TcDev t)
 {
   constexpr int mode = MODE;
   constexpr int H = S / NG;                    // K columns per thread (one group)
-  constexpr int NKA = (S + 31) / 32;           // 128-byte swizzle atoms along K
-  constexpr int B_BYTES = NKA * S * 128;
-  constexpr bool STREAM = stream_images(S);    // B1 and B2 take turns in one buffer
+  constexpr int BB = image_bytes(S);
+  constexpr int AC = a_cols(S);
   constexpr uint32_t TMEM_COLS = tmem_cols(S);
   static_assert(H % 4 == 0, "column group must be a multiple of 4");
   extern __shared__ unsigned char smem_raw[];
   const uint32_t base_u = smem_u32(smem_raw);
   unsigned char *base = smem_raw + ((1024u - (base_u & 1023u)) & 1023u);
-  unsigned char *B1 = base;                     // hi | lo
-  unsigned char *B2 = STREAM ? base : B1 + 2 * B_BYTES;
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(base + (STREAM ? 2 : 4) * B_BYTES);
+  unsigned char *Bq = base;                     // Q image pair: hi | lo
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(base + 2 * BB);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 4);
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *sw = xch + 4 * NG * TPTS;                        // [S] sqrt(w_k), 0 beyond n_theta
@@ -295,35 +369,25 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   const int tbeg = blockIdx.x, tend = ntiles;
 #define QD_DIV(x, m) ((int)(((uint64_t)(uint32_t)(x) * (m)) >> 40))
 #define QD_RUN_OF(tl) (MS && t.run_order ? t.run_order[QD_DIV(tl, t.m_tpr)] : QD_DIV(tl, t.m_tpr))
-  const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the B-image copy
-  // images [first, first + count) of set `st` (B1 hi, B1 lo, B2 hi, B2 lo,
-  // B_BYTES each, multiples of 16) by bulk asynchronous copies from this
-  // GPU's global memory into this CTA's shared memory at B1, completing on
-  // mbar[3]
-#define QD_LOAD_B(st, first, count)                                                    \
+  const uint32_t mb3 = smem_u32(&mbar[3]);      // completion of the image copy
+  // the image pair of set `st` (2 x BB bytes, a multiple of 16) by bulk
+  // asynchronous copies from this GPU's global memory into this CTA's shared
+  // memory, completing on mbar[3]
+#define QD_LOAD_IMAGES(st)                                                             \
   do {                                                                                 \
-    const uint32_t total = (count) * B_BYTES, chunk = 16384;                           \
+    const uint32_t total = 2 * BB, chunk = 16384;                                      \
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"              \
                  :: "r"(mb3), "r"(total) : "memory");                                  \
-    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes + \
-                      (size_t)(first) * B_BYTES;                                       \
+    const char *src = reinterpret_cast<const char *>(t.mats) + (size_t)(st) * t.set_bytes; \
     for (uint32_t off = 0; off < total; off += chunk) {                                \
       const uint32_t n = total - off < chunk ? total - off : chunk;                    \
       asm volatile(                                                                    \
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" \
-          :: "r"(smem_u32(B1) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
+          :: "r"(smem_u32(Bq) + off), "l"(src + off), "r"(n), "r"(mb3) : "memory");    \
     }                                                                                  \
-  } while (0)
-  // the images one launch of this mode needs resident: all four, or with
-  // STREAM the pair of the mode's single GEMM (B2 for HEAD) or B1 to start MID
-#define QD_LOAD_IMAGES(st)                                                             \
-  do {                                                                                 \
-    if (!STREAM) QD_LOAD_B(st, 0, 4);                                                  \
-    else QD_LOAD_B(st, mode == COL_HEAD ? 2 : 0, 2);                                   \
   } while (0)
 #define QD_SET_OF(tl) (MS && t.run_set ? t.run_set[QD_RUN_OF(tl)] : 0)
   int loaded = tbeg < tend ? QD_SET_OF(tbeg) : 0;   // image set in smem
-  bool img_pending = false;                     // a streamed image copy not yet waited on
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])));
@@ -384,31 +448,27 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t lane_base = ((uint32_t)((warp & 3) * 32)) << 16;
-  const uint32_t Ahi = tmem, Alo = tmem + S, D = tmem + 2 * S;       // column bases
-  const uint32_t my_hi = Ahi + lane_base + c0, my_lo = Alo + lane_base + c0;
+  const uint32_t Ahi = tmem, Alo = tmem + AC, D = tmem + 2 * AC;     // column bases
+  const uint32_t my_hi = Ahi + lane_base + c0 / 2, my_lo = Alo + lane_base + c0 / 2;
   const uint32_t my_d = D + lane_base + c0;
   const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
+  const uint32_t bq = smem_u32(Bq);
   uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
   // every thread observes each mbarrier completion itself before it reads
   // what the asynchronous operation wrote
   bool failed = __syncthreads_or(!mbar_wait(mb3, 0));
-  // MID without image streaming: the tile's A1 is already in TMEM and its
-  // GEMM1 issued -- done at the end of the previous tile, as soon as that
-  // tile's GEMM2 output was in registers, so that GEMM1 runs under the
-  // previous tile's norm exchange and stores
+  // MID: the tile's A1 is already in TMEM and its GEMM1 issued -- done at the
+  // end of the previous tile, as soon as that tile's GEMM2 output was in
+  // registers, so that GEMM1 runs under the previous tile's stores
   bool a_ready = false;
+  float n_l_next = 0.f;                         // l-space point norm of that next tile
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
     const int run = QD_RUN_OF(tile);
     int nlr = nl;                               // orders stored for this run
-    if (STREAM && mode == COL_MID && img_pending) {   // B1 of this tile, issued last tile
-      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
-      ph3 ^= 1;
-      img_pending = false;
-    }
     if constexpr (MS) {
       const int set = t.run_set ? t.run_set[run] : 0;
-      if (!a_ready && !(STREAM && mode == COL_MID) && set != loaded) {   // another angular basis
+      if (!a_ready && set != loaded) {          // another angular basis
         if (tid == 0) QD_LOAD_IMAGES(set);      // earlier MMAs have all completed
         if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
         ph3 ^= 1;
@@ -429,43 +489,42 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     // slow tiles form the scaled theta-space state (EX: frow is uniform per tile)
     const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow || p.esum;
     float n_l = 0.f, sc = 1.f;
+    int pe = 0;                                 // the point's scale exponent
     // GEMM1 output (theta values) of this thread; with one CTA per SM (128
     // registers) a slow tile keeps its first TMEM read for the theta-space work
     constexpr bool KEEP = ctas_per_sm(S) == 1;
     float dv[H];
 
     if (mode != COL_HEAD) {
-      // ---- A1 = psi'_l tile into TMEM, its norm, GEMM1 --------------------------------
+      // ---- A1 = psi'_l tile into TMEM (scaled by its point norm), GEMM1 ---------------
       if (!a_ready) {
         float nl_part = 0.f;
 #pragma unroll
-        for (int u = 0; u < H; u += 4) {
-          put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
-          nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
-                    fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
-        }
-        tmem_wait_st();
-        tc_fence_before();
+        for (int u = 0; u < H; u++) nl_part = fmaf(a[u], a[u], nl_part);
         nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
         if (!is_im) xch[grp * TPTS + pt] = nl_part;
         if (mode == COL_MID) asm volatile("cp.async.wait_group 0;" ::: "memory");   // evs
         __syncthreads();
+#pragma unroll
+        for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
+        pe = norm_exp(n_l);
+        put_row<H>(my_hi, my_lo, a, exp2i(A_LOG2 - pe));
+        tmem_wait_st();
+        tc_fence_before();
+        __syncthreads();
         if (tid == 0) {
           tc_fence_after();
-          gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
+          gemm_split_ts<S, false>(D, Ahi, Alo, bq);
           mma_commit(mb1);
         }
+      } else {
+        n_l = n_l_next;
+        pe = norm_exp(n_l);
       }
       a_ready = false;
-#pragma unroll
-      for (int g = 0; g < NG; g++) n_l += xch[g * TPTS + pt];
       if (__syncthreads_or(!mbar_wait(mb1, ph1))) { failed = true; break; }
       ph1 ^= 1;
       tc_fence_after();
-      if (STREAM && mode == COL_MID) {          // B1 is free: B2 of this tile's set in its place
-        if (tid == 0) QD_LOAD_B(QD_SET_OF(tile), 2, 2);
-        img_pending = true;
-      }
       if (slow) {                               // theta norm of GEMM1 -> isometry scale
         float nt_part = 0.f, dn[H];
         float (&dl)[H] = KEEP ? dv : dn;
@@ -478,13 +537,14 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         float n_t = 0.f;
 #pragma unroll
         for (int g = 0; g < NG; g++) n_t += xch[NG * TPTS + g * TPTS + pt];
-        sc = (t.renorm && n_t > 0.f) ? sqrtf(n_l / n_t) : 1.f;
+        // to the exact norm n_l (scale-free), or just undo the scales
+        sc = t.renorm ? (n_t > 0.f ? sqrtf(n_l / n_t) : 1.f) : exp2i(pe - A_LOG2 - B_LOG2);
       }
     }
 
     // ---- theta-space operations, A2 into TMEM ----------------------------------------
     float tsum = 0.f;                           // this thread's share of sum_k |theta'_k|^2
-    const float sin_ = sc * ddv;                // slow tiles: scaled theta values
+    const float sin_ = sc * ddv;                // slow tiles: true theta values
     double *zrow = (mode != COL_HEAD && p.out_z) ? psiz + 2 * ((size_t)run * nth * n12 + q) + comp
                                                  : nullptr;
     float *srow = frow ? surf + 2 * (((size_t)run * p.surf_nrows + (j - p.surf_j0)) * nth * n1 + i) + comp
@@ -518,42 +578,35 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         }
       }
     }
+    if (mode == COL_MID) {                      // V z, into TMEM at the point's scale
 #pragma unroll
-    for (int u = 0; u < H; u += 4) {
-      float v[4];
-      if (mode != COL_HEAD) {
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-          v[x] = dv[u + x];
-          if (mode == COL_MID) {
-            const float other = __shfl_xor_sync(0xffffffffu, v[x], 1);
-            const float2 e = evs[(c0 + u + x) * TPTS + pt];
-            v[x] = fmaf(other * ysg, e.y, v[x] * e.x);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-          const int k = c0 + u + x;
-          float val = 0.f;
-          if (qok && k < nth) {
-            const size_t g = (size_t)k * n12 + q;
-            const double2 z = p.psi_z[(size_t)run * nth * n12 + g];
-            double s, c;
-            sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
-            double2 f = make_double2(c, -s);
-            if (p.prestep) {                     // psi / sqrt(v) * v = psi * sqrt(v)
-              double sh, ch;
-              sincos(0.5 * atan2(-s, c), &sh, &ch);
-              f = make_double2(ch, sh);
-            }
-            val = (float)((is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y) * sqrt(p.w[k]));
-          }
-          v[x] = val;
-          tsum = fmaf(val, val, tsum);
-        }
+      for (int u = 0; u < H; u++) {
+        const float other = __shfl_xor_sync(0xffffffffu, dv[u], 1);
+        const float2 e = evs[(c0 + u) * TPTS + pt];
+        dv[u] = fmaf(other * ysg, e.y, dv[u] * e.x);
       }
-      if (mode != COL_TAIL) put4_tmem(my_hi + u, my_lo + u, v[0], v[1], v[2], v[3]);
+      put_row<H>(my_hi, my_lo, dv, slow ? exp2i(A_LOG2 - pe) : exp2i(-B_LOG2));
+    } else if (mode == COL_HEAD) {              // psi_z -> theta' values (FP64 phase)
+#pragma unroll
+      for (int u = 0; u < H; u++) {
+        const int k = c0 + u;
+        float val = 0.f;
+        if (qok && k < nth) {
+          const size_t g = (size_t)k * n12 + q;
+          const double2 z = p.psi_z[(size_t)run * nth * n12 + g];
+          double s, c;
+          sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
+          double2 f = make_double2(c, -s);
+          if (p.prestep) {                     // psi / sqrt(v) * v = psi * sqrt(v)
+            double sh, ch;
+            sincos(0.5 * atan2(-s, c), &sh, &ch);
+            f = make_double2(ch, sh);
+          }
+          val = (float)((is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y) * sqrt(p.w[k]));
+        }
+        dv[u] = val;
+        tsum = fmaf(val, val, tsum);
+      }
     }
     // target norm of the column output (and the step norm of the point)
     float target;
@@ -561,7 +614,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       tsum += __shfl_xor_sync(0xffffffffu, tsum, 1);
       if (!is_im) xch[2 * NG * TPTS + grp * TPTS + pt] = tsum;
     }
-    if (mode != COL_TAIL) tmem_wait_st();
+    if (mode == COL_MID) tmem_wait_st();
     tc_fence_before();
     __syncthreads();
     if (slow || mode == COL_HEAD) {
@@ -570,6 +623,13 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       for (int g = 0; g < NG; g++) target += xch[2 * NG * TPTS + g * TPTS + pt];
     } else {
       target = ddv * ddv * n_l;
+    }
+    if (mode == COL_HEAD) {                     // A2 at the scale of the point's norm
+      pe = norm_exp(target);
+      put_row<H>(my_hi, my_lo, dv, exp2i(A_LOG2 - pe));
+      tmem_wait_st();
+      tc_fence_before();
+      __syncthreads();
     }
     if (p.norm_out && mode != COL_HEAD) {       // this tile's share of its run's norm
       double s = (grp == 0 && !is_im && qok) ? (double)target : 0.0;
@@ -584,24 +644,15 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
-    if (STREAM && mode == COL_MID) {            // B2 in place
-      if (__syncthreads_or(!mbar_wait(mb3, ph3))) { failed = true; break; }
-      ph3 ^= 1;
-      img_pending = false;
-    }
     if (tid == 0) {
       tc_fence_after();
-      gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B2), B_BYTES);
+      gemm_split_ts<S, true>(D, Ahi, Alo, bq);
       mma_commit(mb2);
     }
     if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
-    if (STREAM && mode == COL_MID && tile + (int)gridDim.x < tend) {   // B1 of the next tile
-      if (tid == 0) QD_LOAD_B(QD_SET_OF(tile + (int)gridDim.x), 0, 2);
-      img_pending = true;
-    }
     float no_part = 0.f, ov[H];
     tmem_ld_all<H>(my_d, ov);
 #pragma unroll
@@ -611,11 +662,10 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     }
     no_part += __shfl_xor_sync(0xffffffffu, no_part, 1);
     if (!is_im) xch[3 * NG * TPTS + grp * TPTS + pt] = no_part;
-    // without streaming: the next tile's A1 into TMEM and its GEMM1, while
-    // this tile finishes (GEMM2 has completed, so its A2 is free, and this
-    // thread's D is in ov)
+    // the next tile's A1 into TMEM and its GEMM1, while this tile finishes
+    // (GEMM2 has completed, so its A2 is free, and this thread's D is in ov)
     const int nxt = tile + (int)gridDim.x;
-    const bool ahead = !STREAM && mode == COL_MID && nxt < tend;
+    const bool ahead = mode == COL_MID && nxt < tend;
     if (ahead) {
       if constexpr (MS) {
         const int set = t.run_set ? t.run_set[QD_RUN_OF(nxt)] : 0;
@@ -628,30 +678,34 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       }
       float nl_part = 0.f;
 #pragma unroll
-      for (int u = 0; u < H; u += 4) {
-        put4_tmem(my_hi + u, my_lo + u, a[u], a[u + 1], a[u + 2], a[u + 3]);
-        nl_part = fmaf(a[u], a[u], fmaf(a[u + 1], a[u + 1],
-                  fmaf(a[u + 2], a[u + 2], fmaf(a[u + 3], a[u + 3], nl_part))));
-      }
-      tmem_wait_st();
+      for (int u = 0; u < H; u++) nl_part = fmaf(a[u], a[u], nl_part);
       nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
       if (!is_im) xch[grp * TPTS + pt] = nl_part;
       asm volatile("cp.async.wait_group 0;" ::: "memory");   // the next tile's evs
     }
     tc_fence_before();
     __syncthreads();
-    if (ahead && tid == 0) {
-      tc_fence_after();
-      gemm_split_ts<S>(D, Ahi, Alo, smem_u32(B1), B_BYTES);
-      mma_commit(mb1);
-    }
-    a_ready = ahead;
     float n_o = 0.f;
 #pragma unroll
     for (int g = 0; g < NG; g++) n_o += xch[3 * NG * TPTS + g * TPTS + pt];
+    if (ahead) {
+      n_l_next = 0.f;
+#pragma unroll
+      for (int g = 0; g < NG; g++) n_l_next += xch[g * TPTS + pt];
+      put_row<H>(my_hi, my_lo, a, exp2i(A_LOG2 - norm_exp(n_l_next)));
+      tmem_wait_st();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        gemm_split_ts<S, false>(D, Ahi, Alo, bq);
+        mma_commit(mb1);
+      }
+    }
+    a_ready = ahead;
     float so;
     if (t.renorm) so = n_o > 0.f ? sqrtf(target / n_o) : 1.f;
-    else so = (slow || mode == COL_HEAD) ? 1.f : ddv;
+    else so = ((slow || mode == COL_HEAD) ? 1.f : ddv) * exp2i(pe - A_LOG2 - B_LOG2);
     float *dst = ldst + (size_t)run * nl * stride + (size_t)c0 * stride + 2 * q + comp;
     if (EX && (!MS || c0 + H <= nlr)) {         // every order of this column group is stored
 #pragma unroll
@@ -666,14 +720,12 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
 #undef QD_PREFETCH_A
 #undef QD_STAGE_EV
 #undef QD_LOAD_IMAGES
-#undef QD_LOAD_B
 #undef QD_SET_OF
 #undef QD_RUN_OF
 #undef QD_DIV
 
   if (failed && lane == 0) atomicExch(t.status, 1);
   asm volatile("cp.async.wait_group 0;" ::: "memory");   // no copy outlives the CTA
-  if (STREAM && img_pending) mbar_wait(mb3, ph3);        // (bounded; after a failed wait)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -741,12 +793,11 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 
 template <int S> constexpr int smem_bytes_for()
 {
-  return 1024 + (stream_images(S) ? 2 : 4) * ((S + 31) / 32) * S * 128 + 4 * 8 + 32 * 8 +
-         4 * NG * TPTS * 4 + 2 * S * 4 +
-         S * TPTS * 8;   // B images, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
+  return 1024 + 2 * image_bytes(S) + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
+         S * TPTS * 8;   // Q image pair, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
-static_assert(smem_bytes_for<128>() <= 227 * 1024 && smem_bytes_for<96>() <= 227 * 1024,
-              "shared memory of the largest column tiles");
+static_assert(smem_bytes_for<128>() <= 227 * 1024 && 2 * smem_bytes_for<64>() <= 227 * 1024,
+              "shared memory of the column tiles");
 
 // the kernel sizes built: S is n_l / n_theta padded up to one of them
 int kernel_size(int n)
@@ -804,26 +855,28 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
     if (have < nth) renorm = false;
     Qx[t] = basis;                                     // nth columns: Q, then the completion
   }
-  const int nka = (S + 31) / 32;
-  const int bb = nka * S * 128;
-  const size_t set_bytes = 4 * (size_t)bb;
+  // one image pair per set: row k (< n_theta) holds Q[k][l] times 2^12 for the
+  // orders GEMM2 forms (the stored ones and, with renormalisation, the
+  // completion up to n_theta), split into FP16 hi and lo parts
+  const int bb = image_bytes(S);
+  const size_t set_bytes = 2 * (size_t)bb;
   std::vector<unsigned char> img(set_bytes * nsets, 0);
-  auto put = [&](unsigned char *img2, int r, int k, double val) {     // hi | lo
-    const float h = tf32_round_host((float)val);
-    const float l = tf32_round_host((float)(val - (double)h));
-    const uint32_t off = sw128_off(r, k, S);
-    std::memcpy(img2 + off, &h, 4);
-    std::memcpy(img2 + bb + off, &l, 4);
+  const double bscale = std::ldexp(1.0, B_LOG2);
+  auto put = [&](unsigned char *im, int r, int c, double val) {     // hi | lo
+    const double v = val * bscale;
+    const __half h = __double2half(v);
+    const __half l = __double2half(v - (double)__half2float(h));
+    const uint32_t off = sw128_off16(r, c, S);
+    std::memcpy(im + off, &h, 2);
+    std::memcpy(im + bb + off, &l, 2);
   };
   for (int t = 0; t < nsets; t++) {
-    unsigned char *b1 = img.data() + t * set_bytes, *b2 = b1 + 2 * bb;
+    unsigned char *b1 = img.data() + t * set_bytes;
     const int m = nl_set[t];
-    const int rows2 = renorm ? nth : m;                  // output orders formed by GEMM2
+    const int cols = renorm ? nth : m;                   // output orders formed by GEMM2
     const std::vector<double> &q2 = renorm ? Qx[t] : Q[t];
-    for (int k = 0; k < nth; k++) {
-      for (int l = 0; l < m; l++) put(b1, k, l, Q[t][(size_t)l * nth + k]);   // B1: row k, K = l
-      for (int l = 0; l < rows2; l++) put(b2, l, k, q2[(size_t)l * nth + k]); // B2: row l, K = k
-    }
+    for (int k = 0; k < nth; k++)
+      for (int l = 0; l < cols; l++) put(b1, k, l, q2[(size_t)l * nth + k]);
   }
   // from the device's stream-ordered pool, like the handle's other buffers;
   // a copy from pageable memory has read `img` when it returns

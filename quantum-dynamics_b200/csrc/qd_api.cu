@@ -1224,6 +1224,9 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     lp = b;
   }
   h->d_lpsi = lp;
+  // orders a run does not store (n_l of its block below the batch's) stay zero:
+  // the column passes read them as A entries of their contraction over l
+  CU(cudaMemsetAsync(lp, 0, csz * h->n12 * h->nl * nruns, h->st));
   TRY(h->alloc(h->d_psi_z, npt * nruns));
   for (int r = 0; r < nruns; r++) {
     bool fin = true;

@@ -8,7 +8,7 @@ struct TcPlan {
   int S = 0;                    // max(n_l, n_theta) padded to 16 (MMA N and K)
   int renorm = 0;               // per-column isometry rescaling (orthonormal Q columns)
   int nsets = 0;                // angular bases (one operand image set each)
-  size_t set_bytes = 0;         // bytes of one image set: B1 hi|lo, B2 hi|lo
+  size_t set_bytes = 0;         // bytes of one image set: Q hi|lo (FP16, times 2^12)
   void *mats = nullptr;         // device: the image sets, then an int status word
   size_t mats_bytes = 0;
   int smem_bytes = 0;
