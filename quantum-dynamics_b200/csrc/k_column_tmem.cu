@@ -486,8 +486,15 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     const float ddv = (mode != COL_HEAD && p.d1 && qok) ? (float)(p.d1[i] * p.d2[j]) : 1.f;
     const bool frow = mode != COL_HEAD && p.do_flux && qok && j >= p.surf_j0 &&
                       j < p.surf_j0 + p.surf_nrows;
-    // slow tiles form the scaled theta-space state (EX: frow is uniform per tile)
-    const bool slow = mode == COL_TAIL || !EX || !t.renorm || p.out_z || frow || p.esum;
+    // slow tiles form the true theta-space state: every tile of a launch that
+    // outputs theta values, and the tiles with a point on a flux row (a
+    // whole-tile test, as the branch holds barriers; EX: a tile lies in one row)
+    bool tile_frow = frow;
+    if (!EX && mode != COL_HEAD && p.do_flux) {
+      const int ja = QD_DIV(q0, t.m_n1), jb = QD_DIV(min(q0 + TPTS, n12) - 1, t.m_n1);
+      tile_frow = jb >= p.surf_j0 && ja < p.surf_j0 + p.surf_nrows;
+    }
+    const bool slow = mode == COL_TAIL || !t.renorm || p.out_z || tile_frow || p.esum;
     float n_l = 0.f, sc = 1.f;
     int pe = 0;                                 // the point's scale exponent
     // GEMM1 output (theta values) of this thread; with one CTA per SM (128
@@ -751,7 +758,7 @@ template <int S> cudaError_t set_smem_attr(int bytes)
 {
   cudaError_t e = set_smem_attr_ex<S, false, false>(bytes);
   if (e == cudaSuccess) e = set_smem_attr_ex<S, false, true>(bytes);
-  if constexpr (S == 64) {
+  if constexpr (S == 64 || S == 128) {
     if (e == cudaSuccess) e = set_smem_attr_ex<S, true, false>(bytes);
     if (e == cudaSuccess) e = set_smem_attr_ex<S, true, true>(bytes);
   }
@@ -781,9 +788,9 @@ template <int S>
 void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, const TcDev &t,
                  int mode)
 {
-  const bool ex = S == 64 && p.nl == S && p.nth == S && p.n12 % TPTS == 0 && p.n1 % TPTS == 0;
+  const bool ex = p.nl == S && p.nth == S && p.n12 % TPTS == 0 && p.n1 % TPTS == 0;
   const bool ms = t.run_set || t.run_nl;
-  if constexpr (S == 64) {
+  if constexpr (S == 64 || S == 128) {   // the exact-shape forms built
     if (ex && ms) { launch_mode_ex<S, true, true>(grid, smem, s, p, t, mode); return; }
     if (ex) { launch_mode_ex<S, true, false>(grid, smem, s, p, t, mode); return; }
   }

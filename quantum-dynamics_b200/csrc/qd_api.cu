@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -23,6 +25,7 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <unistd.h>
 #include "qd.h"
 #include "qd_kernels.h"
 #include "qd_tc.h"
@@ -100,11 +103,78 @@ void radial_tables(const qd_radial &c, std::vector<double> &T, std::vector<doubl
   for (int i = 0; i < n; i++) I[i] = 1.0 / (m2 * c.r[i] * c.r[i]);
 }
 
+// Host worker threads for the input checks and the staging copies: created
+// once per process (up to 16, the calling thread included) and reused, so a
+// 32 MiB chunk costs no thread creation.  run(fn) calls fn(t) for every
+// worker t and returns when all are done; callers take turns.  In a process
+// forked after the pool was made (its workers do not exist there) the calling
+// thread does every part itself.
+class HostPool {
+ public:
+  static HostPool &get()
+  {
+    static HostPool *p = new HostPool();   // never destroyed: workers may outlive exit
+    return *p;
+  }
+  unsigned size() const { return (unsigned)th_.size() + 1; }
+  template <typename F> void run(const F &fn)
+  {
+    std::lock_guard<std::mutex> turn(run_mu_);
+    if (th_.empty() || getpid() != pid_) {
+      for (unsigned t = 0; t < size(); t++) fn(t);
+      return;
+    }
+    const std::function<void(unsigned)> job = fn;
+    {
+      std::lock_guard<std::mutex> l(m_);
+      job_ = &job;
+      pending_ = th_.size();
+      gen_++;
+    }
+    cv_.notify_all();
+    fn(0);
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  HostPool() : pid_(getpid())
+  {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned n = std::max(1u, std::min(16u, hw ? hw : 1u));
+    for (unsigned t = 1; t < n; t++) th_.emplace_back([this, t] { loop(t); });
+  }
+  void loop(unsigned t)
+  {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(unsigned)> *f;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return gen_ != seen; });
+        seen = gen_;
+        f = job_;
+      }
+      (*f)(t);
+      std::lock_guard<std::mutex> l(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  pid_t pid_;
+  std::mutex run_mu_, m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(unsigned)> *job_ = nullptr;
+  uint64_t gen_ = 0;
+  size_t pending_ = 0;
+};
+
 // Inf and NaN are the doubles whose exponent field is all ones.  The scan
 // ORs that test over the words without an early exit (so it stays a stream
 // of independent loads), and splits arrays of a million or more words over
-// up to eight host threads: the check reads the whole input once per call
-// and is bound by host memory bandwidth.
+// the host pool: the check reads the whole input once per call and is bound
+// by host memory bandwidth.
 bool finite_words(const double *a, size_t n)
 {
   constexpr uint64_t E = 0x7ff0000000000000ull;
@@ -129,17 +199,14 @@ bool finite_words(const double *a, size_t n)
 bool all_finite(const double *a, size_t n)
 {
   if (n < (size_t(1) << 20)) return finite_words(a, n);
-  const unsigned hw = std::thread::hardware_concurrency();
-  const unsigned nt = std::max(1u, std::min(8u, hw));
+  HostPool &pool = HostPool::get();
+  const unsigned nt = pool.size();
   const size_t chunk = (n + nt - 1) / nt;
   std::vector<char> ok(nt, 1);
-  std::vector<std::thread> th;
-  for (unsigned t = 1; t < nt; t++) {
-    const size_t b = t * chunk, e = std::min(n, b + chunk);
-    if (b < e) th.emplace_back([&ok, a, b, e, t] { ok[t] = finite_words(a + b, e - b); });
-  }
-  ok[0] = finite_words(a, std::min(n, chunk));
-  for (std::thread &x : th) x.join();
+  pool.run([&](unsigned t) {
+    const size_t b = std::min(n, t * chunk), e = std::min(n, b + chunk);
+    if (b < e) ok[t] = finite_words(a + b, e - b);
+  });
   return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
 }
 
@@ -171,7 +238,8 @@ class Staging {
  public:
   static constexpr size_t CHUNK = size_t(32) << 20;   // bytes per staging buffer
   static constexpr int NBUF = 4;
-  static constexpr size_t LARGE = size_t(64) << 20;   // transfers from this size on use it
+  static constexpr size_t LARGE = size_t(4) << 20;    // transfers from this size on use it
+  static constexpr size_t CHECK_STAGED = size_t(64) << 20;   // inputs checked while staged
 
   static Staging &get()
   {
@@ -254,26 +322,22 @@ class Staging {
     if (!ok_) cudaGetLastError();
     return ok_;
   }
-  // memcpy over up to eight threads; with scan, also the NaN/Inf test of the
+  // memcpy over the host pool; with scan, also the NaN/Inf test of the
   // copied words
   static bool copy_scan(void *dst, const void *src, size_t n, bool scan)
   {
-    const unsigned hw = std::thread::hardware_concurrency();
-    const unsigned nt = std::max(1u, std::min(8u, hw));
+    HostPool &pool = HostPool::get();
+    const unsigned nt = pool.size();
     const size_t part = (n / nt + 63) & ~size_t(63);
     std::vector<char> ok(nt, 1);
-    std::vector<std::thread> th;
-    auto work = [&](unsigned t) {
-      const size_t a = std::min(n, t * part), z = std::min(n, a + part);
+    pool.run([&](unsigned t) {
+      const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
       if (a >= z) return;
       std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, z - a);
       if (scan)
         ok[t] = finite_words(reinterpret_cast<const double *>(static_cast<const char *>(dst) + a),
                              (z - a) / 8);
-    };
-    for (unsigned t = 1; t < nt; t++) th.emplace_back(work, t);
-    work(0);
-    for (std::thread &x : th) x.join();
+    });
     return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
   }
   std::mutex mu_;
@@ -450,11 +514,11 @@ int validate(const qd_data *d)
     return set_err(QD_ERR_INVALID, "centrifugal-sudden block J = %d, K = %d: need 0 <= K <= J",
                    d->cs.J, d->cs.K);
   const size_t npt = (size_t)n1 * n2 * nth;
-  // arrays of Staging::LARGE bytes or more are checked while they are staged
+  // arrays of Staging::CHECK_STAGED bytes or more are checked while they are staged
   // for the upload (create), smaller ones here
-  if (npt * sizeof(double) < Staging::LARGE && !all_finite(d->pot, npt))
+  if (npt * sizeof(double) < Staging::CHECK_STAGED && !all_finite(d->pot, npt))
     return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
-  if (2 * npt * sizeof(double) < Staging::LARGE && !all_finite(d->psi, 2 * npt))
+  if (2 * npt * sizeof(double) < Staging::CHECK_STAGED && !all_finite(d->psi, 2 * npt))
     return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
   if (d->CRP.calculate_CRP) {
     const qd_crp &c = d->CRP;
@@ -1129,7 +1193,8 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   TRY(h->alloc(h->d_pot, npt * npot));
   for (int r = 0; r < npot; r++) {
     bool fin = true;
-    CU(Staging::get().upload(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt, h->st, &fin));
+    CU(Staging::get().upload(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt, h->st,
+                             sizeof(double) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
     if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: pot contains NaN/Inf", r);
   }
   TRY(upload(h, h->d_w, d->theta.w, h->nth));
@@ -1231,7 +1296,7 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   for (int r = 0; r < nruns; r++) {
     bool fin = true;
     CU(Staging::get().upload(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt, h->st,
-                             &fin));
+                             sizeof(double2) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
     if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
   }
   if (h->do_crp) {
