@@ -246,7 +246,9 @@ class Staging {
     static Staging s;
     return s;
   }
-  // host -> device; *finite (if given) = no word of src is NaN/Inf
+  // host -> device; *finite (if given) = no word of src is NaN/Inf.  The
+  // staging buffers are taken in turn across calls, so the host copy of one
+  // call's first chunk overlaps the transfer of the previous call's last.
   cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t st, bool *finite)
   {
     if (finite) *finite = true;
@@ -256,8 +258,8 @@ class Staging {
       return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
     }
     bool ok_all = true;
-    for (size_t off = 0, c = 0; off < bytes; off += CHUNK, c++) {
-      const int b = (int)(c % NBUF);
+    for (size_t off = 0; off < bytes; off += CHUNK) {
+      const int b = (int)(next_++ % NBUF);
       cudaError_t e = cudaEventSynchronize(ev_[b]);     // the buffer's last transfer is done
       if (e != cudaSuccess) return e;
       const size_t n = std::min(CHUNK, bytes - off);
@@ -270,22 +272,52 @@ class Staging {
     if (finite) *finite = ok_all;
     return cudaSuccess;
   }
-  // device -> host; returns once dst holds the data
+  // device -> host of one array; returns once dst holds the data
   cudaError_t download(void *dst, const void *src, size_t bytes, cudaStream_t st)
   {
+    const Piece one{dst, src, bytes};
+    return download(&one, 1, st);
+  }
+  // device -> host of several arrays as one stream of chunks (a chunk may
+  // span the end of one array and the start of the next), so the transfers
+  // of a batch of small arrays overlap the host copies as well
+  struct Piece {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  };
+  cudaError_t download(const Piece *pc, int np, cudaStream_t st)
+  {
     std::lock_guard<std::mutex> lock(mu_);
-    if (bytes < LARGE || !ready()) {
-      cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
-      return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+    size_t total = 0;
+    for (int i = 0; i < np; i++) total += pc[i].bytes;
+    if (!ready() || (np == 1 && total < LARGE)) {
+      for (int i = 0; i < np; i++) {
+        cudaError_t e = cudaMemcpyAsync(pc[i].dst, pc[i].src, pc[i].bytes, cudaMemcpyDeviceToHost,
+                                        st);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaStreamSynchronize(st);
     }
-    const size_t nch = (bytes + CHUNK - 1) / CHUNK;
+    const size_t nch = (total + CHUNK - 1) / CHUNK;
+    // chunk c covers bytes [c*CHUNK, ...) of the concatenation; walk the pieces
+    auto each_part = [&](size_t c, auto &&fn) {
+      const size_t lo = c * CHUNK, hi = std::min(total, lo + CHUNK);
+      size_t base = 0;
+      for (int i = 0; i < np && base < hi; base += pc[i].bytes, i++) {
+        const size_t a = std::max(lo, base), z = std::min(hi, base + pc[i].bytes);
+        if (a < z) fn(i, a - base, a - lo, z - a);   // piece, offset in piece, in chunk, bytes
+      }
+    };
     auto issue = [&](size_t c) -> cudaError_t {
       const int b = (int)(c % NBUF);
-      const size_t off = c * CHUNK, n = std::min(CHUNK, bytes - off);
       cudaError_t e = cudaEventSynchronize(ev_[b]);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(buf_[b], static_cast<const char *>(src) + off, n,
-                            cudaMemcpyDeviceToHost, st);
+      each_part(c, [&](int i, size_t po, size_t co, size_t n) {
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(static_cast<char *>(buf_[b]) + co,
+                              static_cast<const char *>(pc[i].src) + po, n,
+                              cudaMemcpyDeviceToHost, st);
+      });
       if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
       return e;
     };
@@ -297,13 +329,16 @@ class Staging {
       const int b = (int)(c % NBUF);
       cudaError_t e = cudaEventSynchronize(ev_[b]);
       if (e != cudaSuccess) return e;
-      const size_t off = c * CHUNK, n = std::min(CHUNK, bytes - off);
-      copy_scan(static_cast<char *>(dst) + off, buf_[b], n, false);
+      each_part(c, [&](int i, size_t po, size_t co, size_t n) {
+        copy_scan(static_cast<char *>(pc[i].dst) + po, static_cast<const char *>(buf_[b]) + co, n,
+                  false);
+      });
       if (c + NBUF - 1 < nch) {
         e = issue(c + NBUF - 1);
         if (e != cudaSuccess) return e;
       }
     }
+    next_ = 0;   // every buffer's event has completed
     return cudaSuccess;
   }
 
@@ -344,6 +379,7 @@ class Staging {
   bool tried_ = false, ok_ = false;
   void *buf_[NBUF] = {};
   cudaEvent_t ev_[NBUF] = {};
+  size_t next_ = 0;               // the upload's next staging buffer (round robin)
 };
 
 }  // namespace
@@ -1627,11 +1663,22 @@ int qd_download(qd_handle *h)
 {
   if (!h) return set_err(QD_ERR_INVALID, "handle is NULL");
   DevGuard g(h->dev);
+  // every run's psi and P(E) in one pipelined transfer
+  TRY(stage_psi(h));
+  const bool crp = h->do_crp && h->started;
+  if (crp) TRY(compute_crp(h));
+  const long npt = h->n12 * h->nth;
+  std::vector<Staging::Piece> pcs;
   for (int r = 0; r < h->nruns; r++) {
-    TRY(get_psi(h, r, h->runs[r]->psi));
-    if (h->do_crp && h->started) TRY(get_crp(h, r, h->runs[r]->CRP.CRP));
-    h->runs[r]->time.steps = h->steps;
+    pcs.push_back({h->runs[r]->psi, h->d_psi_z + (long)r * npt, sizeof(double2) * npt});
+    if (crp)
+      pcs.push_back({h->runs[r]->CRP.CRP, h->d_crp + (long)r * h->ne, sizeof(double) * h->ne});
   }
+  CU(Staging::get().download(pcs.data(), (int)pcs.size(), h->st));
+  if (h->do_crp && !h->started)
+    for (int r = 0; r < h->nruns; r++)
+      for (int e = 0; e < h->ne; e++) h->runs[r]->CRP.CRP[e] = 0.0;
+  for (int r = 0; r < h->nruns; r++) h->runs[r]->time.steps = h->steps;
   return QD_OK;
 }
 
