@@ -28,13 +28,12 @@
 // image pair (hi | lo) in shared memory, the accumulator in TMEM.  One image
 // serves both GEMMs: stored with rows k and 64 orders l per 128-byte swizzled
 // row, it is the K-major operand of GEMM1 and the MN-major operand of GEMM2.
-// Each tile issues the next tile's GEMM1 as soon as its own GEMM2 output is
-// in registers, and right after that the loads of the tile after next: its
-// psi_l values into registers and its exp(-i V dt) values into the second of
-// two shared-memory buffers (asynchronous copies), so both have a whole tile
-// to arrive.  512 threads per CTA.  S <= 64: two CTAs per SM overlap each
-// other's load / MMA / epilogue phases; S = 96, 128 (n_theta up to 128): one
-// CTA per SM.
+// The tile's exp(-i V dt) values are staged into shared memory by
+// asynchronous copies issued while the previous tile finishes.  512 threads
+// per CTA.  S <= 64: two CTAs per SM overlap each other's load / MMA /
+// epilogue phases; S = 96, 128 (n_theta up to 128): one CTA per SM, which
+// issues the next tile's GEMM1 as soon as the current tile's GEMM2 output is
+// in registers.
 //
 // Norm of each grid column.  The tensor-core FP32 accumulation rounds toward
 // smaller magnitudes (measured ~1e-7 per GEMM), which compounded over 1e4
@@ -344,8 +343,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   float *xch = reinterpret_cast<float *>(mbar + 4 + 32);  // [4 exchanges][NG][TPTS]
   float *sw = xch + 4 * NG * TPTS;                        // [S] sqrt(w_k), 0 beyond n_theta
   float *rsw = sw + S;                                    // [S] 1/sqrt(w_k)
-  // [2][S][TPTS] exp(-i V dt) of a tile: two buffers (MID), tile i uses buffer i % 2
-  float2 *evs = reinterpret_cast<float2 *>(rsw + S);
+  float2 *evs = reinterpret_cast<float2 *>(rsw + S);      // [S][TPTS] exp(-i V dt) of a tile
 
   pdl_trigger();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -421,10 +419,9 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       else a[u] = (ok && c0 + u < nl) ? src[u * stride] : 0.f;                       \
     }                                                                                \
   } while (0)
-  // exp(-i V dt) of tile tl into evs buffer bf, 16-byte asynchronous copies
-  // (zero-filled past n_theta and past the grid; n12 is even, so a copy never
-  // straddles it)
-#define QD_STAGE_EV(tl, bf)                                                          \
+  // exp(-i V dt) of tile tl into evs, 16-byte asynchronous copies (zero-filled
+  // past n_theta and past the grid; n12 is even, so a copy never straddles it)
+#define QD_STAGE_EV(tl)                                                              \
   do {                                                                               \
     if ((tl) < tend) {                                                               \
       const int rr = QD_RUN_OF(tl), qb = ((tl) - QD_DIV(tl, t.m_tpr) * tpr) * TPTS; \
@@ -432,12 +429,12 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       for (int x = tid; x < S * (TPTS / 2); x += NTHREADS) {                         \
         const int k = x / (TPTS / 2), c2 = 2 * (x % (TPTS / 2));                     \
         const bool okv = EX || (k < nth && qb + c2 < n12);                           \
-        cp16_zfill(&evs[(bf) * S * TPTS + k * TPTS + c2], okv ? eb + (size_t)k * n12 + c2 : expv, okv); \
+        cp16_zfill(&evs[k * TPTS + c2], okv ? eb + (size_t)k * n12 + c2 : expv, okv); \
       }                                                                              \
     }                                                                                \
     asm volatile("cp.async.commit_group;" ::: "memory");                             \
   } while (0)
-  if (mode == COL_MID) QD_STAGE_EV(tbeg, 0);   // exp(-iVdt): set up before this launch
+  if (mode == COL_MID) QD_STAGE_EV(tbeg);      // exp(-iVdt): set up before this launch
   pdl_wait();                                   // psi_l, psi_z, flux rows: the previous grid's
   if (mode != COL_HEAD) QD_PREFETCH_A(tbeg);
   // the prologue's loads (images, exp(-iVdt), psi_l, weights) are all in
@@ -464,7 +461,6 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   // end of the previous tile, as soon as that tile's GEMM2 output was in
   // registers, so that GEMM1 runs under the previous tile's stores
   bool a_ready = false;
-  int par = 0;                                  // this tile's exp(-iVdt) buffer
   float n_l_next = 0.f;                         // l-space point norm of that next tile
 
   for (int tile = tbeg; tile < tend && !failed; tile += gridDim.x) {
@@ -504,10 +500,6 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     // GEMM1 output (theta values) of this thread; with one CTA per SM (128
     // registers) a slow tile keeps its first TMEM read for the theta-space work
     constexpr bool KEEP = ctas_per_sm(S) == 1;
-    // one CTA per SM: the psi_l values of the tile after next are loaded a
-    // whole tile ahead (with two CTAs per SM the other CTA covers the latency
-    // of loading them during GEMM2, and the registers are fewer)
-    constexpr bool EARLY = ctas_per_sm(S) == 1;
     float dv[H];
 
     if (mode != COL_HEAD) {
@@ -531,10 +523,6 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
           tc_fence_after();
           gemm_split_ts<S, false>(D, Ahi, Alo, bq);
           mma_commit(mb1);
-        }
-        if (mode == COL_MID) {                  // the next tile's loads (a is free)
-          if (EARLY) QD_PREFETCH_A(tile + (int)gridDim.x);
-          QD_STAGE_EV(tile + (int)gridDim.x, par ^ 1);
         }
       } else {
         n_l = n_l_next;
@@ -601,7 +589,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
 #pragma unroll
       for (int u = 0; u < H; u++) {
         const float other = __shfl_xor_sync(0xffffffffu, dv[u], 1);
-        const float2 e = evs[par * S * TPTS + (c0 + u) * TPTS + pt];
+        const float2 e = evs[(c0 + u) * TPTS + pt];
         dv[u] = fmaf(other * ysg, e.y, dv[u] * e.x);
       }
       put_row<H>(my_hi, my_lo, dv, slow ? exp2i(A_LOG2 - pe) : exp2i(-B_LOG2));
@@ -660,6 +648,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       QD_PREFETCH_A(tile + (int)gridDim.x);
       continue;
     }
+    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
 
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
@@ -667,7 +656,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       gemm_split_ts<S, true>(D, Ahi, Alo, bq);
       mma_commit(mb2);
     }
-    if (mode == COL_MID && !EARLY) QD_PREFETCH_A(tile + (int)gridDim.x);   // during GEMM2
+    if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
     tc_fence_after();
@@ -719,13 +708,8 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         gemm_split_ts<S, false>(D, Ahi, Alo, bq);
         mma_commit(mb1);
       }
-      // a and this tile's exp(-iVdt) buffer are free: the loads of the tile
-      // after next fly during the next tile
-      if (EARLY) QD_PREFETCH_A(nxt + (int)gridDim.x);
-      QD_STAGE_EV(nxt + (int)gridDim.x, par);
     }
     a_ready = ahead;
-    par ^= 1;
     float so;
     if (t.renorm) so = n_o > 0.f ? sqrtf(target / n_o) : 1.f;
     else so = ((slow || mode == COL_HEAD) ? 1.f : ddv) * exp2i(pe - A_LOG2 - B_LOG2);
@@ -817,7 +801,7 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 template <int S> constexpr int smem_bytes_for()
 {
   return 1024 + 2 * image_bytes(S) + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
-         2 * S * TPTS * 8;   // Q image pair, barriers, exchanges, sqrt(w), 1/sqrt(w), 2 x exp(-iVdt)
+         S * TPTS * 8;   // Q image pair, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
 static_assert(smem_bytes_for<128>() <= 227 * 1024 && 2 * smem_bytes_for<64>() <= 227 * 1024,
               "shared memory of the column tiles");

@@ -13,6 +13,38 @@ __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(
 
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// complex64 sums and real scalings as one paired FP32 instruction (sm_100:
+// add/sub/mul/fma on .f32x2, both halves rounded to nearest like the scalar
+// forms), the real and imaginary parts in one 64-bit register pair
+__device__ __forceinline__ float2 cadd(float2 a, float2 b)
+{
+  float2 r;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b)
+{
+  float2 r;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+// (a.x hi + a.x lo, a.y hi + a.y lo), the compensated real scaling below
+__device__ __forceinline__ float2 cscale2_f32x2(float2 a, float hi, float lo)
+{
+  float2 r;
+  asm("{\n\t.reg .b64 ra, rh, rl, rt, rd;\n\tmov.b64 ra, {%2, %3};\n\t"
+      "mov.b64 rh, {%4, %4};\n\tmov.b64 rl, {%5, %5};\n\t"
+      "mul.rn.f32x2 rt, ra, rl;\n\tfma.rn.f32x2 rd, ra, rh, rt;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(hi), "f"(lo));
+  return r;
+}
+#define QD_F32X2 1
+#endif
 template <typename C> __device__ __forceinline__ C cmul(C a, C b)
 { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 template <typename C> __device__ __forceinline__ C cconj(C a) { return mk(a.x, -a.y); }
@@ -78,6 +110,9 @@ template <> struct Konst<double> {
 };
 template <typename C, typename R> __device__ __forceinline__ C cscale2(C a, R hi, R lo)
 { return mk(fma(a.x, hi, a.x * lo), fma(a.y, hi, a.y * lo)); }
+#ifdef QD_F32X2
+__device__ __forceinline__ float2 cscale2(float2 a, float hi, float lo) { return cscale2_f32x2(a, hi, lo); }
+#endif
 
 template <typename C> struct SmallDFT<8, C> {
   static __device__ __forceinline__ void run(C *v, int sgn, const C *, int)
