@@ -107,6 +107,26 @@ template <int A> __device__ __forceinline__ float kcos(float x)
   return ksign(A) < 0 ? -v : v;
 }
 
+#ifdef QD_F32X2
+// z * |cos(2 pi A / 96)| for both parts of z (the sign is the caller's)
+template <int CODE> __device__ __forceinline__ float2 kmag2(float2 z)
+{
+  if constexpr (CODE == 1) return z;
+  else if constexpr (CODE == 2) return make_float2(0.5f * z.x, 0.5f * z.y);
+  else if constexpr (CODE == 3) return cscale2_f32x2(z, 7.07106769e-01f, 1.21016175e-08f);
+  else if constexpr (CODE == 4) return cscale2_f32x2(z, 8.66025388e-01f, 1.55436251e-08f);
+  else if constexpr (CODE == 5) return cscale2_f32x2(z, 9.23879504e-01f, 2.83074897e-08f);
+  else if constexpr (CODE == 6) return cscale2_f32x2(z, 3.82683426e-01f, 6.22335072e-09f);
+  else if constexpr (CODE == 7) return cscale2_f32x2(z, 9.80785251e-01f, 2.97394731e-08f);
+  else if constexpr (CODE == 8) return cscale2_f32x2(z, 8.31469595e-01f, 1.68702634e-08f);
+  else if constexpr (CODE == 9) return cscale2_f32x2(z, 5.55570245e-01f, -1.17695214e-08f);
+  else if constexpr (CODE == 10) return cscale2_f32x2(z, 1.95090324e-01f, -1.67047143e-09f);
+  else if constexpr (CODE == 11) return cscale2_f32x2(z, 9.65925813e-01f, 1.35678162e-08f);
+  else if constexpr (CODE == 12) return cscale2_f32x2(z, 2.58819044e-01f, 1.46619872e-09f);
+  else return make_float2(0.f, 0.f);
+}
+#endif
+
 template <int N, int E, int SGN> __device__ __forceinline__ float2 twk(float2 z)
 {
   static_assert(96 % N == 0, "N must divide 96");
@@ -123,8 +143,17 @@ template <int N, int E, int SGN> __device__ __forceinline__ float2 twk(float2 z)
       re = SGN > 0 ? -kcos<as>(z.y) : kcos<as>(z.y);
       im = SGN > 0 ? kcos<as>(z.x) : -kcos<as>(z.x);
     } else {
+#ifdef QD_F32X2
+      // (c x, c y) and (s x, s y) as paired products, then the cross sums
+      const float2 C = kmag2<kcode(a)>(z), Sn = kmag2<kcode(as)>(z);
+      const float cx = ksign(a) < 0 ? -C.x : C.x, cy = ksign(a) < 0 ? -C.y : C.y;
+      const float sx = ksign(as) < 0 ? -Sn.x : Sn.x, sy = ksign(as) < 0 ? -Sn.y : Sn.y;
+      re = SGN > 0 ? cx - sy : cx + sy;
+      im = SGN > 0 ? sx + cy : cy - sx;
+#else
       re = SGN > 0 ? kcos<a>(z.x) - kcos<as>(z.y) : kcos<a>(z.x) + kcos<as>(z.y);
       im = SGN > 0 ? kcos<as>(z.x) + kcos<a>(z.y) : kcos<a>(z.y) - kcos<as>(z.x);
+#endif
     }
     return make_float2(re, im);
   }
