@@ -63,7 +63,9 @@ namespace {
 
 constexpr int TPTS = 64;          // complex grid points per tile
 constexpr int MROWS = 128;        // GEMM rows per tile
-constexpr int NTHREADS = 512;
+// threads per CTA (a multiple of 128: NG column groups of four warps).  1024
+// threads at S = 128 (64 registers, 16 columns per thread) measured 33 % slower.
+__host__ __device__ constexpr int nthreads(int) { return 512; }
 constexpr int MAXS = 128;         // max padded n_l / n_theta handled here
 constexpr int B_LOG2 = 12;        // Q is stored times 2^12
 constexpr int A_LOG2 = 13;        // scaled A entries are at most 2^13
@@ -283,9 +285,13 @@ __device__ __forceinline__ void mma_f16_ts(uint32_t dtmem, uint32_t atmem, uint6
 // (packed FP16 pairs), B the image pair at b (hi | lo, image_bytes(S) apart):
 // GEMM1 (MN = false) reads it K-major, GEMM2 (MN = true) MN-major.  The small
 // split terms first, the main one last.
+// desc0: the descriptor of the hi image at its first K slice (make_desc_k or
+// make_desc_mn of its address); the others differ only in the start-address
+// field (address / 16, 14 bits: shared-memory offsets stay below 256 KB, so
+// adding to it never carries out)
 template <int S, bool MN>
 __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint32_t alo,
-                                              uint32_t b)
+                                              uint64_t desc0)
 {
   constexpr uint32_t idesc = make_idesc(S, MN);
   constexpr int BB = image_bytes(S);
@@ -293,18 +299,18 @@ __device__ __forceinline__ void gemm_split_ts(uint32_t dtmem, uint32_t ahi, uint
   for (int term = 0; term < 3; term++) {
     // term 0: Ahi*Blo, 1: Alo*Bhi, 2: Ahi*Bhi
     const uint32_t a = term == 1 ? alo : ahi;
-    const uint32_t bt = b + (term == 0 ? BB : 0);
+    const uint64_t dt = desc0 + (term == 0 ? (uint64_t)(BB >> 4) : 0ull);
 #pragma unroll
     for (int kk = 0; kk < S; kk += 16) {
-      uint64_t desc;
-      if constexpr (MN) desc = make_desc_mn(bt + (uint32_t)kk * 128u, (uint32_t)S * 128u);
-      else desc = make_desc_k(bt + (uint32_t)((kk >> 6) * S * 128 + ((kk & 63) >> 4) * 32));
-      mma_f16_ts(dtmem, a + kk / 2, desc, idesc, (term | kk) ? 1u : 0u);
+      const uint32_t off = MN ? (uint32_t)kk * 128u
+                              : (uint32_t)((kk >> 6) * S * 128 + ((kk & 63) >> 4) * 32);
+      mma_f16_ts(dtmem, a + kk / 2, dt + (off >> 4), idesc, (term | kk) ? 1u : 0u);
     }
   }
 }
 
-constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share a TMEM lane quarter)
+// column groups (warps w, w+4, ... share a TMEM lane quarter)
+__host__ __device__ constexpr int ngroups(int S) { return nthreads(S) / 128; }
 
 // EX: exact shape -- n_l = n_theta = S, n12 and n1 multiples of the tile, so
 // every point and column of a tile is valid and a tile lies in one grid row j.
@@ -326,8 +332,9 @@ constexpr int NG = NTHREADS / 128;     // column groups (warps w, w+4, ... share
 // to a known norm above are scale-free.
 // MS: runs of the batch have different angular bases (image sets, orders stored)
 template <int S, int MODE, bool EX, bool MS>
-__global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnParams p, TcDev t)
+__global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(ColumnParams p, TcDev t)
 {
+  constexpr int NTHREADS = nthreads(S), NG = ngroups(S);
   constexpr int mode = MODE;
   constexpr int H = S / NG;                    // K columns per thread (one group)
   constexpr int BB = image_bytes(S);
@@ -420,7 +427,9 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
     }                                                                                \
   } while (0)
   // exp(-i V dt) of tile tl into evs, 16-byte asynchronous copies (zero-filled
-  // past n_theta and past the grid; n12 is even, so a copy never straddles it)
+  // past n_theta and past the grid; n12 is even, so a copy never straddles it).
+  // (One bulk copy per theta row, issued by one warp and waited on through an
+  // mbarrier by every thread, measured 25 % slower on the C4 column pass.)
 #define QD_STAGE_EV(tl)                                                              \
   do {                                                                               \
     if ((tl) < tend) {                                                               \
@@ -453,6 +462,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
   const uint32_t my_d = D + lane_base + c0;
   const uint32_t mb1 = smem_u32(&mbar[0]), mb2 = smem_u32(&mbar[1]);
   const uint32_t bq = smem_u32(Bq);
+  const uint64_t dk0 = make_desc_k(bq), dmn0 = make_desc_mn(bq, (uint32_t)S * 128u);
   uint32_t ph1 = 0, ph2 = 0, ph3 = 1;
   // every thread observes each mbarrier completion itself before it reads
   // what the asynchronous operation wrote
@@ -521,7 +531,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
         __syncthreads();
         if (tid == 0) {
           tc_fence_after();
-          gemm_split_ts<S, false>(D, Ahi, Alo, bq);
+          gemm_split_ts<S, false>(D, Ahi, Alo, dk0);
           mma_commit(mb1);
         }
       } else {
@@ -648,14 +658,13 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       QD_PREFETCH_A(tile + (int)gridDim.x);
       continue;
     }
-    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
-
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
       tc_fence_after();
-      gemm_split_ts<S, true>(D, Ahi, Alo, bq);
+      gemm_split_ts<S, true>(D, Ahi, Alo, dmn0);
       mma_commit(mb2);
     }
+    if (mode == COL_MID) QD_STAGE_EV(tile + (int)gridDim.x);   // evs is free again
     if (mode != COL_HEAD) QD_PREFETCH_A(tile + (int)gridDim.x);   // next tile's loads fly during GEMM2
     if (__syncthreads_or(!mbar_wait(mb2, ph2))) { failed = true; break; }
     ph2 ^= 1;
@@ -688,8 +697,8 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       for (int u = 0; u < H; u++) nl_part = fmaf(a[u], a[u], nl_part);
       nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
       if (!is_im) xch[grp * TPTS + pt] = nl_part;
-      asm volatile("cp.async.wait_group 0;" ::: "memory");   // the next tile's evs
     }
+    if (ahead) asm volatile("cp.async.wait_group 0;" ::: "memory");   // the next tile's evs
     tc_fence_before();
     __syncthreads();
     float n_o = 0.f;
@@ -705,7 +714,7 @@ __global__ void __launch_bounds__(NTHREADS, ctas_per_sm(S)) k_column_tc(ColumnPa
       __syncthreads();
       if (tid == 0) {
         tc_fence_after();
-        gemm_split_ts<S, false>(D, Ahi, Alo, bq);
+        gemm_split_ts<S, false>(D, Ahi, Alo, dk0);
         mma_commit(mb1);
       }
     }
@@ -771,7 +780,7 @@ void launch_mode_ex(int grid, int smem, cudaStream_t s, const ColumnParams &p, c
 {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(NTHREADS);
+  cfg.blockDim = dim3(nthreads(S));
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -800,7 +809,7 @@ void launch_mode(int grid, int smem, cudaStream_t s, const ColumnParams &p, cons
 
 template <int S> constexpr int smem_bytes_for()
 {
-  return 1024 + 2 * image_bytes(S) + 4 * 8 + 32 * 8 + 4 * NG * TPTS * 4 + 2 * S * 4 +
+  return 1024 + 2 * image_bytes(S) + 4 * 8 + 32 * 8 + 4 * ngroups(S) * TPTS * 4 + 2 * S * 4 +
          S * TPTS * 8;   // Q image pair, barriers, exchanges, sqrt(w), 1/sqrt(w), exp(-iVdt)
 }
 static_assert(smem_bytes_for<128>() <= 227 * 1024 && 2 * smem_bytes_for<64>() <= 227 * 1024,
