@@ -241,7 +241,7 @@ template <int N1, int N2, int NT, int CL, int A1X = 0> struct RfShape {
   static constexpr bool SWAP = CL == 4;
   static constexpr int PSLOTS = CL == 1 || SWAP ? 0 : CL - 1;
   static constexpr int P1_UNROLL = 2;                // row items per thread loaded together
-  static constexpr int SWAP_ROUNDS = 4;              // row rounds of the in-place transpose
+  static constexpr int SWAP_ROUNDS = 6;              // row rounds of the in-place transpose (1, 2, 4, 6, 8, 12 measured: 6 best)
   // own rows [HR][RS]; CL = 2: the peer's rows of this CTA's column part
   // [HR][HW]; rc1[l], kc1 (N1 each), W_N2, kc2, rc2[l] (N2 each); CL = 2:
   // one mbarrier
