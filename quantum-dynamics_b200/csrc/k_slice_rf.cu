@@ -333,7 +333,23 @@ __device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
         v[k] = R4[(j * RS + HW * peer) / 2 + x];
       }
     }
-    cluster_arrive_release();                        // every CTA has read this round's rows
+    // every CTA has read this round's rows before any is overwritten.  Round 0
+    // also publishes the row passes' writes (release); later rounds only need
+    // this thread's loads to have returned, which a store of a value computed
+    // from all of them, ahead of a relaxed arrive, guarantees (their rows were
+    // published by round 0, and the stores of round r - 1 touch other rows)
+    if (r == 0) {
+      cluster_arrive_release();
+    } else {
+      uint32_t dep = 0;
+#pragma unroll
+      for (int k = 0; k < F; k++)
+        dep |= __float_as_uint(v[k].x) | __float_as_uint(v[k].y) | __float_as_uint(v[k].z) |
+               __float_as_uint(v[k].w);
+      __shared__ uint32_t sink;                      // a store that reads every loaded value
+      asm volatile("st.shared.u32 [%0], %1;\n\tbarrier.cluster.arrive.relaxed.aligned;"
+                   :: "r"(smem_addr(&sink)), "r"(dep) : "memory");
+    }
     cluster_wait();
 #pragma unroll
     for (int k = 0; k < F; k++) {
