@@ -51,7 +51,7 @@ FLUSH_BYTES = 256 << 20
 EXTRA = {}
 
 
-def surrogate_c1(precision, n_train=200000, steps=60000, seed=12345):
+def surrogate_c1(precision, n_train=400000, steps=240000, seed=12345, e_cut_ev=70.0):
     """C1 with the potential replaced by the MLP surrogate: training on the GPU,
     the judge's |dV| on the grid, and |dP(E)| of two full 10000-step complex64
     propagations (plain LEPS vs surrogate)."""
@@ -62,7 +62,10 @@ def surrogate_c1(precision, n_train=200000, steps=60000, seed=12345):
     m_amu = np.array([18.9984, 1.00783, 1.00783]) * S.AMU_ME
     pes = S.leps_f_h2()
     R, r, x = data.r1.r, data.r2.r, data.theta.x
-    r12, r23, r13, V = training_set(pes, m_amu, n=n_train, seed=seed)
+    # trained over the whole capped range of the grid (2.5 hartree = 68 eV): the
+    # packet's tails in the repulsive walls move P(E) (|dP| 0.015 with a 3 eV
+    # training range, 0.0075 with 8 eV, 0.0047 with 70 eV, same network)
+    r12, r23, r13, V = training_set(pes, m_amu, n=n_train, seed=seed, e_cut_ev=e_cut_ev)
     sur = Surrogate(seed=seed)
     t0 = time.perf_counter()
     loss = sur.fit(r12, r23, r13, V, steps=steps, lr=2e-3, lr_end=1e-6)
@@ -89,6 +92,7 @@ def surrogate_c1(precision, n_train=200000, steps=60000, seed=12345):
     out = S.copy_case(data)
     out.pot = np.ascontiguousarray(pot)
     info = {"n_train": int(r12.size), "adam_steps": steps, "batch": 4096,
+            "training_range_eV": e_cut_ev,
             "train_seconds": t_train, "final_loss_std_units": loss,
             "dV_rms_meV": rms * S.HARTREE_EV * 1e3, "dV_max_meV": mx * S.HARTREE_EV * 1e3,
             "dV_region": "grid points where the plain LEPS is below 3 eV",

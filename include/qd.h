@@ -293,8 +293,8 @@ int qd_legendre_matrix(int32_t n, int32_t m, const double *x, double *legendre);
  * in the reference, which evaluates its PES (Fortran/MEX) at every grid point.
  * Features p_ij = exp(-r_ij / 1.5 bohr): (p23, p12 + p13, p12 p13), invariant
  * under exchanging the two diatom atoms, standardised; four dense SiLU layers
- * of width 64; linear scalar output (standardised V).  BF16-rounded weights in
- * every product, FP32 accumulation, FP32 Adam masters.  Trained and evaluated
+ * of width 64; linear scalar output (standardised V).  FP32 weights and
+ * accumulation in every product, FP32 Adam.  Trained and evaluated
  * on the GPU by this library's kernels; the plain PES judges it. */
 typedef struct qd_mlp qd_mlp;
 int     qd_mlp_create(qd_mlp **out, uint64_t seed);      /* He-uniform initial weights */

@@ -3,8 +3,9 @@ of libqd.so (qd_mlp_*), the checker of its GPU forward and backward kernels.
 
 Same network: features p_ij = exp(-r_ij / 1.5), f = (p23, p12 + p13, p12 p13),
 standardised; four dense SiLU layers of width 64; linear output of the
-standardised V.  The weights are rounded to BF16 (round to nearest even) as
-the GPU kernels use them; everything else is FP64.  Loss: mean squared error
+standardised V.  The weights are the GPU's FP32 values (quant=True rounds them
+to BF16 first, the arithmetic of an earlier form of the kernels); everything
+else is FP64.  Loss: mean squared error
 of the standardised V.  Only tests/ load this module.
 """
 import numpy as np
@@ -52,9 +53,9 @@ def features(r12, r23, r13, norm):
     return (f - norm[0:3].astype(np.float64)) / norm[3:6].astype(np.float64)
 
 
-def forward(w, norm, r12, r23, r13, quant=True):
+def forward(w, norm, r12, r23, r13, quant=False):
     """Standardised output and the per-layer pre-activations and inputs
-    (quant=False: FP64 weights, for finite-difference checks of this module)."""
+    (the FP32 weights in FP64 arithmetic; quant=True: rounded to BF16 first)."""
     layers, wo, bo = _unpack(bf16(w) if quant else np.asarray(w, dtype=np.float64))
     a = features(r12, r23, r13, norm)
     zs, ins = [], []
@@ -72,9 +73,9 @@ def predict(w, norm, r12, r23, r13):
     return y * float(norm[7]) + float(norm[6])
 
 
-def loss_and_grad(w, norm, r12, r23, r13, V, quant=True):
+def loss_and_grad(w, norm, r12, r23, r13, V, quant=False):
     """Mean squared error of the standardised V and its gradient with respect
-    to the (BF16-rounded) parameters, in the parameter layout of the GPU."""
+    to the parameters, in the parameter layout of the GPU."""
     layers, wo, bo = _unpack(bf16(w) if quant else np.asarray(w, dtype=np.float64))
     y, zs, ins, a4 = forward(w, norm, r12, r23, r13, quant)
     t = (np.asarray(V, dtype=np.float64) - float(norm[6])) / float(norm[7])

@@ -26,7 +26,7 @@ def test_forward_and_gradient_match_fp64_restatement():
     with Surrogate(seed=7) as sur:
         sur.fit_normalisation(r12, r23, r13, V)
         w, norm = sur.params()
-        # forward: the GPU output against the FP64 network with the same BF16 weights
+        # forward: the GPU output against the FP64 network with the same FP32 weights
         got = sur(r12, r23, r13)
         ref = M.predict(w, norm, r12, r23, r13)
         assert np.abs(got - ref).max() < 1e-5 * np.abs(ref).max() + 1e-7
