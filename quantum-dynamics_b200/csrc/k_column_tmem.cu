@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
         dv[u] = fmaf(other * ysg, e.y, dv[u] * e.x);
       }
       put_row<H>(my_hi, my_lo, dv, slow ? exp2i(A_LOG2 - pe) : exp2i(-B_LOG2));
-    } else if (mode == COL_HEAD) {              // psi_z -> theta' values (FP64 phase)
+    } else if (mode == COL_HEAD) {              // psi_z -> theta' values
 #pragma unroll
       for (int u = 0; u < H; u++) {
         const int k = c0 + u;
@@ -611,13 +611,18 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
         if (qok && k < nth) {
           const size_t g = (size_t)k * n12 + q;
           const double2 z = p.psi_z[(size_t)run * nth * n12 + g];
-          double s, c;
-          sincos(p.dt * p.pot[voff + g], &s, &c);   // exp(-i V dt) = (c, -s)
-          double2 f = make_double2(c, -s);
-          if (p.prestep) {                     // psi / sqrt(v) * v = psi * sqrt(v)
-            double sh, ch;
-            sincos(0.5 * atan2(-s, c), &sh, &ch);
-            f = make_double2(ch, sh);
+          // exp(-i V dt) from the step's own complex64 table; the first step of
+          // a run takes its principal square root (psi / sqrt(v) * v), by the
+          // half-angle formulas in the form without cancellation
+          float2 f = expv[voff + g];
+          if (p.prestep) {
+            if (f.x >= 0.f) {
+              const float ch = sqrtf(0.5f * (1.f + f.x));
+              f = make_float2(ch, f.y / (2.f * ch));
+            } else {
+              const float sh = copysignf(sqrtf(0.5f * (1.f - f.x)), f.y);
+              f = make_float2(f.y / (2.f * sh), sh);
+            }
           }
           val = (float)((is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y) * sqrt(p.w[k]));
         }
