@@ -144,6 +144,159 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
   }
 }
 
+// ---- chirp-z form of the accumulation, for energies on a uniform grid ------------------
+// With E_e = E_0 + e dE (E_0, dE per run) and c(k) = e^{i dE dt k^2 / 2}, the
+// identity e t = (e^2 + t^2 - (e - t)^2) / 2 (Bluestein's) turns the chunk's sum
+// into a convolution:
+//   sum_t dt e^{i E_e (u + t) dt} x_t = F_e sum_t a_t conj(c(e - t)),
+//   a_t = x_t e^{i E_0 t dt} c(t),  F_e = dt e^{i E_e u dt} c(e),  u = t0 + 1,
+// taken as a cyclic convolution of length CZT_N >= FLUX_CHUNK + n_E - 1:
+// (a * b)_e = IFFT(FFT(a) FFT(b))_e with b_k = conj(c(k)) at k mod CZT_N for
+// -(FLUX_CHUNK - 1) <= k < n_E.  Two FP64 FFTs of 512 points per surface point
+// and field instead of n_E complex products per step: about 9x fewer FLOPs for
+// a full chunk.  FFTs: Stockham radix 8, three passes, one warp per sequence
+// (sixteen values per lane in registers between passes).
+
+// x[0..511] (one warp's sequence in shared memory) <- its DFT with
+// exp(SGN 2 pi i n m / 512); tw[m] = exp(-2 pi i m / 512)
+template <int SGN>
+__device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int lane)
+{
+#pragma unroll
+  for (int s = 0, Ns = 1; s < 3; s++, Ns *= 8) {
+    double2 v[2][8];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int j = lane + 32 * h, k = j & (Ns - 1);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        double2 z = x[j + 64 * i];
+        if (i && k) {                       // exp(SGN 2 pi i i k / (8 Ns)), index < 448
+          const double2 w = tw[i * k * (64 / Ns)];
+          z = cmul(z, SGN < 0 ? w : make_double2(w.x, -w.y));
+        }
+        v[h][i] = z;
+      }
+      SmallDFT<8, double2>::run(v[h], SGN, nullptr, 0);
+    }
+    __syncwarp();                           // every lane has read its inputs
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int j = lane + 32 * h, k = j & (Ns - 1);
+      const int base = (j - k) * 8 + k;
+#pragma unroll
+      for (int i = 0; i < 8; i++) x[base + i * Ns] = v[h][i];
+    }
+    __syncwarp();
+  }
+}
+
+constexpr int CZ_Q = 8;                     // surface points per tile: one warp each
+constexpr int CZ_LD = CZT_N + 2;            // padded sequence row (double2)
+
+// F_e of the chunk into phase[run][e][0]
+__global__ void __launch_bounds__(256) k_czt_f(AccumParams p)
+{
+  const int n = p.nruns * p.ne;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+    const int run = x / p.ne, e = x % p.ne;
+    const double u = (double)(p.t0 + 1);
+    double s1, c1, s2, c2;
+    sincos(p.energies[x] * p.dt * u, &s1, &c1);
+    sincos(0.5 * p.czt_de[run] * p.dt * (double)e * (double)e, &s2, &c2);
+    p.phase[(size_t)x * TMAX] = make_double2(p.dt * (c1 * c2 - s1 * s2), p.dt * (s1 * c2 + c1 * s2));
+  }
+}
+
+// grid (tiles, 2 fields, runs), 256 threads: tiles of CZ_Q surface points
+// strided over blockIdx.x; phi[e][q] += F_e IFFT(FFT(a) B)_e
+__global__ void __launch_bounds__(256) k_flux_czt(AccumParams p)
+{
+  extern __shared__ double2 czs[];
+  double2 *seq = czs;                        // [CZ_Q][CZ_LD]
+  double2 *tw = seq + CZ_Q * CZ_LD;          // [CZT_N]
+  double2 *bh = tw + CZT_N;                  // [CZT_N] this run's FFT(b) / CZT_N
+  double2 *gt = bh + CZT_N;                  // [TMAX]
+  double2 *fe = gt + TMAX;                   // [ne], ne <= CZT_N - TMAX + 1
+  const int field = blockIdx.y, run = blockIdx.z;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int x = tid; x < CZT_N; x += 256) {
+    tw[x] = p.czt_tw[x];
+    bh[x] = p.czt_b[(size_t)run * CZT_N + x];
+  }
+  for (int x = tid; x < p.nt; x += 256) gt[x] = p.czt_g[(size_t)run * TMAX + x];
+  for (int x = tid; x < p.ne; x += 256) fe[x] = p.phase[((size_t)run * p.ne + x) * TMAX];
+  const double2 *ring = field ? p.ring_g : p.ring_psi;
+  double2 *phi = field ? p.dfai : p.fai;
+  const int nqb = (p.nq + CZ_Q - 1) / CZ_Q;
+  const int qi = tid & 7, tl = tid >> 3;    // loads and stores: 8 points x 32 rows
+  for (int qb = blockIdx.x; qb < nqb; qb += gridDim.x) {
+    const int q = qb * CZ_Q + qi;
+    __syncthreads();                         // tables in, the previous tile's outputs read
+    for (int t = tl; t < CZT_N; t += 32) {   // a_t, zero past the chunk
+      double2 v = make_double2(0.0, 0.0);
+      if (t < p.nt && q < p.nq) v = cmul(ring[((size_t)t * p.nruns + run) * p.nq + q], gt[t]);
+      seq[qi * CZ_LD + t] = v;
+    }
+    __syncthreads();
+    double2 *x = seq + warp * CZ_LD;
+    warp_fft512<-1>(x, tw, lane);
+    for (int m = lane; m < CZT_N; m += 32) x[m] = cmul(x[m], bh[m]);
+    __syncwarp();
+    warp_fft512<+1>(x, tw, lane);
+    __syncthreads();
+    if (q < p.nq)
+      for (int e = tl; e < p.ne; e += 32) {
+        const double2 z = cmul(seq[qi * CZ_LD + e], fe[e]);
+        double2 *d = phi + ((size_t)run * p.ne + e) * p.nq + q;
+        double2 o = *d;
+        o.x += z.x;
+        o.y += z.y;
+        *d = o;
+      }
+  }
+}
+
+size_t czt_smem() { return sizeof(double2) * ((size_t)CZ_Q * CZ_LD + 2 * CZT_N + TMAX + (CZT_N - TMAX + 1)); }
+
+// per run: g[t] = e^{i E_0 t dt} c(t), and FFT(b) / CZT_N by one warp; block 0
+// also writes the twiddle table
+__global__ void __launch_bounds__(64) k_czt_tables(int ne, double dt, const double *e0,
+                                                   const double *de, double2 *tw, double2 *g,
+                                                   double2 *b)
+{
+  __shared__ double2 tws[CZT_N], bs[CZT_N];
+  const int run = blockIdx.x, tid = threadIdx.x;
+  for (int m = tid; m < CZT_N; m += 64) {
+    double s, c;
+    sincospi((double)m / (CZT_N / 2), &s, &c);
+    tws[m] = make_double2(c, -s);
+    if (run == 0) tw[m] = tws[m];
+  }
+  const double hd = 0.5 * de[run] * dt;
+  for (int t = tid; t < TMAX; t += 64) {
+    double s1, c1, s2, c2;
+    sincos(e0[run] * dt * (double)t, &s1, &c1);
+    sincos(hd * (double)t * (double)t, &s2, &c2);
+    g[(size_t)run * TMAX + t] = make_double2(c1 * c2 - s1 * s2, s1 * c2 + c1 * s2);
+  }
+  for (int m = tid; m < CZT_N; m += 64) {
+    const int k = m < ne ? m : m - CZT_N;    // k in [-(TMAX-1), ne - 1] or unused
+    double2 v = make_double2(0.0, 0.0);
+    if (k < ne && k > -TMAX) {
+      double s, c;
+      sincos(hd * (double)k * (double)k, &s, &c);
+      v = make_double2(c, -s);               // conj(c(k))
+    }
+    bs[m] = v;
+  }
+  __syncthreads();
+  if (tid < 32) warp_fft512<-1>(bs, tws, tid);
+  __syncthreads();
+  for (int m = tid; m < CZT_N; m += 64)
+    b[(size_t)run * CZT_N + m] = make_double2(bs[m].x / CZT_N, bs[m].y / CZT_N);
+}
+
 __global__ void __launch_bounds__(256) k_crp(CrpParams p)
 {
   __shared__ double red[32];
@@ -184,6 +337,23 @@ cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 {
   if (p.nt <= 0) return cudaSuccess;
   if (p.nt > TMAX) return cudaErrorInvalidValue;
+  if (p.czt_b && p.nt >= CZT_MIN_STEPS && p.ne <= CZT_N - TMAX + 1) {   // chirp-z form
+    static bool attr = false;
+    const size_t sm = czt_smem();
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(k_flux_czt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    const int nf = p.nruns * p.ne;
+    k_czt_f<<<(nf + 255) / 256, 256, 0, s>>>(p);
+    const int nqb = (p.nq + CZ_Q - 1) / CZ_Q;
+    int gx = (148 * 8 + 2 * p.nruns - 1) / (2 * p.nruns);   // about eight CTAs per SM in all
+    gx = gx < 1 ? 1 : gx > nqb ? nqb : gx;
+    k_flux_czt<<<dim3(gx, 2, p.nruns), 256, sm, s>>>(p);
+    return cudaGetLastError();
+  }
   const int n = p.nruns * p.ne * p.nt;
   k_flux_phase<<<(n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096, 256, 0, s>>>(p);
   switch (p.variant) {   // (energies per CTA, steps per staged chunk)
@@ -202,3 +372,11 @@ cudaError_t launch_crp(const CrpParams &p, cudaStream_t s)
 }
 
 int flux_accum_launches() { return 2; }
+
+cudaError_t launch_czt_tables(int nruns, int ne, double dt, const double *e0, const double *de,
+                              double2 *tw, double2 *g, double2 *b, cudaStream_t s)
+{
+  if (ne < 1 || ne > CZT_N - TMAX + 1) return cudaErrorInvalidValue;
+  k_czt_tables<<<nruns, 64, 0, s>>>(ne, dt, e0, de, tw, g, b);
+  return cudaGetLastError();
+}

@@ -431,7 +431,10 @@ struct qd_handle {
   double2 *d_psi_z = nullptr;
   void *d_surf = nullptr;
   double2 *d_ring_psi = nullptr, *d_ring_g = nullptr, *d_fai = nullptr, *d_dfai = nullptr;
-  double2 *d_phase = nullptr;     // chunk phase factors [run][E][128]
+  double2 *d_phase = nullptr;     // chunk phase factors [run][E][FLUX_CHUNK]
+  // chirp-z form of the accumulation (every run's energies on a uniform grid)
+  double2 *d_czt_tw = nullptr, *d_czt_g = nullptr, *d_czt_b = nullptr;
+  double *d_czt_de = nullptr;
   double *d_energies = nullptr, *d_eta = nullptr, *d_crp = nullptr;
   double *d_norms = nullptr;
   int norms_cap = 0;
@@ -698,6 +701,7 @@ AccumParams accum_params(const qd_handle *h)
   a.ring_g = h->d_ring_g; a.fai = h->d_fai; a.dfai = h->d_dfai;
   a.phase = h->d_phase;
   a.variant = h->flux_variant;
+  a.czt_tw = h->d_czt_tw; a.czt_g = h->d_czt_g; a.czt_b = h->d_czt_b; a.czt_de = h->d_czt_de;
   return a;
 }
 
@@ -868,6 +872,7 @@ int tune_flux(qd_handle *h)
   AccumParams a = accum_params(h);
   a.nt = QD_RING;
   a.t0 = 0;
+  a.czt_b = nullptr;      // the GEMM form (with the chirp-z tables: chunks below CZT_MIN_STEPS)
   float best = 1e30f;
   for (int v = 0; v < flux_variants(); v++) {
     a.variant = v;
@@ -1356,6 +1361,35 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
                          sizeof(double) * h->ne, cudaMemcpyHostToDevice, h->st));
     }
     TRY(h->alloc(h->d_crp, (size_t)h->ne * nruns));
+    // energies E_0 + j dE in every run (to a phase error below 1e-12 rad over a
+    // chunk): the accumulation of full chunks takes the chirp-z form
+    // (QD_FLUX_CZT=0 keeps the GEMM form)
+    const char *cz = getenv("QD_FLUX_CZT");
+    bool uniform = h->ne >= 2 && h->ne <= CZT_N - FLUX_CHUNK + 1 && !(cz && cz[0] == '0');
+    std::vector<double> e0(nruns), de(nruns);
+    for (int r = 0; r < nruns && uniform; r++) {
+      const double *E = runs[r].CRP.energies;
+      e0[r] = E[0];
+      de[r] = (E[h->ne - 1] - E[0]) / (h->ne - 1);
+      double dev = 0.0;
+      for (int j = 0; j < h->ne; j++) dev = std::max(dev, std::fabs(E[j] - (e0[r] + j * de[r])));
+      uniform = de[r] != 0.0 && dev * FLUX_CHUNK * std::fabs(h->dt) <= 1e-12;
+    }
+    if (uniform) {
+      double *d_e0 = nullptr;
+      TRY(h->alloc(h->d_czt_tw, (size_t)CZT_N));
+      TRY(h->alloc(h->d_czt_g, (size_t)FLUX_CHUNK * nruns));
+      TRY(h->alloc(h->d_czt_b, (size_t)CZT_N * nruns));
+      TRY(h->alloc(h->d_czt_de, (size_t)nruns));
+      TRY(h->alloc(d_e0, (size_t)nruns));
+      CU(cudaMemcpyAsync(d_e0, e0.data(), sizeof(double) * nruns, cudaMemcpyHostToDevice, h->st));
+      CU(cudaMemcpyAsync(h->d_czt_de, de.data(), sizeof(double) * nruns, cudaMemcpyHostToDevice,
+                         h->st));
+      CU(launch_czt_tables(nruns, h->ne, h->dt, d_e0, h->d_czt_de, h->d_czt_tw, h->d_czt_g,
+                           h->d_czt_b, h->st));
+      g_launches++;
+      CU(cudaStreamSynchronize(h->st));       // e0, de: host vectors of this scope
+    }
   }
   const char *path = getenv("QD_COLUMN_PATH");   // "simt" forces the SIMT column pass
   if (!f64 && !(path && std::string(path) == "simt")) {

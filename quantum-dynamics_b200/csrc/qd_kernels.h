@@ -190,7 +190,17 @@ struct AccumParams {
   double2 *fai, *dfai;
   double2 *phase;          // workspace [nruns][ne][FLUX_CHUNK] for the chunk's e^{iEt} factors
   int variant;             // GEMM tile variant, 0 .. flux_variants() - 1 (the autotuner's choice)
+  // chirp-z form (energies on a uniform grid per run; null czt_b: the GEMM form)
+  const double2 *czt_tw;   // [CZT_N] e^{-2 pi i m / CZT_N}
+  const double2 *czt_g;    // [nruns][FLUX_CHUNK] e^{i E_0 t dt} c(t)
+  const double2 *czt_b;    // [nruns][CZT_N] FFT of b_k = conj(c(k)), divided by CZT_N
+  const double *czt_de;    // [nruns] energy spacing dE; c(k) = e^{i dE dt k^2 / 2}
 };
+constexpr int CZT_N = 512;       // cyclic convolution length of the chirp-z form
+constexpr int CZT_MIN_STEPS = 125;   // chunks of fewer steps take the GEMM form
+// tables of the chirp-z form for runs with energies e0[r] + j de[r], j < ne
+cudaError_t launch_czt_tables(int nruns, int ne, double dt, const double *e0, const double *de,
+                              double2 *tw, double2 *g, double2 *b, cudaStream_t s);
 int flux_accum_launches();
 int flux_variants();
 
