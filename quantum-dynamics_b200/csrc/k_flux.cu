@@ -157,7 +157,13 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
 // a full chunk.  FFTs: Stockham radix 8, three passes, one warp per sequence
 // (sixteen values per lane in registers between passes).
 
-// x[0..511] (one warp's sequence in shared memory) <- its DFT with
+// element m of a sequence in shared memory sits at czp(m): one padding slot
+// after every 8, so that the 16-byte accesses of every pass (stride 1, 8 or 64
+// elements across the lanes) fall into distinct bank groups
+__device__ __forceinline__ int czp(int m) { return m + (m >> 3); }
+constexpr int CZ_PADN = CZT_N + CZT_N / 8;  // padded sequence length (double2)
+
+// x (one warp's sequence in shared memory, padded) <- its DFT with
 // exp(SGN 2 pi i n m / 512); tw[m] = exp(-2 pi i m / 512)
 template <int SGN>
 __device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int lane)
@@ -170,7 +176,7 @@ __device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int l
       const int j = lane + 32 * h, k = j & (Ns - 1);
 #pragma unroll
       for (int i = 0; i < 8; i++) {
-        double2 z = x[j + 64 * i];
+        double2 z = x[czp(j + 64 * i)];
         if (i && k) {                       // exp(SGN 2 pi i i k / (8 Ns)), index < 448
           const double2 w = tw[i * k * (64 / Ns)];
           z = cmul(z, SGN < 0 ? w : make_double2(w.x, -w.y));
@@ -185,14 +191,14 @@ __device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int l
       const int j = lane + 32 * h, k = j & (Ns - 1);
       const int base = (j - k) * 8 + k;
 #pragma unroll
-      for (int i = 0; i < 8; i++) x[base + i * Ns] = v[h][i];
+      for (int i = 0; i < 8; i++) x[czp(base + i * Ns)] = v[h][i];
     }
     __syncwarp();
   }
 }
 
 constexpr int CZ_Q = 8;                     // surface points per tile: one warp each
-constexpr int CZ_LD = CZT_N + 2;            // padded sequence row (double2)
+constexpr int CZ_LD = CZ_PADN + 1;          // sequence row stride (double2): rows 4 banks apart
 
 // F_e of the chunk into phase[run][e][0]
 __global__ void __launch_bounds__(256) k_czt_f(AccumParams p)
@@ -236,18 +242,18 @@ __global__ void __launch_bounds__(256) k_flux_czt(AccumParams p)
     for (int t = tl; t < CZT_N; t += 32) {   // a_t, zero past the chunk
       double2 v = make_double2(0.0, 0.0);
       if (t < p.nt && q < p.nq) v = cmul(ring[((size_t)t * p.nruns + run) * p.nq + q], gt[t]);
-      seq[qi * CZ_LD + t] = v;
+      seq[qi * CZ_LD + czp(t)] = v;
     }
     __syncthreads();
     double2 *x = seq + warp * CZ_LD;
     warp_fft512<-1>(x, tw, lane);
-    for (int m = lane; m < CZT_N; m += 32) x[m] = cmul(x[m], bh[m]);
+    for (int m = lane; m < CZT_N; m += 32) x[czp(m)] = cmul(x[czp(m)], bh[m]);
     __syncwarp();
     warp_fft512<+1>(x, tw, lane);
     __syncthreads();
     if (q < p.nq)
       for (int e = tl; e < p.ne; e += 32) {
-        const double2 z = cmul(seq[qi * CZ_LD + e], fe[e]);
+        const double2 z = cmul(seq[qi * CZ_LD + czp(e)], fe[e]);
         double2 *d = phi + ((size_t)run * p.ne + e) * p.nq + q;
         double2 o = *d;
         o.x += z.x;
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(64) k_czt_tables(int ne, double dt, const doub
                                                    const double *de, double2 *tw, double2 *g,
                                                    double2 *b)
 {
-  __shared__ double2 tws[CZT_N], bs[CZT_N];
+  __shared__ double2 tws[CZT_N], bs[CZ_PADN];
   const int run = blockIdx.x, tid = threadIdx.x;
   for (int m = tid; m < CZT_N; m += 64) {
     double s, c;
@@ -288,13 +294,13 @@ __global__ void __launch_bounds__(64) k_czt_tables(int ne, double dt, const doub
       sincos(hd * (double)k * (double)k, &s, &c);
       v = make_double2(c, -s);               // conj(c(k))
     }
-    bs[m] = v;
+    bs[czp(m)] = v;
   }
   __syncthreads();
   if (tid < 32) warp_fft512<-1>(bs, tws, tid);
   __syncthreads();
   for (int m = tid; m < CZT_N; m += 64)
-    b[(size_t)run * CZT_N + m] = make_double2(bs[m].x / CZT_N, bs[m].y / CZT_N);
+    b[(size_t)run * CZT_N + m] = make_double2(bs[czp(m)].x / CZT_N, bs[czp(m)].y / CZT_N);
 }
 
 __global__ void __launch_bounds__(256) k_crp(CrpParams p)
