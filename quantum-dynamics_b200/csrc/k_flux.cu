@@ -163,10 +163,23 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
 __device__ __forceinline__ int czp(int m) { return m + (m >> 3); }
 constexpr int CZ_PADN = CZT_N + CZT_N / 8;  // padded sequence length (double2)
 
+// twiddles of the two passes that have them, laid out [i][k] so that the
+// lanes of a warp (consecutive k) read consecutive entries: twf[i 8 + k] =
+// w^(8 i k) (pass 2, k < 8), twf[64 + i 64 + k] = w^(i k) (pass 3, k < 64),
+// w = exp(-2 pi i / 512); built from tw[m] = w^m
+constexpr int CZ_TWF = 64 + 8 * 64;
+__device__ __forceinline__ void build_twf(double2 *twf, const double2 *tw, int tid, int nthr)
+{
+  for (int x = tid; x < CZ_TWF; x += nthr) {
+    const int i = x < 64 ? x >> 3 : (x - 64) >> 6, k = x < 64 ? x & 7 : (x - 64) & 63;
+    twf[x] = tw[x < 64 ? 8 * i * k : i * k];
+  }
+}
+
 // x (one warp's sequence in shared memory, padded) <- its DFT with
-// exp(SGN 2 pi i n m / 512); tw[m] = exp(-2 pi i m / 512)
+// exp(SGN 2 pi i n m / 512); twf from build_twf
 template <int SGN>
-__device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int lane)
+__device__ __forceinline__ void warp_fft512(double2 *x, const double2 *twf, int lane)
 {
 #pragma unroll
   for (int s = 0, Ns = 1; s < 3; s++, Ns *= 8) {
@@ -177,8 +190,8 @@ __device__ __forceinline__ void warp_fft512(double2 *x, const double2 *tw, int l
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         double2 z = x[czp(j + 64 * i)];
-        if (i && k) {                       // exp(SGN 2 pi i i k / (8 Ns)), index < 448
-          const double2 w = tw[i * k * (64 / Ns)];
+        if (i && k) {                       // exp(SGN 2 pi i i k / (8 Ns))
+          const double2 w = twf[Ns == 8 ? i * 8 + k : 64 + i * 64 + k];
           z = cmul(z, SGN < 0 ? w : make_double2(w.x, -w.y));
         }
         v[h][i] = z;
@@ -216,34 +229,46 @@ __global__ void __launch_bounds__(256) k_czt_f(AccumParams p)
 
 // grid (tiles, 2 fields, runs), 256 threads: tiles of CZ_Q surface points
 // strided over blockIdx.x; phi[e][q] += F_e IFFT(FFT(a) B)_e
-__global__ void __launch_bounds__(256) k_flux_czt(AccumParams p)
+__global__ void __launch_bounds__(256, 2) k_flux_czt(AccumParams p)
 {
   extern __shared__ double2 czs[];
   double2 *seq = czs;                        // [CZ_Q][CZ_LD]
-  double2 *tw = seq + CZ_Q * CZ_LD;          // [CZT_N]
-  double2 *bh = tw + CZT_N;                  // [CZT_N] this run's FFT(b) / CZT_N
+  double2 *tw = seq + CZ_Q * CZ_LD;          // [CZ_TWF] pass twiddles
+  double2 *bh = tw + CZ_TWF;                 // [CZT_N] this run's FFT(b) / CZT_N
   double2 *gt = bh + CZT_N;                  // [TMAX]
   double2 *fe = gt + TMAX;                   // [ne], ne <= CZT_N - TMAX + 1
   const int field = blockIdx.y, run = blockIdx.z;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int x = tid; x < CZT_N; x += 256) {
-    tw[x] = p.czt_tw[x];
-    bh[x] = p.czt_b[(size_t)run * CZT_N + x];
-  }
+  build_twf(tw, p.czt_tw, tid, 256);
+  for (int x = tid; x < CZT_N; x += 256) bh[x] = p.czt_b[(size_t)run * CZT_N + x];
   for (int x = tid; x < p.nt; x += 256) gt[x] = p.czt_g[(size_t)run * TMAX + x];
   for (int x = tid; x < p.ne; x += 256) fe[x] = p.phase[((size_t)run * p.ne + x) * TMAX];
   const double2 *ring = field ? p.ring_g : p.ring_psi;
   double2 *phi = field ? p.dfai : p.fai;
   const int nqb = (p.nq + CZ_Q - 1) / CZ_Q;
   const int qi = tid & 7, tl = tid >> 3;    // loads and stores: 8 points x 32 rows
+  constexpr int NR = (TMAX + 31) / 32;       // history rows per thread
+  double2 nx[NR];                            // this thread's history values of the tile
+  auto fetch = [&](int qb) {
+    const int q = qb * CZ_Q + qi;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int t = tl + 32 * r;
+      nx[r] = (qb < nqb && t < p.nt && q < p.nq) ? ring[((size_t)t * p.nruns + run) * p.nq + q]
+                                                 : make_double2(0.0, 0.0);
+    }
+  };
   for (int qb = blockIdx.x; qb < nqb; qb += gridDim.x) {
     const int q = qb * CZ_Q + qi;
+    fetch(qb);                               // (loading the next tile's during the transforms
+                                             // measured no faster, with more registers)
     __syncthreads();                         // tables in, the previous tile's outputs read
-    for (int t = tl; t < CZT_N; t += 32) {   // a_t, zero past the chunk
-      double2 v = make_double2(0.0, 0.0);
-      if (t < p.nt && q < p.nq) v = cmul(ring[((size_t)t * p.nruns + run) * p.nq + q], gt[t]);
-      seq[qi * CZ_LD + czp(t)] = v;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {           // a_t
+      const int t = tl + 32 * r;
+      if (t < TMAX) seq[qi * CZ_LD + czp(t)] = t < p.nt ? cmul(nx[r], gt[t]) : make_double2(0.0, 0.0);
     }
+    for (int t = TMAX + tl; t < CZT_N; t += 32) seq[qi * CZ_LD + czp(t)] = make_double2(0.0, 0.0);
     __syncthreads();
     double2 *x = seq + warp * CZ_LD;
     warp_fft512<-1>(x, tw, lane);
@@ -263,7 +288,7 @@ __global__ void __launch_bounds__(256) k_flux_czt(AccumParams p)
   }
 }
 
-size_t czt_smem() { return sizeof(double2) * ((size_t)CZ_Q * CZ_LD + 2 * CZT_N + TMAX + (CZT_N - TMAX + 1)); }
+size_t czt_smem() { return sizeof(double2) * ((size_t)CZ_Q * CZ_LD + CZ_TWF + CZT_N + TMAX + (CZT_N - TMAX + 1)); }
 
 // per run: g[t] = e^{i E_0 t dt} c(t), and FFT(b) / CZT_N by one warp; block 0
 // also writes the twiddle table
@@ -271,7 +296,7 @@ __global__ void __launch_bounds__(64) k_czt_tables(int ne, double dt, const doub
                                                    const double *de, double2 *tw, double2 *g,
                                                    double2 *b)
 {
-  __shared__ double2 tws[CZT_N], bs[CZ_PADN];
+  __shared__ double2 tws[CZT_N], twf[CZ_TWF], bs[CZ_PADN];
   const int run = blockIdx.x, tid = threadIdx.x;
   for (int m = tid; m < CZT_N; m += 64) {
     double s, c;
@@ -297,7 +322,9 @@ __global__ void __launch_bounds__(64) k_czt_tables(int ne, double dt, const doub
     bs[czp(m)] = v;
   }
   __syncthreads();
-  if (tid < 32) warp_fft512<-1>(bs, tws, tid);
+  build_twf(twf, tws, tid, 64);
+  __syncthreads();
+  if (tid < 32) warp_fft512<-1>(bs, twf, tid);
   __syncthreads();
   for (int m = tid; m < CZT_N; m += 64)
     b[(size_t)run * CZT_N + m] = make_double2(bs[czp(m)].x / CZT_N, bs[czp(m)].y / CZT_N);
