@@ -53,7 +53,10 @@ extern "C" {
 /* arithmetic of the propagation */
 #define QD_PREC_FP64  0  /* plain form: complex128 psi, FP64 everywhere       */
 #define QD_PREC_FP32  1  /* complex64 psi, 3xFP16 tensor-core Legendre GEMM,
-                            FP64 flux-to-P(E) accumulation and norm          */
+                            FP64 flux-to-P(E) accumulation and norm; the
+                            input psi is rounded to complex64 when the handle
+                            is created (it crosses the bus in complex64), and
+                            psi read back is that complex64 state, widened  */
 
 /* RadialCoordinate (common/MatlabStructures.h:12-39).  r0, k0, delta are the
  * initial-packet parameters that only the setup helpers read

@@ -191,6 +191,33 @@ cudaError_t launch_legendre_matrices(int nth, int nl, const double *, const doub
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_widen_c(const float2 *src, double2 *dst, size_t n)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = make_double2(src[i].x, src[i].y);
+}
+__global__ void k_narrow_c(const double2 *src, float2 *dst, size_t n)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+}
+}  // namespace
+
+cudaError_t launch_widen_c(const float2 *src, double2 *dst, size_t n, cudaStream_t s)
+{
+  k_widen_c<<<148 * 8, 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_narrow_c(const double2 *src, float2 *dst, size_t n, cudaStream_t s)
+{
+  k_narrow_c<<<148 * 8, 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_legendre_basis(int n, int K, int m, const double *x, double *legendre,
                                   cudaStream_t s)
 {

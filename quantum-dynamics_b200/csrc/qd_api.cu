@@ -272,6 +272,30 @@ class Staging {
     if (finite) *finite = ok_all;
     return cudaSuccess;
   }
+  // host doubles -> device floats (rounded to nearest), staged like upload; the
+  // doubles are checked on the way: *in_range = none is NaN/Inf or beyond the
+  // FP32 range
+  cudaError_t upload_narrow(float *dst, const double *src, size_t n, cudaStream_t st,
+                            bool *in_range)
+  {
+    *in_range = true;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!ready()) return cudaErrorMemoryAllocation;
+    const size_t per = CHUNK / sizeof(float);    // doubles per staged chunk
+    bool ok_all = true;
+    for (size_t off = 0; off < n; off += per) {
+      const int b = (int)(next_++ % NBUF);
+      cudaError_t e = cudaEventSynchronize(ev_[b]);
+      if (e != cudaSuccess) return e;
+      const size_t m = std::min(per, n - off);
+      ok_all = narrow_copy(static_cast<float *>(buf_[b]), src + off, m) && ok_all;
+      e = cudaMemcpyAsync(dst + off, buf_[b], m * sizeof(float), cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
+      if (e != cudaSuccess) return e;
+    }
+    *in_range = ok_all;
+    return cudaSuccess;
+  }
   // device -> host of one array; returns once dst holds the data
   cudaError_t download(void *dst, const void *src, size_t bytes, cudaStream_t st)
   {
@@ -284,14 +308,20 @@ class Staging {
   struct Piece {
     void *dst;
     const void *src;
-    size_t bytes;
+    size_t bytes;         // device bytes
+    bool widen = false;   // src holds floats, dst receives them as doubles (2 x bytes)
   };
   cudaError_t download(const Piece *pc, int np, cudaStream_t st)
   {
     std::lock_guard<std::mutex> lock(mu_);
     size_t total = 0;
-    for (int i = 0; i < np; i++) total += pc[i].bytes;
-    if (!ready() || (np == 1 && total < LARGE)) {
+    bool widen = false;
+    for (int i = 0; i < np; i++) {
+      total += pc[i].bytes;
+      widen = widen || pc[i].widen;
+    }
+    if (widen && !ready()) return cudaErrorMemoryAllocation;
+    if (!widen && (!ready() || (np == 1 && total < LARGE))) {
       for (int i = 0; i < np; i++) {
         cudaError_t e = cudaMemcpyAsync(pc[i].dst, pc[i].src, pc[i].bytes, cudaMemcpyDeviceToHost,
                                         st);
@@ -330,8 +360,13 @@ class Staging {
       cudaError_t e = cudaEventSynchronize(ev_[b]);
       if (e != cudaSuccess) return e;
       each_part(c, [&](int i, size_t po, size_t co, size_t n) {
-        copy_scan(static_cast<char *>(pc[i].dst) + po, static_cast<const char *>(buf_[b]) + co, n,
-                  false);
+        if (pc[i].widen)
+          widen_copy(static_cast<double *>(pc[i].dst) + po / sizeof(float),
+                     reinterpret_cast<const float *>(static_cast<const char *>(buf_[b]) + co),
+                     n / sizeof(float));
+        else
+          copy_scan(static_cast<char *>(pc[i].dst) + po, static_cast<const char *>(buf_[b]) + co,
+                    n, false);
       });
       if (c + NBUF - 1 < nch) {
         e = issue(c + NBUF - 1);
@@ -374,6 +409,37 @@ class Staging {
                              (z - a) / 8);
     });
     return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
+  }
+  // dst[i] = (float)src[i] over the host pool; false if some src[i] is NaN,
+  // Inf or beyond the FP32 range
+  static bool narrow_copy(float *dst, const double *src, size_t n)
+  {
+    HostPool &pool = HostPool::get();
+    const unsigned nt = pool.size();
+    const size_t part = (n / nt + 15) & ~size_t(15);
+    std::vector<char> ok(nt, 1);
+    pool.run([&](unsigned t) {
+      const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
+      bool good = true;
+      for (size_t i = a; i < z; i++) {
+        const double v = src[i];
+        good = good && std::fabs(v) <= 3.4028234663852886e38;   // false for NaN too
+        dst[i] = (float)v;
+      }
+      ok[t] = good;
+    });
+    return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
+  }
+  // dst[i] = src[i] widened to double, over the host pool
+  static void widen_copy(double *dst, const float *src, size_t n)
+  {
+    HostPool &pool = HostPool::get();
+    const unsigned nt = pool.size();
+    const size_t part = (n / nt + 15) & ~size_t(15);
+    pool.run([&](unsigned t) {
+      const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
+      for (size_t i = a; i < z; i++) dst[i] = (double)src[i];
+    });
   }
   std::mutex mu_;
   bool tried_ = false, ok_ = false;
@@ -429,6 +495,9 @@ struct qd_handle {
   float2 *d_tw1_32 = nullptr, *d_tw2_32 = nullptr;
   void *d_lpsi = nullptr;
   double2 *d_psi_z = nullptr;
+  // complex64 handles: the theta-space state crosses the bus in complex64 (the
+  // precision it is propagated in), through this buffer
+  float2 *d_psi32 = nullptr;
   void *d_surf = nullptr;
   double2 *d_ring_psi = nullptr, *d_ring_g = nullptr, *d_fai = nullptr, *d_dfai = nullptr;
   double2 *d_phase = nullptr;     // chunk phase factors [run][E][FLUX_CHUNK]
@@ -1334,11 +1403,27 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   // the column passes read them as A entries of their contraction over l
   CU(cudaMemsetAsync(lp, 0, csz * h->n12 * h->nl * nruns, h->st));
   TRY(h->alloc(h->d_psi_z, npt * nruns));
-  for (int r = 0; r < nruns; r++) {
-    bool fin = true;
-    CU(Staging::get().upload(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt, h->st,
-                             sizeof(double2) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
-    if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
+  if (f64) {
+    for (int r = 0; r < nruns; r++) {
+      bool fin = true;
+      CU(Staging::get().upload(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt, h->st,
+                               sizeof(double2) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
+      if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
+    }
+  } else {
+    // complex64 form: psi rounded to complex64 by the host threads that stage it
+    // (half the bytes over the bus), then widened into the FP64 staging array
+    TRY(h->alloc(h->d_psi32, npt * nruns));
+    for (int r = 0; r < nruns; r++) {
+      bool ok = true;
+      CU(Staging::get().upload_narrow(reinterpret_cast<float *>(h->d_psi32 + r * npt),
+                                      runs[r].psi, 2 * (size_t)npt, h->st, &ok));
+      if (!ok)
+        return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf or values beyond the "
+                       "complex64 range", r);
+    }
+    CU(launch_widen_c(h->d_psi32, h->d_psi_z, (size_t)npt * nruns, h->st));
+    g_launches++;
   }
   if (h->do_crp) {
     const size_t nq = (size_t)h->nth * h->n1;
@@ -1423,6 +1508,13 @@ int get_psi(qd_handle *h, int run, double *psi_out)
   if (run < 0 || run >= h->nruns) return set_err(QD_ERR_INVALID, "run %d of %d", run, h->nruns);
   const long npt = h->n12 * h->nth;
   TRY(stage_psi(h));
+  if (h->d_psi32) {             // complex64 form: every value is a complex64 one
+    CU(launch_narrow_c(h->d_psi_z + (long)run * npt, h->d_psi32 + (long)run * npt, npt, h->st));
+    g_launches++;
+    Staging::Piece pc{psi_out, h->d_psi32 + (long)run * npt, sizeof(float2) * npt, true};
+    CU(Staging::get().download(&pc, 1, h->st));
+    return QD_OK;
+  }
   CU(Staging::get().download(psi_out, h->d_psi_z + (long)run * npt, sizeof(double2) * npt,
                              h->st));
   return QD_OK;
@@ -1703,8 +1795,15 @@ int qd_download(qd_handle *h)
   if (crp) TRY(compute_crp(h));
   const long npt = h->n12 * h->nth;
   std::vector<Staging::Piece> pcs;
+  if (h->d_psi32) {             // complex64 form: every value is a complex64 one
+    CU(launch_narrow_c(h->d_psi_z, h->d_psi32, (size_t)npt * h->nruns, h->st));
+    g_launches++;
+  }
   for (int r = 0; r < h->nruns; r++) {
-    pcs.push_back({h->runs[r]->psi, h->d_psi_z + (long)r * npt, sizeof(double2) * npt});
+    if (h->d_psi32)
+      pcs.push_back({h->runs[r]->psi, h->d_psi32 + (long)r * npt, sizeof(float2) * npt, true});
+    else
+      pcs.push_back({h->runs[r]->psi, h->d_psi_z + (long)r * npt, sizeof(double2) * npt});
     if (crp)
       pcs.push_back({h->runs[r]->CRP.CRP, h->d_crp + (long)r * h->ne, sizeof(double) * h->ne});
   }

@@ -259,6 +259,9 @@ cudaError_t launch_legendre_matrices(int nth, int nl, const double *x, const dou
                                      const double *legendre, double *P, double *WP,
                                      float *P32, float *WP32, float *P32lo, float *WP32lo,
                                      cudaStream_t s);
+// complex64 <-> complex128 copies of the theta-space state (n complex values)
+cudaError_t launch_widen_c(const float2 *src, double2 *dst, size_t n, cudaStream_t s);
+cudaError_t launch_narrow_c(const double2 *src, float2 *dst, size_t n, cudaStream_t s);
 cudaError_t launch_legendre_basis(int n, int K, int m, const double *x, double *legendre,
                                   cudaStream_t s);
 cudaError_t launch_roots(int n, double2 *tw64, float2 *tw32, cudaStream_t s);
