@@ -26,6 +26,9 @@
 #include <tuple>
 #include <vector>
 #include <unistd.h>
+#ifdef __SSE2__
+#include <emmintrin.h>
+#endif
 #include "qd.h"
 #include "qd_kernels.h"
 #include "qd_tc.h"
@@ -420,13 +423,30 @@ class Staging {
     std::vector<char> ok(nt, 1);
     pool.run([&](unsigned t) {
       const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
-      bool good = true;
-      for (size_t i = a; i < z; i++) {
-        const double v = src[i];
-        good = good && std::fabs(v) <= 3.4028234663852886e38;   // false for NaN too
-        dst[i] = (float)v;
+      // |v| above FLT_MAX, Inf and NaN are the magnitudes above FLT_MAX's bits
+      constexpr uint64_t MAGN = 0x7fffffffffffffffull, FMAX = 0x47efffffe0000000ull;
+      uint64_t bad = 0;
+      size_t i = a;
+#ifdef __SSE2__
+      // four values a round, streamed past the caches into the staging buffer
+      // (dst + a is 16-byte aligned: a is a multiple of 16 and dst a page-locked buffer)
+      for (; i + 4 <= z; i += 4) {
+        const __m128d v0 = _mm_loadu_pd(src + i), v1 = _mm_loadu_pd(src + i + 2);
+        _mm_stream_ps(dst + i, _mm_movelh_ps(_mm_cvtpd_ps(v0), _mm_cvtpd_ps(v1)));
+        uint64_t u[4];
+        std::memcpy(u, src + i, sizeof u);
+        bad |= ((u[0] & MAGN) > FMAX) | ((u[1] & MAGN) > FMAX) | ((u[2] & MAGN) > FMAX) |
+               ((u[3] & MAGN) > FMAX);
       }
-      ok[t] = good;
+      _mm_sfence();
+#endif
+      for (; i < z; i++) {
+        uint64_t u;
+        std::memcpy(&u, src + i, sizeof u);
+        bad |= (u & MAGN) > FMAX;
+        dst[i] = (float)src[i];
+      }
+      ok[t] = bad == 0;
     });
     return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
   }
@@ -438,7 +458,18 @@ class Staging {
     const size_t part = (n / nt + 15) & ~size_t(15);
     pool.run([&](unsigned t) {
       const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
-      for (size_t i = a; i < z; i++) dst[i] = (double)src[i];
+      size_t i = a;
+#ifdef __SSE2__
+      // two values a round, streamed to the caller's array when it is 16-byte aligned
+      if ((reinterpret_cast<uintptr_t>(dst + a) & 15) == 0) {
+        for (; i + 2 <= z; i += 2) {
+          const __m128 f = _mm_castsi128_ps(_mm_loadl_epi64(reinterpret_cast<const __m128i *>(src + i)));
+          _mm_stream_pd(dst + i, _mm_cvtps_pd(f));
+        }
+        _mm_sfence();
+      }
+#endif
+      for (; i < z; i++) dst[i] = (double)src[i];
     });
   }
   std::mutex mu_;
