@@ -239,14 +239,15 @@ def test_fp32_tensor_core_and_simt_agree(monkeypatch):
                                    (256, 192, 16)])
 def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
     # fused slice kernel with 1, 2, 4 CTAs per slice and the register-FFT slice
-    # kernel on 1 (8), 2 (9) and 4 (10) CTAs per slice, where they are built, against
-    # the three-kernel split pass;
+    # kernel on 1 (8), 2 (9) and 4 (10) CTAs per slice, and its 4-CTA form with
+    # 16 x 16 row transforms (11), where they are built, against the three-kernel
+    # split pass;
     # the flux preparation rides in the fused launches, so P(E) is compared too
     n1, n2, nth = shape
     base = S.build_case("f+h2", n1, n2, nth, m=nth - 1, total_steps=8, n_energies=5,
                         n_gradient_points=5, r=(0.5, 9.0))
     out = {}
-    for cl in ("0", "1", "2", "4", "8", "9", "10"):
+    for cl in ("0", "1", "2", "4", "8", "9", "10", "11"):
         monkeypatch.setenv("QD_SLICE_CLUSTER", cl)
         d = S.copy_case(base)
         d.options.precision = QD_PREC_FP32
@@ -260,7 +261,8 @@ def test_fp32_l_space_pass_variants_agree(shape, monkeypatch):
 
 
 @pytest.mark.parametrize("shape,kind", [((64, 64, 32), "8"), ((128, 96, 64), "8"),
-                                        ((128, 96, 64), "9"), ((256, 192, 16), "10")])
+                                        ((128, 96, 64), "9"), ((256, 192, 16), "10"),
+                                        ((256, 192, 16), "11")])
 def test_fp32_register_fft_slice_batch_matches_fp64(shape, kind, monkeypatch):
     # the register-FFT slice kernel (one CTA, or a 2- or 4-CTA cluster per slice) on
     # a 3-run batch (flux preparation in its extra CTAs) against the FP64
