@@ -54,6 +54,7 @@
 // in the status word, releases its TMEM and returns.
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include <cuda_fp16.h>
 #include "qd.h"
@@ -838,23 +839,38 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
   // Q[k][l] = sqrt(w_k) sqrt(l+1/2) L[l][k] per angular set; the transform pair
   // is an isometry per grid column when Q has orthonormal columns, and GEMM2
   // then also forms an orthonormal completion of them (modified Gram-Schmidt
-  // against the unit vectors, twice) so that its output norm is exact.
+  // against the unit vectors, twice) so that its output norm is exact.  The
+  // sets are independent: each is built on a host thread of its own.
   std::vector<std::vector<double>> Q(nsets), Qx(nsets);
-  bool renorm = true;
-  for (int t = 0; t < nsets; t++) {
+  std::vector<double> sw(nth), sl(nl > nth ? nl : nth);
+  for (int k = 0; k < nth; k++) sw[k] = std::sqrt(w[k]);
+  for (size_t l = 0; l < sl.size(); l++) sl[l] = std::sqrt(l + 0.5);
+  std::vector<char> set_ok(nsets, 1);
+  auto build_set = [&](int t) {
     const int m = nl_set[t];
     Q[t].assign((size_t)nth * m, 0.0);
-    for (int k = 0; k < nth; k++)
-      for (int l = 0; l < m; l++)
-        Q[t][(size_t)l * nth + k] = std::sqrt(w[k]) * std::sqrt(l + 0.5) * leg[t][l + (long)k * m];
-    if (m > nth) { renorm = false; continue; }
-    for (int l = 0; l < m && renorm; l++)
-      for (int l2 = 0; l2 < m; l2++) {
-        double g = 0.0;
-        for (int k = 0; k < nth; k++) g += Q[t][(size_t)l * nth + k] * Q[t][(size_t)l2 * nth + k];
-        if (std::fabs(g - (l == l2 ? 1.0 : 0.0)) > 1e-9) { renorm = false; break; }
+    for (int l = 0; l < m; l++)
+      for (int k = 0; k < nth; k++)
+        Q[t][(size_t)l * nth + k] = sw[k] * sl[l] * leg[t][l + (long)k * m];
+    if (m > nth) { set_ok[t] = 0; return; }
+    // the Gram matrix (symmetric: l2 >= l), four partial sums per entry
+    for (int l = 0; l < m; l++) {
+      const double *ql = Q[t].data() + (size_t)l * nth;
+      for (int l2 = l; l2 < m; l2++) {
+        const double *qm = Q[t].data() + (size_t)l2 * nth;
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+        int k = 0;
+        for (; k + 4 <= nth; k += 4) {
+          g0 += ql[k] * qm[k];
+          g1 += ql[k + 1] * qm[k + 1];
+          g2 += ql[k + 2] * qm[k + 2];
+          g3 += ql[k + 3] * qm[k + 3];
+        }
+        for (; k < nth; k++) g0 += ql[k] * qm[k];
+        const double g = (g0 + g1) + (g2 + g3);
+        if (std::fabs(g - (l == l2 ? 1.0 : 0.0)) > 1e-9) { set_ok[t] = 0; return; }
       }
-    if (!renorm) continue;
+    }
     std::vector<double> basis = Q[t];                // columns, each nth long
     int have = m;
     for (int c = 0; c < nth && have < nth; c++) {
@@ -873,9 +889,18 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
       for (int k = 0; k < nth; k++) basis.push_back(v[k] * nv);
       have++;
     }
-    if (have < nth) renorm = false;
-    Qx[t] = basis;                                     // nth columns: Q, then the completion
-  }
+    if (have < nth) set_ok[t] = 0;
+    Qx[t] = std::move(basis);                         // nth columns: Q, then the completion
+  };
+  auto each_set = [&](auto &&fn) {
+    std::vector<std::thread> th;
+    for (int t = 1; t < nsets; t++) th.emplace_back(fn, t);
+    fn(0);
+    for (auto &x : th) x.join();
+  };
+  each_set(build_set);
+  bool renorm = true;
+  for (int t = 0; t < nsets; t++) renorm = renorm && set_ok[t];
   // one image pair per set: row k (< n_theta) holds Q[k][l] times 2^12 for the
   // orders GEMM2 forms (the stored ones and, with renormalisation, the
   // completion up to n_theta), split into FP16 hi and lo parts
@@ -891,14 +916,14 @@ int tc_plan_create(TcPlan &plan, int nth, int nl, int nsets, const double *const
     std::memcpy(im + off, &h, 2);
     std::memcpy(im + bb + off, &l, 2);
   };
-  for (int t = 0; t < nsets; t++) {
+  each_set([&](int t) {
     unsigned char *b1 = img.data() + t * set_bytes;
     const int m = nl_set[t];
     const int cols = renorm ? nth : m;                   // output orders formed by GEMM2
     const std::vector<double> &q2 = renorm ? Qx[t] : Q[t];
     for (int k = 0; k < nth; k++)
       for (int l = 0; l < cols; l++) put(b1, k, l, q2[(size_t)l * nth + k]);
-  }
+  });
   // from the device's stream-ordered pool, like the handle's other buffers;
   // a copy from pageable memory has read `img` when it returns
   void *d = nullptr;

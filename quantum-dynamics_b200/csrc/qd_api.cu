@@ -242,61 +242,81 @@ class Staging {
   static constexpr size_t CHUNK = size_t(32) << 20;   // bytes per staging buffer
   static constexpr int NBUF = 4;
   static constexpr size_t LARGE = size_t(4) << 20;    // transfers from this size on use it
-  static constexpr size_t CHECK_STAGED = size_t(64) << 20;   // inputs checked while staged
 
   static Staging &get()
   {
     static Staging s;
     return s;
   }
-  // host -> device; *finite (if given) = no word of src is NaN/Inf.  The
-  // staging buffers are taken in turn across calls, so the host copy of one
-  // call's first chunk overlaps the transfer of the previous call's last.
-  cudaError_t upload(void *dst, const void *src, size_t bytes, cudaStream_t st, bool *finite)
+  // an upload of `bytes` goes through the staging buffers, so upload() checks
+  // its words while it copies them (inputs that are not staged are checked
+  // before any device work)
+  bool staged(size_t bytes)
   {
-    if (finite) *finite = true;
     std::lock_guard<std::mutex> lock(mu_);
-    if (bytes < LARGE || !ready()) {
-      if (finite) *finite = all_finite(static_cast<const double *>(src), bytes / 8);
-      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
-    }
-    bool ok_all = true;
-    for (size_t off = 0; off < bytes; off += CHUNK) {
-      const int b = (int)(next_++ % NBUF);
-      cudaError_t e = cudaEventSynchronize(ev_[b]);     // the buffer's last transfer is done
-      if (e != cudaSuccess) return e;
-      const size_t n = std::min(CHUNK, bytes - off);
-      ok_all = copy_scan(buf_[b], static_cast<const char *>(src) + off, n, finite != nullptr) &&
-               ok_all;
-      e = cudaMemcpyAsync(static_cast<char *>(dst) + off, buf_[b], n, cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
-      if (e != cudaSuccess) return e;
-    }
-    if (finite) *finite = ok_all;
-    return cudaSuccess;
+    return bytes >= LARGE && ready();
   }
-  // host doubles -> device floats (rounded to nearest), staged like upload; the
-  // doubles are checked on the way: *in_range = none is NaN/Inf or beyond the
-  // FP32 range
-  cudaError_t upload_narrow(float *dst, const double *src, size_t n, cudaStream_t st,
-                            bool *in_range)
+  // One host array of doubles for upload(): copied as doubles (their words
+  // checked for NaN/Inf when `check`), or rounded to floats (`narrow`: always
+  // checked for NaN, Inf and values beyond the FP32 range).
+  struct Up {
+    void *dst;            // device
+    const double *src;    // host
+    size_t n;             // doubles
+    bool narrow = false;
+    bool check = false;
+  };
+  // host -> device of several arrays as one stream of whole staging buffers
+  // (a buffer holds the end of one array and the start of the next), so a
+  // batch of mid-size arrays moves in as few chunks as its bytes need;
+  // bad[i] = array i failed its check.  The staging buffers are taken in
+  // turn across calls, so the host copy of one call's first chunk overlaps
+  // the transfer of the previous call's last.
+  cudaError_t upload(const Up *pc, int np, cudaStream_t st, std::vector<char> &bad)
   {
-    *in_range = true;
+    bad.assign(np, 0);
     std::lock_guard<std::mutex> lock(mu_);
-    if (!ready()) return cudaErrorMemoryAllocation;
-    const size_t per = CHUNK / sizeof(float);    // doubles per staged chunk
-    bool ok_all = true;
-    for (size_t off = 0; off < n; off += per) {
+    if (!ready()) {
+      for (int i = 0; i < np; i++) {
+        if (pc[i].narrow) return cudaErrorMemoryAllocation;
+        if (pc[i].check && !all_finite(pc[i].src, pc[i].n)) bad[i] = 1;
+        cudaError_t e = cudaMemcpyAsync(pc[i].dst, pc[i].src, sizeof(double) * pc[i].n,
+                                        cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    }
+    int i = 0;
+    size_t done = 0;                             // doubles of array i already staged
+    while (i < np) {
       const int b = (int)(next_++ % NBUF);
-      cudaError_t e = cudaEventSynchronize(ev_[b]);
+      cudaError_t e = cudaEventSynchronize(ev_[b]);   // the buffer's last transfer is done
       if (e != cudaSuccess) return e;
-      const size_t m = std::min(per, n - off);
-      ok_all = narrow_copy(static_cast<float *>(buf_[b]), src + off, m) && ok_all;
-      e = cudaMemcpyAsync(dst + off, buf_[b], m * sizeof(float), cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ev_[b], st);
+      size_t co = 0;                             // bytes of the buffer in use
+      while (i < np) {
+        const size_t w = pc[i].narrow ? sizeof(float) : sizeof(double);
+        const size_t m = std::min(pc[i].n - done, (CHUNK - co) / w);
+        if (m == 0 && done < pc[i].n) break;     // the buffer is full
+        char *sb = static_cast<char *>(buf_[b]) + co;
+        const bool ok = pc[i].narrow ? narrow_copy(reinterpret_cast<float *>(sb), pc[i].src + done, m)
+                                     : copy_scan(sb, pc[i].src + done, m * w, pc[i].check);
+        if (!ok) bad[i] = 1;
+        if (m > 0) {
+          e = cudaMemcpyAsync(static_cast<char *>(pc[i].dst) + done * w, sb, m * w,
+                              cudaMemcpyHostToDevice, st);
+          if (e != cudaSuccess) return e;
+        }
+        done += m;
+        if (done == pc[i].n) {
+          i++;
+          done = 0;
+        }
+        co = (co + m * w + 63) & ~size_t(63);    // each part starts 64-byte aligned
+        if (co >= CHUNK) break;
+      }
+      e = cudaEventRecord(ev_[b], st);
       if (e != cudaSuccess) return e;
     }
-    *in_range = ok_all;
     return cudaSuccess;
   }
   // device -> host of one array; returns once dst holds the data
@@ -395,8 +415,9 @@ class Staging {
     if (!ok_) cudaGetLastError();
     return ok_;
   }
-  // memcpy over the host pool; with scan, also the NaN/Inf test of the
-  // copied words
+  // memcpy over the host pool, the stores streamed past the caches where the
+  // destination is 16-byte aligned (no read of the destination lines); with
+  // scan, also the NaN/Inf test of the copied words, on the loaded values
   static bool copy_scan(void *dst, const void *src, size_t n, bool scan)
   {
     HostPool &pool = HostPool::get();
@@ -406,10 +427,35 @@ class Staging {
     pool.run([&](unsigned t) {
       const size_t a = std::min(n, t * part), z = t + 1 == nt ? n : std::min(n, a + part);
       if (a >= z) return;
-      std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, z - a);
+      char *d = static_cast<char *>(dst) + a;
+      const char *s = static_cast<const char *>(src) + a;
+      const size_t len = z - a;
+      size_t i = 0;
+      uint64_t bad = 0;
+#ifdef __SSE2__
+      if ((reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+        constexpr uint64_t E = 0x7ff0000000000000ull;
+        for (; i + 64 <= len; i += 64) {
+          const __m128i *p = reinterpret_cast<const __m128i *>(s + i);
+          const __m128i v0 = _mm_loadu_si128(p), v1 = _mm_loadu_si128(p + 1);
+          const __m128i v2 = _mm_loadu_si128(p + 2), v3 = _mm_loadu_si128(p + 3);
+          __m128i *q = reinterpret_cast<__m128i *>(d + i);
+          _mm_stream_si128(q, v0);
+          _mm_stream_si128(q + 1, v1);
+          _mm_stream_si128(q + 2, v2);
+          _mm_stream_si128(q + 3, v3);
+          if (scan) {
+            uint64_t u[8];
+            std::memcpy(u, s + i, sizeof u);
+            for (int k = 0; k < 8; k++) bad |= (u[k] & E) == E;
+          }
+        }
+        _mm_sfence();
+      }
+#endif
+      std::memcpy(d + i, s + i, len - i);
       if (scan)
-        ok[t] = finite_words(reinterpret_cast<const double *>(static_cast<const char *>(dst) + a),
-                             (z - a) / 8);
+        ok[t] = bad == 0 && finite_words(reinterpret_cast<const double *>(d + i), (len - i) / 8);
     });
     return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
   }
@@ -653,11 +699,12 @@ int validate(const qd_data *d)
     return set_err(QD_ERR_INVALID, "centrifugal-sudden block J = %d, K = %d: need 0 <= K <= J",
                    d->cs.J, d->cs.K);
   const size_t npt = (size_t)n1 * n2 * nth;
-  // arrays of Staging::CHECK_STAGED bytes or more are checked while they are staged
-  // for the upload (create), smaller ones here
-  if (npt * sizeof(double) < Staging::CHECK_STAGED && !all_finite(d->pot, npt))
+  // arrays that the upload stages are checked while they are copied into the
+  // staging buffers (create), the others here; so every input word is read once
+  // for the check, and a process without a device checks them all here
+  if (!Staging::get().staged(npt * sizeof(double)) && !all_finite(d->pot, npt))
     return set_err(QD_ERR_NONFINITE, "pot contains NaN/Inf");
-  if (2 * npt * sizeof(double) < Staging::CHECK_STAGED && !all_finite(d->psi, 2 * npt))
+  if (!Staging::get().staged(2 * npt * sizeof(double)) && !all_finite(d->psi, 2 * npt))
     return set_err(QD_ERR_NONFINITE, "psi contains NaN/Inf");
   if (d->CRP.calculate_CRP) {
     const qd_crp &c = d->CRP;
@@ -1332,11 +1379,16 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   const int npot = shared_pot ? 1 : nruns;
   h->vrun = shared_pot ? 0 : npt;
   TRY(h->alloc(h->d_pot, npt * npot));
-  for (int r = 0; r < npot; r++) {
-    bool fin = true;
-    CU(Staging::get().upload(h->d_pot + r * npt, runs[r].pot, sizeof(double) * npt, h->st,
-                             sizeof(double) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
-    if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: pot contains NaN/Inf", r);
+  {
+    // the potentials (and below the wavepackets) of all runs as one staged
+    // stream; validate() has checked the arrays that are not staged
+    const bool chk = Staging::get().staged(sizeof(double) * npt);
+    std::vector<Staging::Up> up(npot);
+    for (int r = 0; r < npot; r++) up[r] = {h->d_pot + r * npt, runs[r].pot, (size_t)npt, false, chk};
+    std::vector<char> bad;
+    CU(Staging::get().upload(up.data(), npot, h->st, bad));
+    for (int r = 0; r < npot; r++)
+      if (bad[r]) return set_err(QD_ERR_NONFINITE, "run %d: pot contains NaN/Inf", r);
   }
   TRY(upload(h, h->d_w, d->theta.w, h->nth));
   // each set's legendre matrix padded to nl functions (zero rows beyond its own)
@@ -1435,24 +1487,27 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
   CU(cudaMemsetAsync(lp, 0, csz * h->n12 * h->nl * nruns, h->st));
   TRY(h->alloc(h->d_psi_z, npt * nruns));
   if (f64) {
-    for (int r = 0; r < nruns; r++) {
-      bool fin = true;
-      CU(Staging::get().upload(h->d_psi_z + r * npt, runs[r].psi, sizeof(double2) * npt, h->st,
-                               sizeof(double2) * npt >= Staging::CHECK_STAGED ? &fin : nullptr));
-      if (!fin) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
-    }
+    const bool chk = Staging::get().staged(sizeof(double2) * npt);
+    std::vector<Staging::Up> up(nruns);
+    for (int r = 0; r < nruns; r++)
+      up[r] = {h->d_psi_z + r * npt, runs[r].psi, 2 * (size_t)npt, false, chk};
+    std::vector<char> bad;
+    CU(Staging::get().upload(up.data(), nruns, h->st, bad));
+    for (int r = 0; r < nruns; r++)
+      if (bad[r]) return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf", r);
   } else {
     // complex64 form: psi rounded to complex64 by the host threads that stage it
     // (half the bytes over the bus), then widened into the FP64 staging array
     TRY(h->alloc(h->d_psi32, npt * nruns));
-    for (int r = 0; r < nruns; r++) {
-      bool ok = true;
-      CU(Staging::get().upload_narrow(reinterpret_cast<float *>(h->d_psi32 + r * npt),
-                                      runs[r].psi, 2 * (size_t)npt, h->st, &ok));
-      if (!ok)
+    std::vector<Staging::Up> up(nruns);
+    for (int r = 0; r < nruns; r++)
+      up[r] = {h->d_psi32 + r * npt, runs[r].psi, 2 * (size_t)npt, true, true};
+    std::vector<char> bad;
+    CU(Staging::get().upload(up.data(), nruns, h->st, bad));
+    for (int r = 0; r < nruns; r++)
+      if (bad[r])
         return set_err(QD_ERR_NONFINITE, "run %d: psi contains NaN/Inf or values beyond the "
                        "complex64 range", r);
-    }
     CU(launch_widen_c(h->d_psi32, h->d_psi_z, (size_t)npt * nruns, h->st));
     g_launches++;
   }

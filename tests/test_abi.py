@@ -10,7 +10,7 @@ import pytest
 
 from conftest import REPO, GOLDEN, have_gpu
 from qd_b200 import _abi, systems as S
-from qd_b200.timeevolution import TimeEvolutionMexCUDA
+from qd_b200.timeevolution import TimeEvolutionMexCUDA, _c_runs
 
 
 def header_functions():
@@ -85,12 +85,17 @@ def test_nonfinite_found_in_large_inputs(qdlib, where):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("where", ["pot", "psi"])
-def test_nonfinite_found_while_staging_large_inputs(qdlib, where):
-    # arrays of 64 MiB or more are checked while they are copied into the
-    # page-locked staging buffers of the upload
-    d = S.build_case("h+h2", 256, 256, 128, m=63, total_steps=1, n_energies=5,
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("shape", [(128, 128, 64), (256, 256, 128)])
+def test_nonfinite_found_while_staging_large_inputs(qdlib, where, prec, shape):
+    # arrays of 4 MiB or more are checked while they are copied into the
+    # page-locked staging buffers of the upload (one staging buffer's worth and
+    # several), in both precisions
+    n1, n2, nth = shape
+    d = S.build_case("h+h2", n1, n2, nth, m=63, total_steps=1, n_energies=5,
                      n_gradient_points=5)
-    assert d.pot.nbytes >= 64 << 20
+    d.options.precision = prec
+    assert d.pot.nbytes >= 4 << 20
     if where == "pot":
         d.pot[-1, -1, -3] = np.inf
     else:
@@ -99,6 +104,21 @@ def test_nonfinite_found_while_staging_large_inputs(qdlib, where):
     h = C.c_void_p()
     assert qdlib.qd_create(C.byref(c), C.byref(h)) == _abi.QD_ERR_NONFINITE
     assert where.encode() in qdlib.qd_last_error()
+    assert not h.value
+
+
+@pytest.mark.gpu
+def test_nonfinite_found_in_one_run_of_a_batch(qdlib):
+    # a batch whose third run carries a NaN in its potential: create reports that run
+    d = S.build_case("h+h2", 128, 128, 64, m=63, total_steps=1, n_energies=5,
+                     n_gradient_points=5)
+    runs = [S.copy_case(d) for _ in range(4)]
+    runs[2].pot = d.pot.copy()                  # copy_case shares the potential
+    runs[2].pot[3, 5, 7] = np.nan
+    arr = _c_runs(runs)
+    h = C.c_void_p()
+    assert qdlib.qd_create_batch(arr, 4, C.byref(h)) == _abi.QD_ERR_NONFINITE
+    assert b"run 2" in qdlib.qd_last_error()
     assert not h.value
 
 

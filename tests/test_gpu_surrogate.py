@@ -106,10 +106,16 @@ def test_surrogate_against_the_plain_surfaces():
     with Surrogate(seed=10) as sur:
         sur.fit(r12, r23, r13, V, steps=300, lr=3e-3, lr_end=1e-3)
         sur.potential(R, r, x, MASSES)                   # warm-up
-        t_mlp, g = _best_of(lambda: sur.potential(R, r, x, MASSES))
+        potential_leps_gpu(R, r, x, MASSES, pes)
+        # the two GPU grids timed in turn, so that both see the same load of
+        # the shared host (their host copies are most of either time)
+        t_mlp = t_leps = 1e30
+        for _ in range(5):
+            t, g = _best_of(lambda: sur.potential(R, r, x, MASSES), n=1)
+            t_mlp = min(t_mlp, t)
+            t, pl = _best_of(lambda: potential_leps_gpu(R, r, x, MASSES, pes), n=1)
+            t_leps = min(t_leps, t)
     t_host, p = _best_of(lambda: potential_jacobi(R, r, x, MASSES, pes))
-    potential_leps_gpu(R, r, x, MASSES, pes)
-    t_leps, pl = _best_of(lambda: potential_leps_gpu(R, r, x, MASSES, pes))
     tables = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "hsw_tables.npz")))
     hsw = HswSurface(tables=tables)
     hsw.potential(R, r, x, MASSES)
