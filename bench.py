@@ -341,11 +341,30 @@ def device_phase(data, prec, K, W, clk=None, profile=True):
             lib.qd_set_profiling(p._h, 0)
             kc = list(buf)[:nw.value]
             out["kclass_ms"] = {KCLASS[i]: kc[i] for i in range(min(5, len(kc)))}
+            ch = (C.c_int32 * 4)()
+            lib.qd_kernel_choice(p._h, ch)
+            out["choice"] = list(ch)
             t0 = time.perf_counter()
             p.propagate(K)
             out["plain_s"] = time.perf_counter() - t0
             out["ms_warm"] = p.propagate_timed(K, 0)
     return out
+
+
+SLICE_KINDS = {0: "split row and column kernels", 1: "Stockham cluster kernel, 1 CTA per slice",
+               2: "Stockham cluster kernel, 2-CTA clusters", 4: "Stockham cluster kernel, 4-CTA clusters",
+               8: "register-FFT kernel k_slice_rf, 1 CTA per slice",
+               9: "register-FFT kernel k_slice_rf, 2-CTA clusters",
+               10: "register-FFT kernel k_slice_rf, 4-CTA clusters",
+               11: "register-FFT kernel k_slice_rf, 4-CTA clusters, 16x16 row transforms"}
+
+
+def describe_choice(ch, fp64):
+    """The autotuners' picks for the timed handle (qd_kernel_choice)."""
+    return {"l_space": "FP64 split kernels" if fp64 else SLICE_KINDS.get(ch[0], str(ch[0])),
+            "column": "tensor cores (k_column_tc, tcgen05 kind::f16)" if ch[1] else "SIMT",
+            "flux_gemm_variant": ch[2],
+            "flux_full_chunks": "chirp-z (k_flux_czt)" if ch[3] else "direct GEMM (k_flux_gemm)"}
 
 
 def roofline_entry(name, alg_bytes, ms, peak, peak_kind, traffic):
@@ -464,6 +483,8 @@ def run_ours(args):
                                                           "alg_bytes_per_launch", "traffic")}
                            for k in kernels}
     roofline["kernel_class_ms"] = per
+    if dev.get("choice"):
+        roofline["tuned"] = describe_choice(dev["choice"], args.fp64)
     step_ms = t_max / K
     step_bytes = 36 if not args.fp64 else 72
     roofline["whole_step"] = {"alg_bytes_per_grid_pt_step": step_bytes,

@@ -229,6 +229,15 @@ int qd_steps(qd_handle *h, int32_t *steps_out);
  * qd_propagate call when profiling is enabled via qd_set_profiling(h, 1). */
 int qd_set_profiling(qd_handle *h, int32_t on);
 int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written);
+/* The kernels this handle's autotuners picked (the choice is kept per shape
+ * for the process): out[0] = the complex64 l-space kernel (0 the split row and
+ * column kernels, 1/2/4 the Stockham cluster kernel on that many CTAs per
+ * slice, 8/9/10 the register-FFT kernel on 1/2/4 CTAs per slice, 11 its 4-CTA
+ * form with 16 x 16 row transforms; 0 for the FP64 form), out[1] = 1 if the
+ * column pass runs on the tensor cores, out[2] = the flux-accumulation GEMM
+ * tile variant (0-3), out[3] = 1 if full 250-step chunks of flux history are
+ * accumulated in the chirp-z form (energies on a uniform grid). */
+int qd_kernel_choice(qd_handle *h, int32_t out[4]);
 
 /* Checkpoint / restart of the full propagation state: the l-space
  * wavepacket, time.steps, the flux accumulators phi_E, dphi_E and the

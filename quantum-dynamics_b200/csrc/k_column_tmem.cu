@@ -605,17 +605,30 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
       }
       put_row<H>(my_hi, my_lo, dv, slow ? exp2i(A_LOG2 - pe) : exp2i(-B_LOG2));
     } else if (mode == COL_HEAD) {              // psi_z -> theta' values
+      // eight values' loads are issued before their arithmetic, so that their
+      // latencies overlap
+      constexpr int GV = H % 8 == 0 ? 8 : 4;          // H is a multiple of 4
+      const double2 *zr = p.psi_z + (size_t)run * nth * n12 + q;
+      const float2 *fr = expv + voff + q;
 #pragma unroll
-      for (int u = 0; u < H; u++) {
-        const int k = c0 + u;
-        float val = 0.f;
-        if (qok && k < nth) {
-          const size_t g = (size_t)k * n12 + q;
-          const double2 z = p.psi_z[(size_t)run * nth * n12 + g];
+      for (int u0 = 0; u0 < H; u0 += GV) {
+        double2 z[GV];
+        float2 fv[GV];
+        double wv[GV];
+#pragma unroll
+        for (int v = 0; v < GV; v++) {
+          const int k = c0 + u0 + v;
+          const bool ok = qok && k < nth;
+          z[v] = ok ? __ldg(zr + (size_t)k * n12) : make_double2(0.0, 0.0);
+          fv[v] = ok ? __ldg(fr + (size_t)k * n12) : make_float2(1.f, 0.f);
+          wv[v] = ok ? __ldg(p.w + k) : 0.0;
+        }
+#pragma unroll
+        for (int v = 0; v < GV; v++) {
           // exp(-i V dt) from the step's own complex64 table; the first step of
           // a run takes its principal square root (psi / sqrt(v) * v), by the
           // half-angle formulas in the form without cancellation
-          float2 f = expv[voff + g];
+          float2 f = fv[v];
           if (p.prestep) {
             if (f.x >= 0.f) {
               const float ch = sqrtf(0.5f * (1.f + f.x));
@@ -625,10 +638,12 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
               f = make_float2(f.y / (2.f * sh), sh);
             }
           }
-          val = (float)((is_im ? z.x * f.y + z.y * f.x : z.x * f.x - z.y * f.y) * sqrt(p.w[k]));
+          const double2 zz = z[v];
+          const float val = (float)((is_im ? zz.x * f.y + zz.y * f.x : zz.x * f.x - zz.y * f.y) *
+                                    sqrt(wv[v]));
+          dv[u0 + v] = val;
+          tsum = fmaf(val, val, tsum);
         }
-        dv[u] = val;
-        tsum = fmaf(val, val, tsum);
       }
     }
     // target norm of the column output (and the step norm of the point)

@@ -1932,6 +1932,16 @@ int qd_set_profiling(qd_handle *h, int32_t on)
   return QD_OK;
 }
 
+int qd_kernel_choice(qd_handle *h, int32_t out[4])
+{
+  if (!h || !out) return set_err(QD_ERR_INVALID, "NULL argument");
+  out[0] = h->slice_cluster;
+  out[1] = h->use_tc ? 1 : 0;
+  out[2] = h->flux_variant;
+  out[3] = h->d_czt_b ? 1 : 0;
+  return QD_OK;
+}
+
 int qd_kernel_times(qd_handle *h, double *ms_out, int32_t n, int32_t *n_written)
 {
   if (!h || !n_written) return set_err(QD_ERR_INVALID, "NULL argument");

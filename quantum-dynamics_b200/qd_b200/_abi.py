@@ -193,6 +193,7 @@ def lib():
         "qd_steps": (C.c_int, [H, P(C.c_int32)]),
         "qd_set_profiling": (C.c_int, [H, C.c_int32]),
         "qd_kernel_times": (C.c_int, [H, c_double_p, C.c_int32, P(C.c_int32)]),
+        "qd_kernel_choice": (C.c_int, [H, P(C.c_int32)]),
         "qd_checkpoint": (C.c_int, [H, C.c_char_p]),
         "qd_restore": (C.c_int, [H, C.c_char_p]),
         "qd_create_batch": (C.c_int, [P(QdData), C.c_int32, P(H)]),

@@ -108,6 +108,25 @@ def test_nonfinite_found_while_staging_large_inputs(qdlib, where, prec, shape):
 
 
 @pytest.mark.gpu
+def test_kernel_choice_reports_the_tuned_kernels(qdlib):
+    # a complex64 handle on a uniform energy grid: tensor-core column pass,
+    # a register-FFT or other built l-space kernel, chirp-z accumulation
+    from qd_b200 import Propagator
+    d = S.build_case("f+h2", 128, 96, 64, m=63, total_steps=2, n_energies=9,
+                     n_gradient_points=5)
+    d.options.precision = 1
+    with Propagator(d) as p:
+        p.propagate(2)
+        ch = (C.c_int32 * 4)()
+        assert qdlib.qd_kernel_choice(p._h, ch) == 0
+    assert ch[0] in (0, 1, 2, 4, 8, 9, 10, 11)
+    assert ch[1] == 1
+    assert 0 <= ch[2] < 4
+    assert ch[3] == 1
+    assert qdlib.qd_kernel_choice(None, ch) == _abi.QD_ERR_INVALID
+
+
+@pytest.mark.gpu
 def test_nonfinite_found_in_one_run_of_a_batch(qdlib):
     # a batch whose third run carries a NaN in its potential: create reports that run
     d = S.build_case("h+h2", 128, 128, 64, m=63, total_steps=1, n_energies=5,
