@@ -142,6 +142,27 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
         if (dst) *dst = acc[i][j];
       }
   }
+  if (p.crp_part) {
+    // this tile's share of P(E): sum over its points of w_k Im(conj(phi) dphi)
+    // of the updated values (columns j and j + 2 of a thread are phi and dphi
+    // of one point; entries past n_E or past the surface are zero), reduced
+    // over the 16 column groups of each energy row
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      double sum = 0.0;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int q = q0 + tc + 16 * j;
+        if (q < p.nq)
+          sum += p.w[q / p.n1] * (acc[i][j].x * acc[i][j + 2].y - acc[i][j].y * acc[i][j + 2].x);
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      const int e = e0 + te + (GE / 4) * i;
+      if (tc == 0 && e < p.ne)
+        p.crp_part[((size_t)run * p.ne + e) * gridDim.y + blockIdx.y] = sum;
+    }
+  }
 }
 
 // ---- chirp-z form of the accumulation, for energies on a uniform grid ------------------
@@ -346,6 +367,18 @@ __global__ void __launch_bounds__(256) k_crp(CrpParams p)
   if (threadIdx.x == 0) p.crp[b] = s / p.eta_sq[b] * p.dr1_mu2;
 }
 
+// P(E) from the per-tile sums of a fused accumulation, in a fixed order
+__global__ void __launch_bounds__(256) k_crp_parts(CrpParams p, const double *part, int nqt)
+{
+  __shared__ double red[32];
+  const int b = blockIdx.x;                    // run * ne + e
+  const double *pp = part + (size_t)b * nqt;
+  double s = 0.0;
+  for (int x = threadIdx.x; x < nqt; x += blockDim.x) s += pp[x];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) p.crp[b] = s / p.eta_sq[b] * p.dr1_mu2;
+}
+
 template <int GE, int KT> void launch_gemm(const AccumParams &p, cudaStream_t s)
 {
   dim3 grid((p.ne + GE - 1) / GE, (p.nq + GQ - 1) / GQ, p.nruns);
@@ -366,11 +399,18 @@ template cudaError_t launch_flux_prep<double>(const FluxParams &, cudaStream_t);
 
 int flux_variants() { return 4; }
 
+bool flux_accum_is_czt(const AccumParams &p)
+{
+  return p.czt_b && p.nt >= CZT_MIN_STEPS && p.ne <= CZT_N - TMAX + 1;
+}
+
+int flux_q_tiles(int nq) { return (nq + GQ - 1) / GQ; }
+
 cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 {
   if (p.nt <= 0) return cudaSuccess;
   if (p.nt > TMAX) return cudaErrorInvalidValue;
-  if (p.czt_b && p.nt >= CZT_MIN_STEPS && p.ne <= CZT_N - TMAX + 1) {   // chirp-z form
+  if (flux_accum_is_czt(p)) {                                   // chirp-z form
     static bool attr = false;
     const size_t sm = czt_smem();
     if (!attr) {
@@ -401,6 +441,12 @@ cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s)
 cudaError_t launch_crp(const CrpParams &p, cudaStream_t s)
 {
   k_crp<<<p.nruns * p.ne, 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crp_parts(const CrpParams &p, const double *part, int nqt, cudaStream_t s)
+{
+  k_crp_parts<<<p.nruns * p.ne, 256, 0, s>>>(p, part, nqt);
   return cudaGetLastError();
 }
 

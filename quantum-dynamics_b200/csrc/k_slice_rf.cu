@@ -52,9 +52,10 @@
 // one transpose between them is a set of bulk shared-memory-to-shared-memory
 // copies of whole row halves, so no pass touches the other CTA's memory
 // itself.  A 256 x 192 slice (384 KB) runs on a 4-CTA cluster, a quarter of
-// the rows and of the columns per CTA; its transpose swaps row parts between
-// the CTAs in place (registers, cluster barrier, remote stores), so each CTA
-// holds only its own 101 KB of rows and two clusters' CTAs share an SM.
+// the rows and of the columns per CTA; its transpose is folded into the last
+// row pass, which stores each result into the CTA whose columns it belongs to
+// (rounds of rows between cluster barriers), so each CTA holds only its own
+// 101 KB of rows and two clusters' CTAs share an SM.
 //
 // The 6-, 12-, 16-, 24- and 32-point DFTs are P x Q compositions whose
 // internal twiddles are compensated constants (value + residual), like the
@@ -241,7 +242,6 @@ template <int N1, int N2, int NT, int CL, int A1X = 0> struct RfShape {
   static constexpr bool SWAP = CL == 4;
   static constexpr int PSLOTS = CL == 1 || SWAP ? 0 : CL - 1;
   static constexpr int P1_UNROLL = 2;                // row items per thread loaded together
-  static constexpr int SWAP_ROUNDS = 6;              // row rounds of the in-place transpose (1, 2, 4, 6, 8, 12 measured: 6 best)
   // own rows [HR][RS]; CL = 2: the peer's rows of this CTA's column part
   // [HR][HW]; rc1[l], kc1 (N1 each), W_N2, kc2, rc2[l] (N2 each); CL = 2:
   // one mbarrier
@@ -294,75 +294,65 @@ __device__ __forceinline__ bool mbar_wait0(uint32_t mbar)
   return false;
 }
 
-// st.shared::cluster of 16 bytes (a mapa address)
-__device__ __forceinline__ void st_peer4(uint32_t a, float4 v)
+// st.shared::cluster of 8 bytes (a mapa address)
+__device__ __forceinline__ void st_peer2(uint32_t a, float2 v)
 {
-  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};"
-               :: "r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" :: "r"(a), "f"(v.x), "f"(v.y) : "memory");
 }
 
-// The in-place transpose of a CL-CTA slice: for every peer o, row part o of
-// this CTA's rows and row part `rank` of o's rows trade places (the same
-// rows j, the same HW-complex columns in both row arrays), so afterwards row
-// part o of the array holds the rows of CTA o in this CTA's column part;
-// called again it undoes itself.  NR rounds of HR / NR rows each: every
-// thread reads its share of the round's row parts into registers, the
-// cluster barrier guarantees that every CTA has read them, and the values
-// are stored into the peers' arrays; the rows of one round are disjoint
-// from the others', so only the final barrier orders the last round's
-// stores before the following passes.
-template <int NT, int CL, int HR, int HW, int RS, int NR>
-__device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
+// Pc fused with the in-place transpose of a CL-CTA slice.  In rounds of whole
+// rows, one item (j, a) per thread: the thread loads slot a of every block of
+// row j, arrives on the cluster barrier once the values are in its registers,
+// runs the inverse row pass (W^{-a c}, B1-point inverse DFT over c, D1) while
+// the other CTAs arrive, waits, and stores each result where the column passes
+// read it: block b of row j lies in column part o = b / (B1 / CL), which CTA o
+// holds as row part `rank` of its row j, in CTA o's column part.  Every CTA has read a round's rows before any CTA writes into them,
+// the rounds' rows are disjoint, and the closing barrier (release, acquire)
+// makes every store visible to the column passes.
+template <int A1, int B1, int RS, int HR, int HW, int NT, int CL>
+__device__ __forceinline__ void pc_swap(float2 *R, const float2 *r1, const float2 *tw1, int rank,
+                                        int tid)
 {
-  constexpr int XW = HW / 2;                          // float4 per row part
-  constexpr int HALF = HR / NR;                       // rows per round
-  constexpr int PER = (CL - 1) * HALF * XW;           // float4 of one round
-  constexpr int F = (PER + NT - 1) / NT;              // per thread
-  static_assert(HW % 2 == 0 && RS % 2 == 0 && HR % NR == 0, "16-byte row parts, whole rows");
-  float4 *R4 = reinterpret_cast<float4 *>(R);
+  constexpr int BPP = B1 / CL;                        // row blocks per column part
+  constexpr int NRF = HR * A1 / NT;                   // rounds: one item per thread each
+  constexpr int RPR = HR / NRF;                       // rows per round
+  static_assert(NRF >= 1 && NRF * NT == HR * A1 && HR % NRF == 0 && NT % A1 == 0,
+                "one item per thread and round, whole rows per round");
+  static_assert(HW == BPP * (A1 + 1), "column parts of whole row blocks");
+  const int a = tid % A1;
+  float2 w[B1];
+#pragma unroll
+  for (int c = 0; c < B1; c++) w[c] = cconj(__ldg(tw1 + a * c));
+  uint32_t rb[CL];                                    // the row array in each CTA of the cluster
+#pragma unroll
+  for (int o = 0; o < CL; o++) rb[o] = peer_addr(smem_addr(R), (uint32_t)o);
+  __shared__ uint32_t sink;                           // a store that reads every loaded value
 #pragma unroll 1
-  for (int r = 0; r < NR; r++) {
-    float4 v[F];
+  for (int r = 0; r < NRF; r++) {
+    const int j = r * RPR + tid / A1;
+    float2 v[B1];
+    uint32_t dep = 0;
 #pragma unroll
-    for (int k = 0; k < F; k++) {
-      const int e = k * NT + tid;
-      if (e < PER) {
-        const int pi = e / (HALF * XW), rem = e % (HALF * XW);
-        const int j = r * HALF + rem / XW, x = rem % XW;
-        const int peer = pi < rank ? pi : pi + 1;
-        v[k] = R4[(j * RS + HW * peer) / 2 + x];
-      }
+    for (int c = 0; c < B1; c++) {
+      v[c] = R[j * RS + a + (A1 + 1) * c];
+      dep |= __float_as_uint(v[c].x) | __float_as_uint(v[c].y);
     }
-    // every CTA has read this round's rows before any is overwritten.  Round 0
-    // also publishes the row passes' writes (release); later rounds only need
-    // this thread's loads to have returned, which a store of a value computed
-    // from all of them, ahead of a relaxed arrive, guarantees (their rows were
-    // published by round 0, and the stores of round r - 1 touch other rows)
-    if (r == 0) {
-      cluster_arrive_release();
-    } else {
-      uint32_t dep = 0;
+    asm volatile("st.shared.u32 [%0], %1;\n\tbarrier.cluster.arrive.relaxed.aligned;"
+                 :: "r"(smem_addr(&sink)), "r"(dep) : "memory");
 #pragma unroll
-      for (int k = 0; k < F; k++)
-        dep |= __float_as_uint(v[k].x) | __float_as_uint(v[k].y) | __float_as_uint(v[k].z) |
-               __float_as_uint(v[k].w);
-      __shared__ uint32_t sink;                      // a store that reads every loaded value
-      asm volatile("st.shared.u32 [%0], %1;\n\tbarrier.cluster.arrive.relaxed.aligned;"
-                   :: "r"(smem_addr(&sink)), "r"(dep) : "memory");
-    }
+    for (int c = 1; c < B1; c++) v[c] = cmul(v[c], w[c]);
+    Dft<B1, +1>::run(v);
+#pragma unroll
+    for (int b = 0; b < B1; b++) v[b] = cmul(v[b], r1[a + A1 * b]);
     cluster_wait();
 #pragma unroll
-    for (int k = 0; k < F; k++) {
-      const int e = k * NT + tid;
-      if (e < PER) {
-        const int pi = e / (HALF * XW), rem = e % (HALF * XW);
-        const int j = r * HALF + rem / XW, x = rem % XW;
-        const int peer = pi < rank ? pi : pi + 1;
-        st_peer4(peer_addr(smem_addr(R4 + (j * RS + HW * rank) / 2 + x), (uint32_t)peer), v[k]);
-      }
+    for (int b = 0; b < B1; b++) {
+      const int o = b / BPP;
+      st_peer2(rb[o] + (uint32_t)sizeof(float2) * (j * RS + HW * rank + a + (A1 + 1) * (b - o * BPP)),
+               v[b]);
     }
   }
-  cluster_arrive_release();                          // every CTA's incoming rows are in
+  cluster_arrive_release();
   cluster_wait();
 }
 
@@ -372,10 +362,10 @@ __device__ __forceinline__ void swap_parts(float2 *R, int rank, int tid)
 // rank N1/CL .. (rank+1) N1/CL - 1) over all N2 rows.  CL = 2: its own rows
 // in place in its row array, the peer's rows in a second array, filled after
 // Pc by bulk copies of whole row halves (544 bytes) from the peer (an
-// mbarrier in the receiving CTA counts the bytes in).  CL = 4: the in-place
-// swap of swap_parts, after which row part o of the row array holds CTA o's
-// rows in this CTA's column part.  Every load and store of the passes is
-// local.  CL = 1 keeps the slice in one array in place.
+// mbarrier in the receiving CTA counts the bytes in).  CL = 4: Pc stores its
+// results into the CTA that holds their column part (pc_swap), after which row
+// part o of the row array holds CTA o's rows in this CTA's column part.  Every
+// load and store of the other passes is local.  CL = 1 keeps the slice in one array in place.
 template <int N1, int N2, int NT, int CL, int A1X>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
@@ -479,8 +469,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   __syncthreads();
   // Pc: items (j, a): slot a of every block c, W^{-a c}, B1-point inverse DFT
-  // over c -> element i = a + A1 b, D1 -> slot a of block b (the same slots)
-  {
+  // over c -> element i = a + A1 b, D1 -> slot a of block b (the same slots);
+  // CL = 4: fused with the transpose (pc_swap)
+  if constexpr (!Sh::SWAP) {
     const int a = tid % A1;
     float2 w[B1];
 #pragma unroll
@@ -500,8 +491,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   bool ok = true;
   if constexpr (Sh::SWAP) {
-    __syncthreads();
-    swap_parts<NT, CL, HR, HW, RS, Sh::SWAP_ROUNDS>(R, rank, tid);
+    pc_swap<A1, B1, RS, HR, HW, NT, CL>(R, r1, tw1, rank, tid);
   } else if constexpr (CL > 1) {
     // peer o's column part of every own row -> this CTA's slot of o's P array
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -582,6 +582,8 @@ struct qd_handle {
   double2 *d_czt_tw = nullptr, *d_czt_g = nullptr, *d_czt_b = nullptr;
   double *d_czt_de = nullptr;
   double *d_energies = nullptr, *d_eta = nullptr, *d_crp = nullptr;
+  double *d_crp_part = nullptr;   // [run][energy][surface-point tile]: fused P(E) sums
+                                  // (null: P(E) by its own pass, QD_CRP_FUSED=0)
   double *d_norms = nullptr;
   int norms_cap = 0;
   TcPlan tc;                      // tensor-core column pass (FP32), if usable
@@ -1106,14 +1108,30 @@ int flush_accum(qd_handle *h)
 int compute_crp(qd_handle *h)
 {
   if (!h->do_crp || h->crp_valid) return QD_OK;
-  TRY(flush_accum(h));
+  // a pending partial chunk that the GEMM form accumulates also yields P(E):
+  // its epilogue sums w_k Im(conj(phi) dphi) of the values it writes per tile,
+  // which saves reading phi_E and dphi_E once more
+  bool fused = false;
+  if (h->ring_fill > 0 && h->d_crp_part) {
+    AccumParams a = accum_params(h);
+    if (!flux_accum_is_czt(a)) {
+      a.crp_part = h->d_crp_part; a.w = h->d_w; a.n1 = h->n1;
+      CU(launch_flux_accum(a, h->st));
+      g_launches += flux_accum_launches();
+      h->acc_done += h->ring_fill;
+      h->ring_fill = 0;
+      fused = true;
+    }
+  }
+  if (!fused) TRY(flush_accum(h));
   CrpParams c{};
   c.n1 = h->n1; c.nth = h->nth; c.ne = h->ne; c.w = h->d_w; c.eta_sq = h->d_eta;
   c.nruns = h->nruns;
   c.dr1_mu2 = h->data->r1.dr / h->data->r2.mass;
   c.fai = h->d_fai; c.dfai = h->d_dfai; c.crp = h->d_crp;
   TRY(prof_mark(h, -1));
-  CU(launch_crp(c, h->st));
+  if (fused) CU(launch_crp_parts(c, h->d_crp_part, flux_q_tiles(h->nth * h->n1), h->st));
+  else CU(launch_crp(c, h->st));
   g_launches++;
   TRY(prof_mark(h, PROF_CRP));
   h->crp_valid = true;
@@ -1532,6 +1550,9 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
                          sizeof(double) * h->ne, cudaMemcpyHostToDevice, h->st));
     }
     TRY(h->alloc(h->d_crp, (size_t)h->ne * nruns));
+    const char *cf = getenv("QD_CRP_FUSED");
+    if (!(cf && cf[0] == '0'))
+      TRY(h->alloc(h->d_crp_part, (size_t)h->ne * nruns * flux_q_tiles((int)nq)));
     // energies E_0 + j dE in every run (to a phase error below 1e-12 rad over a
     // chunk): the accumulation of full chunks takes the chirp-z form
     // (QD_FLUX_CZT=0 keeps the GEMM form)

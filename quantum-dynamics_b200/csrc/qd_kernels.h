@@ -195,6 +195,11 @@ struct AccumParams {
   const double2 *czt_g;    // [nruns][FLUX_CHUNK] e^{i E_0 t dt} c(t)
   const double2 *czt_b;    // [nruns][CZT_N] FFT of b_k = conj(c(k)), divided by CZT_N
   const double *czt_de;    // [nruns] energy spacing dE; c(k) = e^{i dE dt k^2 / 2}
+  // P(E) of the updated accumulators fused into the GEMM form (null: off):
+  // crp_part[run][e][q tile] = the tile's sum of w_k Im(conj(phi) dphi)
+  double *crp_part;
+  const double *w;         // theta weights (with crp_part)
+  int n1;                  // surface points per theta row (with crp_part)
 };
 constexpr int CZT_N = 512;       // cyclic convolution length of the chirp-z form
 constexpr int CZT_MIN_STEPS = 125;   // chunks of fewer steps take the GEMM form
@@ -203,6 +208,8 @@ cudaError_t launch_czt_tables(int nruns, int ne, double dt, const double *e0, co
                               double2 *tw, double2 *g, double2 *b, cudaStream_t s);
 int flux_accum_launches();
 int flux_variants();
+bool flux_accum_is_czt(const AccumParams &p);   // the chunk takes the chirp-z form
+int flux_q_tiles(int nq);                       // surface-point tiles of the GEMM form
 
 struct CrpParams {
   int n1, nth, ne, nruns;
@@ -218,6 +225,8 @@ template <typename R> cudaError_t launch_lines(const LineParams &p, cudaStream_t
 template <typename R> cudaError_t launch_flux_prep(const FluxParams &p, cudaStream_t s);
 cudaError_t launch_flux_accum(const AccumParams &p, cudaStream_t s);
 cudaError_t launch_crp(const CrpParams &p, cudaStream_t s);
+// P(E) from the per-tile sums that a fused GEMM-form accumulation wrote
+cudaError_t launch_crp_parts(const CrpParams &p, const double *part, int nqt, cudaStream_t s);
 
 // set-up kernels
 cudaError_t launch_setup_tables_fp64(int n1, int n2, int nth, int nl, double dt,

@@ -48,3 +48,23 @@ def test_nonuniform_energies_keep_the_direct_sum(monkeypatch):
     a = _crp(d, 260, monkeypatch, czt=True)
     b = _crp(d, 260, monkeypatch, czt=False)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, 1])
+def test_pe_fused_into_the_closing_accumulation(prec, monkeypatch):
+    # a call that ends with a partial chunk: its GEMM-form accumulation also
+    # sums P(E) per tile; the separate P(E) pass over phi_E must agree
+    d = _case(prec, 140)
+    out = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("QD_CRP_FUSED", fused)
+        with Propagator(S.copy_case(d)) as p:
+            p.propagate(70)
+            first = p.crp()
+            p.propagate(70)
+            out[fused] = (first, p.crp())
+    for a, b in zip(out["1"], out["0"]):
+        scale = np.abs(b).max()
+        assert scale > 0
+        assert np.abs(a - b).max() < 1e-12 * scale + 1e-15
