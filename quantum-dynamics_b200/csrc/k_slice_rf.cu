@@ -47,15 +47,13 @@
 // dimension) and the rotational energy of the step's final l-space values.
 //
 // A slice may also run on a 2-CTA cluster (for small batches, where one CTA
-// per slice leaves most SMs idle): each CTA then keeps half the rows for the
-// row passes and half the columns, over all rows, for the column passes; the
-// one transpose between them is a set of bulk shared-memory-to-shared-memory
-// copies of whole row halves, so no pass touches the other CTA's memory
-// itself.  A 256 x 192 slice (384 KB) runs on a 4-CTA cluster, a quarter of
-// the rows and of the columns per CTA; its transpose is folded into the last
-// row pass, which stores each result into the CTA whose columns it belongs to
-// (rounds of rows between cluster barriers), so each CTA holds only its own
-// 101 KB of rows and two clusters' CTAs share an SM.
+// per slice leaves most SMs idle) or, at 256 x 192 (384 KB), on a 4-CTA
+// cluster: each CTA then keeps 1/CL of the rows for the row passes and 1/CL
+// of the columns, over all rows, for the column passes.  The one transpose
+// between them is folded into the last row pass, which stores each result
+// into the CTA whose columns it belongs to (rounds of rows between cluster
+// barriers), so each CTA holds only its own rows (101 KB at 256 x 192, where
+// two clusters' CTAs share an SM).
 //
 // The 6-, 12-, 16-, 24- and 32-point DFTs are P x Q compositions whose
 // internal twiddles are compensated constants (value + residual), like the
@@ -235,26 +233,18 @@ template <int N1, int N2, int NT, int CL, int A1X = 0> struct RfShape {
   static constexpr int HR = N2 / CL;                  // rows held by one CTA
   static constexpr int HW = RS / CL;                  // column part width: B1 / CL whole blocks
   static constexpr int BPO = B2 / CL;                 // column-pass row groups per CTA's rows
-  // CL = 4: the transpose swaps row parts between the CTAs in place (SWAP),
-  // so a CTA holds only its row array and two CTAs fit on an SM; CL = 2
-  // receives the peer's rows of its column part in a second array, filled
-  // by bulk copies
-  static constexpr bool SWAP = CL == 4;
-  static constexpr int PSLOTS = CL == 1 || SWAP ? 0 : CL - 1;
+  // CL > 1: the transpose moves row parts between the CTAs' row arrays in
+  // place (pc_swap), so a CTA holds only its own rows
   static constexpr int P1_UNROLL = 2;                // row items per thread loaded together
-  // own rows [HR][RS]; CL = 2: the peer's rows of this CTA's column part
-  // [HR][HW]; rc1[l], kc1 (N1 each), W_N2, kc2, rc2[l] (N2 each); CL = 2:
-  // one mbarrier
+  // own rows [HR][RS]; rc1[l], kc1 (N1 each), W_N2, kc2, rc2[l] (N2 each)
   static constexpr size_t TABLES = 2 * N1 + 3 * N2;
-  static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + (size_t)PSLOTS * HR * HW +
-                                                   TABLES) + (PSLOTS > 0 ? 16 : 0);
-  static constexpr uint32_t HALF_BYTES = sizeof(float2) * HW;   // one row part, one bulk copy
+  static constexpr size_t SMEM = sizeof(float2) * ((size_t)HR * RS + TABLES);
   // 8 B1 blocks of A1 + 1 slots with RS = 8 mod 16, or 16 blocks with RS = 0
   // mod 16: either way a warp's access of any pass touches each bank pair twice
   static_assert((B1 == 8 && RS % 16 == 8) || (B1 == 16 && RS % 16 == 0), "row layout");
   static_assert(NT % A1 == 0 && NT % B1 == 0, "per-thread constant row index");
   static_assert(CL == 1 || ((CL == 2 || CL == 4) && B1 % CL == 0 && HR == BPO * A2 &&
-                            HW == (B1 / CL) * (A1 + 1) && HALF_BYTES % 16 == 0),
+                            HW == (B1 / CL) * (A1 + 1)),
                 "cluster split: whole row blocks per column part, whole column row groups per CTA");
 };
 
@@ -267,33 +257,10 @@ __device__ __forceinline__ uint32_t peer_addr(uint32_t a, uint32_t rank)
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
   return r;
 }
-__device__ __forceinline__ void cluster_arrive_relaxed()
-{ asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_arrive_release()
 { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait()
 { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
-// bulk copy of `bytes` from this CTA's shared memory into the peer's, whose
-// mbarrier receives the byte count
-__device__ __forceinline__ void bulk_to_peer(uint32_t dst, uint32_t src, uint32_t bytes, uint32_t mbar)
-{
-  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               :: "r"(dst), "r"(src), "r"(bytes), "r"(mbar) : "memory");
-}
-// bounded wait on phase 0 of a local mbarrier; false if it ran out
-__device__ __forceinline__ bool mbar_wait0(uint32_t mbar)
-{
-  for (int it = 0; it < (1 << 22); it++) {
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], 0;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}\n"
-                 : "=r"(ok) : "r"(mbar) : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
 // st.shared::cluster of 8 bytes (a mapa address)
 __device__ __forceinline__ void st_peer2(uint32_t a, float2 v)
 {
@@ -359,13 +326,11 @@ __device__ __forceinline__ void pc_swap(float2 *R, const float2 *r1, const float
 // CL = 2 or 4: a CL-CTA thread-block cluster per slice.  CTA `rank` runs
 // the row passes on rows [rank HR, (rank+1) HR) and the column passes on
 // column part `rank` (row blocks rank B1/CL .. (rank+1) B1/CL - 1, columns
-// rank N1/CL .. (rank+1) N1/CL - 1) over all N2 rows.  CL = 2: its own rows
-// in place in its row array, the peer's rows in a second array, filled after
-// Pc by bulk copies of whole row halves (544 bytes) from the peer (an
-// mbarrier in the receiving CTA counts the bytes in).  CL = 4: Pc stores its
-// results into the CTA that holds their column part (pc_swap), after which row
-// part o of the row array holds CTA o's rows in this CTA's column part.  Every
-// load and store of the other passes is local.  CL = 1 keeps the slice in one array in place.
+// rank N1/CL .. (rank+1) N1/CL - 1) over all N2 rows.  Pc stores its results
+// into the CTA that holds their column part (pc_swap), after which row part o
+// of the row array holds CTA o's rows in this CTA's column part; every load
+// and store of the other passes is local.  CL = 1 keeps the slice in one array
+// in place.
 template <int N1, int N2, int NT, int CL, int A1X>
 __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 {
@@ -374,13 +339,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   constexpr int HR = Sh::HR, HW = Sh::HW;
   extern __shared__ float4 smem4[];
   float2 *R = reinterpret_cast<float2 *>(smem4);    // own rows [HR][RS]
-  float2 *P = R + HR * RS;                           // CL = 2: peer rows, own column part [HR][HW]
-  float2 *r1 = P + Sh::PSLOTS * HR * HW;             // rc1[l][0..N1)
+  float2 *r1 = R + HR * RS;                          // rc1[l][0..N1)
   float2 *k1 = r1 + N1;                              // kc1
   float2 *t2 = k1 + N1;                              // W_N2^k, k < N2
   float2 *k2 = t2 + N2;                              // kc2
   float2 *r2 = k2 + N2;                              // rc2[l][0..N2)
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(r2 + N2);   // CL = 2: the peer's rows are in
   __shared__ double red[32];                         // energy steps: block sums
   const int tid = threadIdx.x;
   pdl_trigger();
@@ -392,17 +355,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   }
   int rank = 0;
   if constexpr (CL > 1) asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  if constexpr (Sh::PSLOTS > 0) {
-    if (tid == 0) {
-      const uint32_t tx = (CL - 1) * HR * Sh::HALF_BYTES;   // from every peer, every row
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar[0])));
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                   :: "r"(smem_addr(&mbar[0])), "r"(tx) : "memory");
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    cluster_arrive_relaxed();                        // waited on before the first copy
-  }
   const int sl = blockIdx.x / CL, l = rot_row(p, sl);   // slice = run * nl + l; l = table row
   const int j0 = rank * HR, q0 = rank * (N1 / CL);
   float2 *g = reinterpret_cast<float2 *>(p.lpsi) + (long)sl * (N1 * N2);
@@ -470,8 +422,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   __syncthreads();
   // Pc: items (j, a): slot a of every block c, W^{-a c}, B1-point inverse DFT
   // over c -> element i = a + A1 b, D1 -> slot a of block b (the same slots);
-  // CL = 4: fused with the transpose (pc_swap)
-  if constexpr (!Sh::SWAP) {
+  // CL > 1: fused with the transpose (pc_swap)
+  if constexpr (CL == 1) {
     const int a = tid % A1;
     float2 w[B1];
 #pragma unroll
@@ -488,30 +440,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
 #pragma unroll
       for (int b = 0; b < B1; b++) R[j * RS + a + (A1 + 1) * b] = cmul(v[b], r1[a + A1 * b]);
     }
-  }
-  bool ok = true;
-  if constexpr (Sh::SWAP) {
-    pc_swap<A1, B1, RS, HR, HW, NT, CL>(R, r1, tw1, rank, tid);
-  } else if constexpr (CL > 1) {
-    // peer o's column part of every own row -> this CTA's slot of o's P array
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    cluster_wait();                                  // the peers' mbarriers are initialised
-    for (int e = tid; e < (CL - 1) * HR; e += NT) {
-      const int pi = e / HR, j = e % HR;
-      const uint32_t peer = pi < rank ? pi : pi + 1;
-      const int slot = rank < (int)peer ? rank : rank - 1;
-      bulk_to_peer(peer_addr(smem_addr(P + (slot * HR + j) * HW), peer),
-                   smem_addr(R + j * RS + HW * peer), Sh::HALF_BYTES,
-                   peer_addr(smem_addr(&mbar[0]), peer));
-    }
-    ok = mbar_wait0(smem_addr(&mbar[0]));            // the peers' rows of this part are in
-    // this CTA's incoming copies are complete; the peers wait on this
-    // barrier at exit, so no CTA leaves while a copy out of it may run
-    cluster_arrive_release();
-    if (!ok && tid == 0 && p.status) atomicExch(p.status, 2);
   } else {
-    __syncthreads();
+    pc_swap<A1, B1, RS, HR, HW, NT, CL>(R, r1, tw1, rank, tid);
   }
 
   // ---- the column operator D2 IFFT_r K2 FFT_r D2 on this CTA's columns ------------
@@ -519,18 +450,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   // part; row A2 b + r (b < B2) is held by CTA b / BPO, as its row A2 (b % BPO) + r
   constexpr int BPO = Sh::BPO;
   auto pcol = [](int qq) { return (qq % A1) + (A1 + 1) * (qq / A1); };
-  float2 *cb[Sh::SWAP ? 1 : CL];                     // row 0 of CTA o's rows, this part
-  int cs[Sh::SWAP ? 1 : CL];                         // and their row stride
-  if constexpr (!Sh::SWAP) {
-#pragma unroll
-    for (int o = 0; o < CL; o++) {
-      cb[o] = o == rank ? R + HW * rank : P + (o - (o > rank ? 1 : 0)) * HR * HW;
-      cs[o] = o == rank ? RS : HW;
-    }
-  }
   auto at = [&](int b, int inner, int qq) -> float2 & {
-    if constexpr (Sh::SWAP) return R[(inner + A2 * (b % BPO)) * RS + HW * (b / BPO) + pcol(qq)];
-    else return cb[b / BPO][(inner + A2 * (b % BPO)) * cs[b / BPO] + pcol(qq)];
+    return R[(inner + A2 * (b % BPO)) * RS + HW * (b / BPO) + pcol(qq)];
   };
   constexpr int QC = N1 / CL;
   // Pd: items (q, a'): rows a' + A2 b, D2, B2-point DFT over b, W^{a' c} -> rows a' + A2 c
@@ -547,19 +468,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
   // Pe: items (q, c'): rows a' + A2 c'; forward pass 2, K2 / (n1 n2), inverse pass 1
   for (int e = tid; e < QC * B2; e += NT) {
     const int qq = e % QC, cp = e / QC;
-    float2 *col;
-    int cst;
-    if constexpr (Sh::SWAP) {
-      col = R + A2 * (cp % BPO) * RS + HW * (cp / BPO) + pcol(qq);
-      cst = RS;
-    } else {
-      float2 *cbase = cb[0];
-      cst = cs[0];
-#pragma unroll
-      for (int o = 1; o < CL; o++)
-        if (cp / BPO == o) { cbase = cb[o]; cst = cs[o]; }
-      col = cbase + A2 * (cp % BPO) * cst + pcol(qq);
-    }
+    float2 *col = R + A2 * (cp % BPO) * RS + HW * (cp / BPO) + pcol(qq);
+    constexpr int cst = RS;
     float2 v[A2];
 #pragma unroll
     for (int a = 0; a < A2; a++) v[a] = col[a * cst];
@@ -610,10 +520,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_slice_rf(LineParams p)
     const double er = block_sum(e_r, red);
     if (tid == 0) atomicAdd(p.esum + 3 * run + 1, er * jj * (jj + 1.0) * wl);
   }
-  // CL = 2: no CTA leaves while its shared memory may still be the source of
-  // a copy (a peer arrives only once all of its incoming copies are
-  // complete); CL = 4 touches no peer's memory after the swap's final barrier
-  if constexpr (Sh::PSLOTS > 0) cluster_wait();
+  // (no CTA touches a peer's memory after the transpose's closing barrier)
 }
 
 template <int N1, int N2, int NT, int CL, int A1X = 0>

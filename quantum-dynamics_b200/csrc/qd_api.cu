@@ -563,7 +563,6 @@ struct qd_handle {
   double2 *d_expV = nullptr, *d_rot = nullptr, *d_kin = nullptr;
   float2 *d_expV32 = nullptr;
   float2 *d_rc1 = nullptr, *d_rc2 = nullptr, *d_kc1 = nullptr, *d_kc2 = nullptr;
-  int *d_lstatus = nullptr;       // status word of the l-space kernels (0 = ok)
   int slice_cluster = 0;          // l-space kernel (LineParams::cluster code)
   int flux_variant = 0;           // flux-accumulation GEMM tile variant (tune_flux)
   bool psi_z_valid = false;       // d_psi_z holds the theta-space state of every run
@@ -779,19 +778,14 @@ FluxParams flux_params(qd_handle *h)
 int after_flux_prep(qd_handle *h);
 template <typename R> int issue_flux_prep(qd_handle *h);
 
-// Device-side status words of the tensor-core pass and of the l-space
-// kernels (bounded waits that ran out).
+// Device-side status word of the tensor-core pass (bounded waits that ran
+// out; the l-space kernels wait only on hardware cluster barriers).
 int check_status(qd_handle *h)
 {
   int st = 0;
   if (h->use_tc) {
     CU(cudaMemcpy(&st, tc_status_ptr(h->tc), sizeof(int), cudaMemcpyDeviceToHost));
     if (st) return set_err(QD_ERR_DEVICE, "tensor-core column pass: an MMA completion wait "
-                           "timed out (status %d)", st);
-  }
-  if (h->d_lstatus) {
-    CU(cudaMemcpy(&st, h->d_lstatus, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st) return set_err(QD_ERR_DEVICE, "l-space pass: a shared-memory exchange wait "
                            "timed out (status %d)", st);
   }
   return QD_OK;
@@ -895,7 +889,6 @@ LineParams line_params(qd_handle *h, bool f32)
   else { p.tw1 = h->d_tw1_32; p.tw2 = h->d_tw2_32; }
   p.pl1 = h->pl1; p.pl2 = h->pl2;
   p.run_k = h->d_run_k; p.jrows = h->jrows;
-  p.status = h->d_lstatus;
   p.T1 = h->d_T1; p.T2 = h->d_T2; p.I1 = h->d_I1; p.I2 = h->d_I2;
   p.orth = h->prec == QD_PREC_FP32 && h->use_tc ? 1 : 0;
   return p;
@@ -1485,8 +1478,6 @@ int create(const qd_data *runs, int nruns, qd_handle **out)
     TRY(h->alloc(h->d_rc2, (size_t)h->jrows * h->n2));
     TRY(h->alloc(h->d_kc1, h->n1));
     TRY(h->alloc(h->d_kc2, h->n2));
-    TRY(h->alloc(h->d_lstatus, 1));
-    CU(cudaMemsetAsync(h->d_lstatus, 0, sizeof(int), h->st));
     CU(launch_setup_tables_fp32(h->n1, h->n2, h->nth * npot, h->jrows, h->dt, h->d_pot, h->d_I1,
                                 h->d_I2, h->d_T1, h->d_T2, h->d_expV32, h->d_rc1, h->d_rc2,
                                 h->d_kc1, h->d_kc2, h->st));

@@ -128,7 +128,6 @@ struct LineParams {
   // the rotational tables have jrows rows
   const int *run_k;
   int jrows;
-  int *status;             // device status word: bounded waits that ran out (0 = ok)
   // energy step (null: none): per run r, esum[3 r] += the kinetic energy sum (the
   // (T1 + T2) |FFT2 psi_l|^2 / (n1 n2) of kinetic_energy_for_legendre_psi,
   // timeEvol.C:390-436) and esum[3 r + 1] += sum j(j+1) (I1 + I2) |psi_l|^2 after the
