@@ -506,30 +506,6 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
       tile_frow = jb >= p.surf_j0 && ja < p.surf_j0 + p.surf_nrows;
     }
     const bool slow = mode == COL_TAIL || !t.renorm || p.out_z || tile_frow || p.esum;
-    // a closing (TAIL) tile with no flux row, no theta output and no energy sum
-    // needs only its norm, which the transform (an isometry per grid column)
-    // leaves as the point's l-space norm times the absorber's square, as on the
-    // fast tiles of a step: no GEMM for it
-    if (mode == COL_TAIL && t.renorm && !tile_frow && !p.out_z && !p.esum) {
-      float nl_part = 0.f;
-#pragma unroll
-      for (int u = 0; u < H; u++) nl_part = fmaf(a[u], a[u], nl_part);
-      nl_part += __shfl_xor_sync(0xffffffffu, nl_part, 1);
-      if (!is_im) xch[grp * TPTS + pt] = nl_part;
-      __syncthreads();
-      if (p.norm_out) {
-        float nl_pt = 0.f;
-#pragma unroll
-        for (int g = 0; g < NG; g++) nl_pt += xch[g * TPTS + pt];
-        double s = (grp == 0 && !is_im && qok) ? (double)(ddv * ddv * nl_pt) : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
-      }
-      __syncthreads();                          // xch is written again by the next tile
-      QD_PREFETCH_A(tile + (int)gridDim.x);
-      continue;
-    }
     float n_l = 0.f, sc = 1.f;
     int pe = 0;                                 // the point's scale exponent
     // GEMM1 output (theta values) of this thread; with one CTA per SM (128
