@@ -121,6 +121,24 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
     if (e >= p.ne || q >= p.nq) return nullptr;
     return (c < GQ ? p.fai : p.dfai) + ((size_t)run * p.ne + e) * p.nq + q;
   };
+  // with crp_part: this tile's share of P(E), the sum over its points of
+  // w_k Im(conj(phi) dphi) of the updated values (columns j and j + 2 of a
+  // thread are phi and dphi of one point; entries past n_E or past the
+  // surface are zero), formed as each energy row pair is written and reduced
+  // over the 16 column groups of each row at the end.  A tile of GQ points
+  // spans at most two theta rows when n1 >= GQ.
+  const bool want_pe = p.crp_part != nullptr;
+  double wq[2] = {0.0, 0.0};
+  if (want_pe) {
+    const int k0 = q0 / p.n1;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int q = q0 + tc + 16 * j;
+      const int k = p.n1 >= GQ ? (q - k0 * p.n1 >= p.n1 ? k0 + 1 : k0) : q / p.n1;
+      wq[j] = q < p.nq ? __ldg(p.w + k) : 0.0;
+    }
+  }
+  double pe[4];
 #pragma unroll
   for (int h = 0; h < 4; h += 2) {
 #pragma unroll
@@ -135,27 +153,20 @@ __global__ void __launch_bounds__(GE * 4) k_flux_gemm(AccumParams p)
         }
       }
 #pragma unroll
-    for (int i = h; i < h + 2; i++)
+    for (int i = h; i < h + 2; i++) {
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         double2 *dst = at(i, j);
         if (dst) *dst = acc[i][j];
       }
+      pe[i] = wq[0] * (acc[i][0].x * acc[i][2].y - acc[i][0].y * acc[i][2].x) +
+              wq[1] * (acc[i][1].x * acc[i][3].y - acc[i][1].y * acc[i][3].x);
+    }
   }
-  if (p.crp_part) {
-    // this tile's share of P(E): sum over its points of w_k Im(conj(phi) dphi)
-    // of the updated values (columns j and j + 2 of a thread are phi and dphi
-    // of one point; entries past n_E or past the surface are zero), reduced
-    // over the 16 column groups of each energy row
+  if (want_pe) {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      double sum = 0.0;
-#pragma unroll
-      for (int j = 0; j < 2; j++) {
-        const int q = q0 + tc + 16 * j;
-        if (q < p.nq)
-          sum += p.w[q / p.n1] * (acc[i][j].x * acc[i][j + 2].y - acc[i][j].y * acc[i][j + 2].x);
-      }
+      double sum = pe[i];
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
       const int e = e0 + te + (GE / 4) * i;
