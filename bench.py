@@ -403,7 +403,7 @@ def run_ours(args):
     t_max = grp.max(dev["ms"])
     value = pts * K * world / (t_max * 1e-3)
 
-    # --- the plain FP64 form on the same workload (the north-star ratio) ---------------
+    # --- the plain FP64 form on the same workload (the batched form's speed-up over it) ---
     fp64 = None
     if not args.fp64 and not args.no_fp64_arm:
         grp.barrier()

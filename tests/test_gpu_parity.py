@@ -1,7 +1,7 @@
 """GPU propagation through the C ABI against the CPU oracle (which is pinned
 bit-exactly to the reference's own common/timeEvol.C).
 
-Tolerances (north_star): FP64 plain form -- wavepacket norm 1e-10 relative,
+Tolerances of the path's precision contract: FP64 plain form -- wavepacket norm 1e-10 relative,
 P(E) 1e-8 absolute; complex64 form -- |dP(E)| <= 1e-3 over energies where
 eta^2 > 1e-3 max eta^2, norm 1e-5 relative.
 """
