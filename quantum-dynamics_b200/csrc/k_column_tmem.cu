@@ -535,6 +535,9 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
           gemm_split_ts<S, false>(D, Ahi, Alo, dk0);
           mma_commit(mb1);
         }
+        // TAIL: this tile's values are in TMEM, so the next tile's loads can
+        // fly during its GEMM and theta-space work
+        if (mode == COL_TAIL) QD_PREFETCH_A(tile + (int)gridDim.x);
       } else {
         n_l = n_l_next;
         pe = norm_exp(n_l);
@@ -676,10 +679,7 @@ __global__ void __launch_bounds__(nthreads(S), ctas_per_sm(S)) k_column_tc(Colum
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       if (grp == 0 && lane == 0) atomicAdd(p.norm_out + run, s);
     }
-    if (mode == COL_TAIL) {
-      QD_PREFETCH_A(tile + (int)gridDim.x);
-      continue;
-    }
+    if (mode == COL_TAIL) continue;            // the next tile's loads were issued after GEMM1
     // ---- GEMM2: psi' = Q^T A2 ------------------------------------------------------------
     if (tid == 0) {
       tc_fence_after();
